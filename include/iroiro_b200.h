@@ -1,0 +1,200 @@
+/* iroiro_b200.h -- C ABI of the B200 fermion-solve library.
+ *
+ * Drop-in for the hot path of IroIro's Wilson-type fermion solves.  Every
+ * entry point returns an int status (IRO_OK on success) and never throws or
+ * aborts; the message for the last failure on a context is available from
+ * iro_last_error().
+ *
+ * Host arrays are in the reference's own layouts:
+ *   spinor  (Format_F, include/format_F.h:36-42)
+ *           index_r(c,s,site) = 2*(c + 3*s) + 24*site     (24 doubles/site)
+ *           full-lattice fields: site = x + Lx*(y + Ly*(z + Lz*t))
+ *           e/o half fields:     site = hs, the hs-th even (odd) site in
+ *                                lexicographic order, i.e. SiteIndex_EvenOdd
+ *                                esec/osec (lib/Geometry/siteIndex_EvenOdd.cpp:21-62)
+ *   gauge   (Format_G, include/format_G.h:34-36)
+ *           index_r(c1,c2,site,mu) = 2*(3*c1 + c2) + 18*(site + V*mu)
+ * They are converted once at the boundary into the device layouts; gauge and
+ * clover data stay resident on the GPU until the next upload.
+ *
+ * Operators are given by `mass` as in the reference constructors
+ * (Dirac_Wilson(double mass, const Field* u), lib/Dirac_ops/dirac_wilson.hpp:89-128);
+ * kappa = 0.5/(4 + mass) exactly as dirac_wilson.hpp:93 computes it.
+ */
+#ifndef IROIRO_B200_H
+#define IROIRO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+  IRO_OK = 0,
+  IRO_NOT_CONVERGED = 1, /* Solver_CG aborts (lib/Solver/solver_CG.cpp:63-67) and
+                            MultiShiftSolver_CG throws (multiShiftSolver_CG.cpp:163)
+                            in this case; here the best iterate is still returned */
+  IRO_BAD_ARG = 2,       /* the reference asserts on size mismatches
+                            (include/common_fields.hpp:48) */
+  IRO_CUDA_ERROR = 3,
+  IRO_TIMEOUT = 4,       /* a device-side wait hit its iteration limit */
+  IRO_NO_GAUGE = 5,      /* operator applied before iro_gauge_upload */
+  IRO_NO_CLOVER = 6,     /* clover operator applied before iro_clover_setup */
+  IRO_OUT_OF_MEMORY = 7
+};
+
+/* ---- operators ----------------------------------------------------------- */
+enum {
+  /* Dirac_Wilson(mass,u)::mult, full lattice: f - kappa*H f
+     (lib/Dirac_ops/dirac_wilson.cpp:28-32,115-118) */
+  IRO_OP_WILSON_FULL = 0,
+  /* Dirac_Wilson(mass,u,Dop::EOtag)::mult: -kappa*H_eo f_o, odd -> even
+     (lib/Dirac_ops/dirac_wilson.hpp:89-100, dirac_wilson.cpp:107-113) */
+  IRO_OP_WILSON_HOP_EO = 1,
+  /* Dirac_Wilson(mass,u,Dop::OEtag)::mult: -kappa*H_oe f_e, even -> odd
+     (lib/Dirac_ops/dirac_wilson.hpp:103-114) */
+  IRO_OP_WILSON_HOP_OE = 2,
+  /* Dirac_Wilson_EvenOdd<Dirac_Wilson>::mult: f_e - kappa^2 H_eo H_oe f_e
+     (lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:80-84) */
+  IRO_OP_WILSON_SCHUR_EE = 3,
+  /* Dirac_Clover::mult, full lattice: A f - kappa*H f with
+     A = 1 - kappa*csw*sum F_{mu nu} (i sigma_{mu nu})
+     (lib/Dirac_ops/dirac_clover.cpp:38-136,334-349) */
+  IRO_OP_CLOVER_FULL = 4,
+  /* Even-odd clover Schur operator A_ee - kappa^2 H_eo A_oo^-1 H_oe.  The
+     reference has no e/o clover; this is the Schur complement of
+     IRO_OP_CLOVER_FULL on even sites. */
+  IRO_OP_CLOVER_SCHUR_EE = 5,
+  /* -kappa*A_ee^-1... hopping blocks with the clover inverse applied to the
+     output sites: A_oo^-1 (-kappa H_oe) f_e, used to rebuild odd sites */
+  IRO_OP_CLOVER_HOP_OE_INV = 6
+};
+
+/* ---- storage precisions -------------------------------------------------- */
+enum {
+  IRO_PREC_DOUBLE = 0, /* FP64 storage and arithmetic */
+  IRO_PREC_SINGLE = 1, /* FP32 storage and arithmetic */
+  IRO_PREC_HALF = 2    /* FP16 storage (spinors with a per-site FP32 norm),
+                          FP32 arithmetic */
+};
+
+typedef struct iro_ctx iro_ctx;
+typedef struct iro_field iro_field;
+
+/* ---- context ------------------------------------------------------------- */
+/* One context per lattice and device; it owns all device memory.  Replaces
+   the geometry singletons CommonPrms::instance(Lattice)
+   (lib/Main/commonPrms.cpp:22-65) and SiteIndex_EvenOdd
+   (lib/Geometry/siteIndex_EvenOdd.cpp:21-62).  Every extent must be even. */
+int iro_ctx_create(const int L[4], int device, iro_ctx** ctx);
+int iro_ctx_destroy(iro_ctx* ctx);
+const char* iro_last_error(const iro_ctx* ctx);
+/* The CUDA stream (cudaStream_t) the context launches on.  By default the
+   context creates its own; set_stream makes it use the caller's. */
+void* iro_ctx_get_stream(const iro_ctx* ctx);
+int iro_ctx_set_stream(iro_ctx* ctx, void* stream);
+
+/* ---- gauge and clover ---------------------------------------------------- */
+/* Uploads a Format_G gauge field (18*4*V doubles) and keeps it resident in
+   FP64, FP32 and FP16, two-row (reconstruct-12) form when every link is in
+   SU(3) to 1e-12, full 3x3 form otherwise.  This is the update_internal_state
+   hook of the reference (lib/Dirac_ops/dirac.hpp:28).  Invalidates clover. */
+int iro_gauge_upload(iro_ctx* ctx, const double* u);
+
+/* Builds the clover term for (mass, csw) from the resident gauge field:
+   F_{mu nu} by Staples::fieldStrength (lib/Measurements/GaugeM/staples.cpp:587-666),
+   A = 1 - kappa*csw*sum F (i sigma) as two Hermitian 6x6 blocks per site in
+   the gamma5 eigenbasis, and their inverses.  Dirac_Clover::set_csw
+   (lib/Dirac_ops/dirac_clover.cpp:139-162). */
+int iro_clover_setup(iro_ctx* ctx, double mass, double csw);
+
+/* F_{mu nu} as computed on the device, returned in Format_G with one
+   direction (18*V doubles), for checking against Staples::fieldStrength. */
+int iro_field_strength(iro_ctx* ctx, int mu, int nu, double* out);
+
+/* ---- operator application on host fields --------------------------------- */
+/* out = op(in) (dagger=0) or op^dagger(in) = gamma5 op gamma5 (in)
+   (dagger=1; Dirac_Wilson::mult_dag, dirac_wilson.cpp:34-36).  `in` and
+   `out` hold nrhs consecutive fields of the op's size (24*V doubles for full
+   lattice ops, 12*V for e/o ops).  Storage and arithmetic in `prec`. */
+int iro_dirac_apply(iro_ctx* ctx, int op, double mass, double csw, int dagger, int prec,
+                    const double* in, double* out, int nrhs);
+
+/* gamma5 on a host spinor of nsites sites (Dirac_Wilson::gamma5,
+   dirac_wilson.cpp:120-126; GammaMatrix::gamma5core, wilsonLikeUtils.cpp:42-49). */
+int iro_gamma5(iro_ctx* ctx, const double* in, double* out, int64_t nsites);
+
+/* ---- device-resident fields ---------------------------------------------- */
+/* subset: 0 = even half, 1 = odd half, 2 = full lattice (even half then odd
+   half).  Fields hold nrhs right-hand sides in the device layout of `prec`. */
+int iro_field_create(iro_ctx* ctx, int subset, int prec, int nrhs, iro_field** f);
+int iro_field_destroy(iro_field* f);
+int iro_field_upload(iro_ctx* ctx, iro_field* f, const double* host);
+int iro_field_download(iro_ctx* ctx, const iro_field* f, double* host);
+/* out = op(in) on device fields (no host traffic).  Subsets and precisions
+   of in/out must match the operator. */
+int iro_dirac_apply_field(iro_ctx* ctx, int op, double mass, double csw, int dagger,
+                          const iro_field* in, iro_field* out);
+
+/* ---- solvers -------------------------------------------------------------- */
+/* Mirrors SolverOutput (lib/Solver/solver.hpp:16-22). */
+typedef struct {
+  double diff;          /* final true residual |A x - b| / |b| in FP64 */
+  int iterations;       /* 0-based index of the converging iteration as in
+                           Solver_CG::solve (solver_CG.cpp:57-58); -1 if not */
+  double timing_ms;     /* wall time of the solve on the host */
+  int reliable_updates; /* FP64 residual recomputations (mixed precision) */
+  int operator_applies; /* applications of the normal operator */
+} iro_solver_out;
+
+typedef struct {
+  double precision; /* stop when |r|^2/|b|^2 < precision (squared, as
+                       Solver_CG_Prms::GoalPrecision, solver_CG.cpp:57) */
+  int max_iter;
+  int inner_prec;   /* IRO_PREC_DOUBLE: the reference's FP64 CG.
+                       IRO_PREC_SINGLE / IRO_PREC_HALF: reliable-update CG with
+                       inner iterations in that storage, FP32 arithmetic and
+                       FP64 residual recomputation, solution and reductions */
+  double delta;     /* reliable update when |r| < delta * max |r| since the
+                       last update (mixed precision only); <= 0 selects 0.1 */
+  int use_graph;    /* capture the iteration as a CUDA graph */
+} iro_cg_params;
+
+/* Solve (D^dagger D) x = b by CG for the operator `op` (Fopr_DdagD with
+   Solver_CG, lib/Fopr/fopr.h:146-153, lib/Solver/solver_CG.cpp:29-160).
+   The initial guess is x0 = b as in solver_CG.cpp:40.  b and x hold nrhs
+   consecutive fields; the right-hand sides are solved together, sharing
+   every gauge-link load.  out receives nrhs records.  op is one of
+   IRO_OP_WILSON_FULL, IRO_OP_WILSON_SCHUR_EE, IRO_OP_CLOVER_FULL,
+   IRO_OP_CLOVER_SCHUR_EE. */
+int iro_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
+                 const double* b, double* x, int nrhs, iro_solver_out* out);
+
+/* MultiShiftSolver_CG::solve for (D^dagger D + sigma_i) x_i = b
+   (lib/Solver/multiShiftSolver_CG.cpp:95-185) in FP64: x_i = 0 start,
+   convergence on shift 0 only, pruning of converged shifts by
+   |p_i|^2/|b|^2 <= precision.  x holds nshift consecutive fields.  *diff is
+   sqrt of the largest squared relative true residual, *nconv the iteration
+   index of convergence (-1 if not). */
+int iro_multishift_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const double* b,
+                            int nshift, const double* shifts, double* x, double precision,
+                            int max_iter, iro_solver_out* out, int* nconv);
+
+/* ---- synthetic inputs (host) ---------------------------------------------- */
+/* Seeded SU(3) field U = exp(i eps H), H = sum theta_a lambda_a / 2,
+   theta_a ~ N(0,1), projected onto SU(3); optionally followed by a random
+   gauge transformation U_mu(x) -> G(x) U_mu(x) G(x+mu)^dagger.  Format_G. */
+int iro_synth_gauge(const int L[4], double eps, uint64_t seed, int gauge_transform, double* u);
+/* N(0,1) in every real component of nsites Format_F sites. */
+int iro_synth_gaussian(int64_t nsites, uint64_t seed, double* f);
+/* The 12 point sources (c,s) at `site`, Source_local semantics
+   (lib/Measurements/FermionicM/source_types.hpp:40-60): 12 consecutive
+   Format_F fields of nsites sites. */
+int iro_synth_point_sources(int64_t nsites, int64_t site, double* f12);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IROIRO_B200_H */
