@@ -1,0 +1,412 @@
+"""Benchmark of the even-odd Wilson Dslash hot path on B200.
+
+Workload (one "step"): one application of the even-odd Schur operator
+Dirac_Wilson_EvenOdd<Dirac_Wilson>::mult, M f_e = f_e - kappa^2 H_eo H_oe f_e
+(lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:80-84), on a 24^3x48 lattice, kappa =
+0.12, seeded synthetic SU(3) links exp(i*0.2*H) followed by a random gauge
+transformation, FP64 storage and arithmetic (the reference's own arithmetic),
+reconstruct-12 links.  One step = two launches of the hopping kernel.
+
+value     algorithmic GB/s of the step, fields resident in HBM, L2 flushed
+          (256 MiB written) before every step, CUDA events on the launching
+          stream around each step; summed over ranks (replicas) / max time.
+e2e       the same metric through the C ABI with host buffers:
+          iro_dirac_apply() on pinned Format_F arrays, H2D + D2H inside the
+          timed region.
+roofline  achieved = algorithmic bytes per hopping launch / its mean
+          duration; bytes per even output site 2496 (8 neighbour spinors,
+          8 two-row links, 1 output spinor) for the first hop and 2688
+          (+ the f_e read of the fused x + a*y epilogue) for the second.
+solve     time to a 1e-10 FP64 true relative residual on the e/o Wilson-
+          clover Schur operator (csw=1.0) of the same field, for the
+          reference's FP64 CG and the mixed-precision reliable-update CG.
+
+--impl reference runs the reference's own C++ (compiled from its sources
+into oracle/_ref) on the host cores for the same metric, config and step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L = [24, 24, 24, 48]
+KAPPA = 0.12
+MASS = 0.5 / KAPPA - 4.0
+CSW = 1.0
+EPS = 0.2
+SEED = 20240601
+BYTES_HOP = 2496          # FP64, reconstruct-12, per even/odd output site
+BYTES_XPAY = 192          # extra f_e read of the fused epilogue
+FLOPS_SCHUR = 2 * 1320 + 48
+METRIC = "EO-Wilson Dslash GB/s (FP64 Schur operator, algorithmic bytes)"
+WORKLOAD = "Dirac_Wilson_EvenOdd::mult 24^3x48, kappa=0.12, FP64, recon-12"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def traffic_per_launch(vh: int):
+    """DRAM bytes per hopping launch from the committed ncu summary, scaled
+    from the captured lattice to this one by the sites processed."""
+    p = ROOT / "profiles" / "hop_fp64_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d["dram_bytes_per_site"]) * vh
+    except (KeyError, ValueError):
+        return None
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- reference arm ----------------------------------------------------------------------
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libiroiro_ref.so was not built (needs the reference tree)"}))
+        return 0
+    import iroiro_b200 as ib
+    V = int(np.prod(L))
+    u = ib.synth_gauge(L, EPS, SEED, gauge_transform=True)
+    f = ib.synth_gaussian(V // 2, SEED + 1)
+    ref = oracle.ref()
+    ref.init(L)
+    threads = cpu_cores()
+    for _ in range(args.warmup):
+        ref.eo_mult_throughput(u, MASS, f, threads, 1)
+    t = 0.0
+    for _ in range(args.steps):
+        _, s = ref.eo_mult_throughput(u, MASS, f, threads, 1)
+        t += s
+    steps_bytes = (2 * BYTES_HOP + BYTES_XPAY) * (V // 2) * threads * args.steps
+    val = steps_bytes / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": L, "kappa": KAPPA,
+                   "sample": f"{threads} concurrent Dirac_Wilson_EvenOdd::mult per step"},
+        "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{threads} threads x 1 mult per step, {args.steps} steps"},
+        "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline_leg():
+    """The reference's own e/o mult on the host cores, a bounded sample."""
+    import oracle
+    import iroiro_b200 as ib
+    if not oracle.ref_available():
+        return None
+    V = int(np.prod(L))
+    u = ib.synth_gauge(L, EPS, SEED, gauge_transform=True)
+    f = ib.synth_gaussian(V // 2, SEED + 1)
+    ref = oracle.ref()
+    ref.init(L)
+    threads = cpu_cores()
+    ref.eo_mult_throughput(u, MASS, f, threads, 1)
+    reps = 3
+    _, s = ref.eo_mult_throughput(u, MASS, f, threads, reps)
+    val = (2 * BYTES_HOP + BYTES_XPAY) * (V // 2) * threads * reps / s / 1e9
+    return {"value": round(val, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+            "sample": f"{threads} threads x {reps} Dirac_Wilson_EvenOdd::mult at 24^3x48 "
+                      f"({s:.1f} s)"}
+
+
+# ---- our arm --------------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import torch
+    import iroiro_b200 as ib
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    V = int(np.prod(L))
+    Vh = V // 2
+    u = ib.synth_gauge(L, EPS, SEED + rank, gauge_transform=True)
+    h = ib.synth_gaussian(Vh, SEED + 100 + rank)
+    ctx = ib.Context(L, local)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_gauge(u, force=True)
+    lib = ctx._lib
+    import ctypes
+    fin = ctypes.c_void_p()
+    fout = ctypes.c_void_p()
+    ctx.check(lib.iro_field_create(ctx.h, 0, ib.PREC_DOUBLE, 1, ctypes.byref(fin)), "field")
+    ctx.check(lib.iro_field_create(ctx.h, 0, ib.PREC_DOUBLE, 1, ctypes.byref(fout)), "field")
+    ctx.check(lib.iro_field_upload(ctx.h, fin, h.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              "upload")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, fin, fout),
+                  "apply")
+
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    for s, e in ev:
+        flush.zero_()
+        s.record(stream)
+        step()
+        e.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ck = clocks.stop()
+    t_ms = sum(s.elapsed_time(e) for s, e in ev)
+    t_max = reduce_max(t_ms, world)
+    step_bytes = (2 * BYTES_HOP + BYTES_XPAY) * Vh
+    value = world * step_bytes * args.steps / (t_max * 1e-3) / 1e9
+    achieved = step_bytes / ((t_ms / args.steps) * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+
+    # e2e: through the C ABI with pinned host buffers (H2D + D2H inside)
+    hin = torch.from_numpy(h).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    pin_in = ctypes.cast(hin.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    pin_out = ctypes.cast(hout.data_ptr(), ctypes.POINTER(ctypes.c_double))
+
+    def e2e_step():
+        ctx.check(lib.iro_dirac_apply(ctx.h, ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, ib.PREC_DOUBLE,
+                                      pin_in, pin_out, 1), "iro_dirac_apply")
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    es, ee = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    es.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    ee.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(es.elapsed_time(ee), world)
+    e2e_val = world * step_bytes * args.steps / (e2e_ms * 1e-3) / 1e9
+
+    # FP32 / FP16 Schur and clover variants, same protocol (reported, not the headline)
+    variants = {}
+    for name, op, csw, prec, bps in (
+            ("wilson_fp32", ib.OP_WILSON_SCHUR_EE, 0.0, ib.PREC_SINGLE, 2 * 1248 + 96),
+            ("wilson_fp16", ib.OP_WILSON_SCHUR_EE, 0.0, ib.PREC_HALF, 2 * 660 + 52),
+            ("clover_fp64", ib.OP_CLOVER_SCHUR_EE, CSW, ib.PREC_DOUBLE, 2 * (2496 + 576) + 192),
+            ("clover_fp32", ib.OP_CLOVER_SCHUR_EE, CSW, ib.PREC_SINGLE, 2 * (1248 + 288) + 96)):
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        ctx.check(lib.iro_field_create(ctx.h, 0, prec, 1, ctypes.byref(a)), "field")
+        ctx.check(lib.iro_field_create(ctx.h, 0, prec, 1, ctypes.byref(b)), "field")
+        ctx.check(lib.iro_field_upload(ctx.h, a, h.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "up")
+        for _ in range(3):
+            ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, csw, 0, a, b), "apply")
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, csw, 0, a, b), "apply")
+            e.record(stream)
+            e.synchronize()
+            tot += s.elapsed_time(e)
+        ms = tot / args.steps
+        variants[name] = {"ms_per_op": round(ms, 4), "GBps": round(bps * Vh / (ms * 1e-3) / 1e9, 1),
+                          "frac_of_measured_hbm": round(bps * Vh / (ms * 1e-3) / 1e9 / peak, 3)}
+        lib.iro_field_destroy(a)
+        lib.iro_field_destroy(b)
+
+    # time to a 1e-10 FP64 true residual, e/o Wilson-clover, FP64 CG vs mixed precision
+    solve = {}
+    if not args.no_solve:
+        D = ib.Dirac_Clover_EvenOdd(MASS, CSW, u, ctx=ctx)
+        for inner in ("double", "single", "half"):
+            slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner)
+            slv.solve_many(h, 1)  # warm-up (workspace allocation, graph capture)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            x, outs, rc = slv.solve_many(h, 1)
+            dt = time.perf_counter() - t0
+            solve[inner] = {"ms": round(dt * 1e3, 2), "iterations": outs[0].Iterations,
+                            "true_residual": outs[0].diff,
+                            "reliable_updates": outs[0].reliable_updates}
+        base = solve["double"]["ms"]
+        for k in ("single", "half"):
+            solve[k]["speedup_vs_fp64_cg"] = round(base / solve[k]["ms"], 2)
+
+    lib.iro_field_destroy(fin)
+    lib.iro_field_destroy(fout)
+    if rank != 0:
+        return 0
+    cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline_leg()
+    traffic = traffic_per_launch(Vh)
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": L, "kappa": KAPPA, "eps": EPS,
+                   "gauge_transform": True, "l2": "flushed (256 MiB write) before every step",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 3), "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "bytes_model": "per even site: hop 2496 + hop 2496 + f_e 192 (FP64, recon-12)",
+                     "gflops": round(FLOPS_SCHUR * Vh / ((t_ms / args.steps) * 1e-3) / 1e9, 1)},
+        "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": 24 * 8 * Vh,
+                "d2h_bytes_per_step": 24 * 8 * Vh, "ms_per_step": round(e2e_ms / args.steps, 3)},
+        "gpu_launches": 2 * args.steps,
+        "clocks": ck,
+        "variants": variants,
+        "solve": solve,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = (1, 0, 0) if args.impl == "reference" and _env_int("WORLD_SIZE", 1) == 1 \
+        else ((_env_int("WORLD_SIZE", 1), _env_int("RANK", 0), _env_int("LOCAL_RANK", 0))
+              if args.impl == "reference" else dist_setup())
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_ours(args, world, rank, local)
+    finally:
+        if world > 1 and args.impl != "reference":
+            import torch.distributed as dist
+            if dist.is_initialized():
+                dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

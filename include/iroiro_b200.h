@@ -67,8 +67,8 @@ enum {
      reference has no e/o clover; this is the Schur complement of
      IRO_OP_CLOVER_FULL on even sites. */
   IRO_OP_CLOVER_SCHUR_EE = 5,
-  /* -kappa*A_ee^-1... hopping blocks with the clover inverse applied to the
-     output sites: A_oo^-1 (-kappa H_oe) f_e, used to rebuild odd sites */
+  /* First half of the clover Schur operator, A_oo^-1 (-kappa H_oe f_e),
+     even -> odd; it rebuilds odd sites in an even-odd solve. */
   IRO_OP_CLOVER_HOP_OE_INV = 6
 };
 

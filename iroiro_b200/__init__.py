@@ -1,0 +1,527 @@
+"""B200-native fermion-solve hot path of IroIro, behind the reference's interfaces.
+
+The classes here mirror the reference's operator and solver API for this path
+(names, argument meaning and error behaviour), on numpy arrays in the
+reference's own host layouts (Format_F spinors, Format_G links):
+
+=============================  ==============================================
+this package                   reference
+=============================  ==============================================
+``Dirac_Wilson``               lib/Dirac_ops/dirac_wilson.hpp:89-175
+``Dirac_Wilson_EvenOdd``       lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:14-119
+``Dirac_Clover``               lib/Dirac_ops/dirac_clover.hpp:14-100
+``Fopr_DdagD``                 lib/Fopr/fopr.h:146-153
+``Solver_CG``                  lib/Solver/solver_CG.hpp:20-50
+``MultiShiftSolver_CG``        lib/Solver/multiShiftSolver_CG.hpp:30-90
+``SolverOutput``               lib/Solver/solver.hpp:16-22
+=============================  ==============================================
+
+Every computation runs in libiroiro_b200.so (CUDA, sm_100a) through its C
+ABI (include/iroiro_b200.h); there is no CPU fallback: importing works
+without a GPU, but the first operator call raises if the library or a CUDA
+device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "IroError", "ConvergenceError", "lib", "Context", "context", "init",
+    "Dirac_Wilson", "Dirac_Wilson_EvenOdd", "Dirac_Clover", "Dirac_Clover_EvenOdd",
+    "Fopr_DdagD", "Solver_CG", "MultiShiftSolver_CG", "SolverOutput",
+    "synth_gauge", "synth_gaussian", "synth_point_sources",
+    "OP_WILSON_FULL", "OP_WILSON_HOP_EO", "OP_WILSON_HOP_OE", "OP_WILSON_SCHUR_EE",
+    "OP_CLOVER_FULL", "OP_CLOVER_SCHUR_EE", "OP_CLOVER_HOP_OE_INV", "PREC_DOUBLE", "PREC_SINGLE", "PREC_HALF",
+]
+
+_HERE = Path(__file__).resolve().parent
+_LIBPATH = _HERE / "libiroiro_b200.so"
+
+OK, NOT_CONVERGED, BAD_ARG, CUDA_ERROR, TIMEOUT, NO_GAUGE, NO_CLOVER, OUT_OF_MEMORY = range(8)
+(OP_WILSON_FULL, OP_WILSON_HOP_EO, OP_WILSON_HOP_OE, OP_WILSON_SCHUR_EE,
+ OP_CLOVER_FULL, OP_CLOVER_SCHUR_EE, OP_CLOVER_HOP_OE_INV) = range(7)
+PREC_DOUBLE, PREC_SINGLE, PREC_HALF = range(3)
+_PREC = {"double": PREC_DOUBLE, "single": PREC_SINGLE, "half": PREC_HALF,
+         PREC_DOUBLE: PREC_DOUBLE, PREC_SINGLE: PREC_SINGLE, PREC_HALF: PREC_HALF}
+
+
+class IroError(RuntimeError):
+    """A status other than IRO_OK from the library."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class ConvergenceError(IroError):
+    """Solver did not converge: Solver_CG aborts through Errors::ConvergenceErr
+    (lib/Solver/solver_CG.cpp:63-67) and MultiShiftSolver_CG throws
+    "Not converged." (lib/Solver/multiShiftSolver_CG.cpp:163)."""
+
+
+class SolverOut(ctypes.Structure):
+    _fields_ = [("diff", ctypes.c_double), ("iterations", ctypes.c_int),
+                ("timing_ms", ctypes.c_double), ("reliable_updates", ctypes.c_int),
+                ("operator_applies", ctypes.c_int)]
+
+
+class CGParams(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_double), ("max_iter", ctypes.c_int),
+                ("inner_prec", ctypes.c_int), ("delta", ctypes.c_double),
+                ("use_graph", ctypes.c_int)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+_D = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+
+
+def _declare(L):
+    I, D = ctypes.c_int, ctypes.c_double
+    L4 = ctypes.POINTER(ctypes.c_int)
+    sig = {
+        "iro_ctx_create": (I, [L4, I, ctypes.POINTER(_VP)]),
+        "iro_ctx_destroy": (I, [_VP]),
+        "iro_last_error": (ctypes.c_char_p, [_VP]),
+        "iro_ctx_get_stream": (_VP, [_VP]),
+        "iro_ctx_set_stream": (I, [_VP, _VP]),
+        "iro_gauge_upload": (I, [_VP, _D]),
+        "iro_clover_setup": (I, [_VP, D, D]),
+        "iro_field_strength": (I, [_VP, I, I, _D]),
+        "iro_dirac_apply": (I, [_VP, I, D, D, I, I, _D, _D, I]),
+        "iro_gamma5": (I, [_VP, _D, _D, ctypes.c_int64]),
+        "iro_field_create": (I, [_VP, I, I, I, ctypes.POINTER(_VP)]),
+        "iro_field_destroy": (I, [_VP]),
+        "iro_field_upload": (I, [_VP, _VP, _D]),
+        "iro_field_download": (I, [_VP, _VP, _D]),
+        "iro_dirac_apply_field": (I, [_VP, I, D, D, I, _VP, _VP]),
+        "iro_cg_solve": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
+                             ctypes.POINTER(SolverOut)]),
+        "iro_multishift_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, I,
+                                        ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
+        "iro_synth_gauge": (I, [L4, D, ctypes.c_uint64, I, _D]),
+        "iro_synth_gaussian": (I, [ctypes.c_int64, ctypes.c_uint64, _D]),
+        "iro_synth_point_sources": (I, [ctypes.c_int64, ctypes.c_int64, _D]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libiroiro_b200.so; raises if it has not been built."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not _LIBPATH.exists():
+                raise IroError(CUDA_ERROR, f"{_LIBPATH} is missing: run python -m iroiro_b200.build")
+            L = ctypes.CDLL(str(_LIBPATH))
+            _declare(L)
+            _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+def _f64(a, n=None, name="field") -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise IroError(BAD_ARG, f"{name} has {a.size} doubles, expected {n}")
+    return a
+
+
+# ---- synthetic inputs ----------------------------------------------------------------
+
+def synth_gauge(L, eps: float, seed: int, gauge_transform: bool = False) -> np.ndarray:
+    """Seeded SU(3) field exp(i eps H) in Format_G (18*4*V doubles)."""
+    L = [int(v) for v in L]
+    V = int(np.prod(L))
+    u = np.empty(18 * 4 * V)
+    rc = lib().iro_synth_gauge((ctypes.c_int * 4)(*L), eps, seed, int(gauge_transform), _ptr(u))
+    if rc:
+        raise IroError(rc, "iro_synth_gauge")
+    return u
+
+
+def synth_gaussian(nsites: int, seed: int) -> np.ndarray:
+    """N(0,1) in every real component of nsites Format_F sites."""
+    f = np.empty(24 * nsites)
+    rc = lib().iro_synth_gaussian(nsites, seed, _ptr(f))
+    if rc:
+        raise IroError(rc, "iro_synth_gaussian")
+    return f
+
+
+def synth_point_sources(nsites: int, site: int) -> np.ndarray:
+    """The 12 point sources at `site` (Source_local semantics), shape (12, 24*nsites)."""
+    f = np.empty(12 * 24 * nsites)
+    rc = lib().iro_synth_point_sources(nsites, site, _ptr(f))
+    if rc:
+        raise IroError(rc, "iro_synth_point_sources")
+    return f.reshape(12, 24 * nsites)
+
+
+# ---- context -------------------------------------------------------------------------
+
+class Context:
+    """One lattice on one GPU: the geometry singletons of the reference
+    (CommonPrms, SiteIndex_EvenOdd) plus the resident gauge/clover data."""
+
+    def __init__(self, L, device: int = 0):
+        self.L = [int(v) for v in L]
+        self.V = int(np.prod(self.L))
+        self.Vh = self.V // 2
+        self._lib = lib()
+        h = _VP()
+        rc = self._lib.iro_ctx_create((ctypes.c_int * 4)(*self.L), device, ctypes.byref(h))
+        if rc:
+            raise IroError(rc, f"iro_ctx_create({self.L}, device={device})")
+        self.h = h
+        self._gauge_key = None
+
+    def check(self, rc: int, what: str):
+        if rc == OK:
+            return
+        msg = self._lib.iro_last_error(self.h).decode()
+        if rc == NOT_CONVERGED:
+            raise ConvergenceError(rc, f"{what}: {msg}")
+        raise IroError(rc, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.iro_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.iro_ctx_get_stream(self.h) or 0)
+
+    def set_stream(self, stream_handle: int):
+        self.check(self._lib.iro_ctx_set_stream(self.h, _VP(stream_handle)), "set_stream")
+
+    def upload_gauge(self, u: np.ndarray, force: bool = False):
+        u = _f64(u, 72 * self.V, "gauge field")
+        key = (id(u), u.ctypes.data)
+        if force or key != self._gauge_key:
+            self.check(self._lib.iro_gauge_upload(self.h, _ptr(u)), "iro_gauge_upload")
+            self._gauge_key = key
+            self._gauge_ref = u
+
+    def apply(self, op: int, mass: float, csw: float, dag: bool, f: np.ndarray, prec=PREC_DOUBLE,
+              nrhs: int = 1) -> np.ndarray:
+        full = op in (OP_WILSON_FULL, OP_CLOVER_FULL)
+        n = (24 * self.V if full else 12 * self.V) * nrhs
+        f = _f64(f, n, "spinor")
+        out = np.empty(n)
+        self.check(self._lib.iro_dirac_apply(self.h, op, mass, csw, int(bool(dag)), _PREC[prec],
+                                             _ptr(f), _ptr(out), nrhs), "iro_dirac_apply")
+        return out
+
+    def gamma5(self, f: np.ndarray) -> np.ndarray:
+        f = _f64(f)
+        if f.size % 24:
+            raise IroError(BAD_ARG, "gamma5: spinor size not a multiple of 24")
+        out = np.empty_like(f)
+        self.check(self._lib.iro_gamma5(self.h, _ptr(f), _ptr(out), f.size // 24), "iro_gamma5")
+        return out
+
+    def field_strength(self, mu: int, nu: int) -> np.ndarray:
+        out = np.empty(18 * self.V)
+        self.check(self._lib.iro_field_strength(self.h, mu, nu, _ptr(out)), "iro_field_strength")
+        return out
+
+
+_contexts: dict = {}
+
+
+def context(L, device: int = 0) -> Context:
+    """The shared context of lattice L on `device` (created on first use)."""
+    key = (tuple(int(v) for v in L), device)
+    if key not in _contexts:
+        _contexts[key] = Context(L, device)
+    return _contexts[key]
+
+
+_default_L = None
+
+
+def init(L, device: int = 0) -> Context:
+    """Sets the lattice used by operators built without an explicit context,
+    as CommonPrms::instance(Lattice) does for the reference."""
+    global _default_L
+    _default_L = (tuple(int(v) for v in L), device)
+    return context(L, device)
+
+
+def _ctx_for(u: np.ndarray, ctx):
+    if ctx is not None:
+        return ctx
+    if _default_L is None:
+        raise IroError(BAD_ARG, "no lattice: call iroiro_b200.init(L) or pass ctx=")
+    return context(*_default_L)
+
+
+# ---- operators ---------------------------------------------------------------------
+
+class _Dirac:
+    op: int
+    csw = 0.0
+
+    def __init__(self, mass: float, u: np.ndarray, ctx=None, prec="double"):
+        self.ctx = _ctx_for(u, ctx)
+        self.mass = float(mass)
+        self.u = u
+        self.prec = _PREC[prec]
+        self.ctx.upload_gauge(u)
+
+    def update_internal_state(self):
+        """Re-reads the gauge field (Dirac::update_internal_state, dirac.hpp:28)."""
+        self.ctx.upload_gauge(self.u, force=True)
+
+    def _apply(self, op, dag, f, nrhs=1):
+        self.ctx.upload_gauge(self.u)
+        return self.ctx.apply(op, self.mass, self.csw, dag, f, self.prec, nrhs)
+
+    def mult(self, f):
+        return self._apply(self.op, False, f)
+
+    def mult_dag(self, f):
+        return self._apply(self.op, True, f)
+
+    def gamma5(self, f):
+        return self.ctx.gamma5(f)
+
+    def getKappa(self) -> float:
+        return 0.5 / (4.0 + self.mass)
+
+    def getMass(self) -> float:
+        return self.mass
+
+    def gsize(self) -> int:
+        return 72 * self.ctx.V
+
+    def getGaugeField_ptr(self):
+        return self.u
+
+
+class Dirac_Wilson(_Dirac):
+    """Dirac_Wilson(mass, u[, tag]).  tag None: full lattice, mult = f - kappa H f;
+    "EO": -kappa D_eo (odd -> even); "OE": -kappa D_oe (even -> odd)
+    (lib/Dirac_ops/dirac_wilson.hpp:89-128)."""
+
+    def __init__(self, mass, u, tag=None, ctx=None, prec="double"):
+        super().__init__(mass, u, ctx, prec)
+        self.tag = tag
+        self.op = {None: OP_WILSON_FULL, "EO": OP_WILSON_HOP_EO, "OE": OP_WILSON_HOP_OE}[tag]
+
+    def fsize(self) -> int:
+        return 24 * self.ctx.V if self.tag is None else 12 * self.ctx.V
+
+
+class Dirac_Wilson_EvenOdd(_Dirac):
+    """Dirac_Wilson_EvenOdd<Dirac_Wilson>: the Schur operator f - Deo(Doe f) on
+    even half fields (lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:24-92)."""
+
+    op = OP_WILSON_SCHUR_EE
+
+    def fsize(self) -> int:
+        return 12 * self.ctx.V
+
+    def mult_eo(self, f):
+        return self._apply(OP_WILSON_HOP_EO, False, f)
+
+    def mult_oe(self, f):
+        return self._apply(OP_WILSON_HOP_OE, False, f)
+
+    def mult_eo_dag(self, f):  # Doe_.mult_dag (dirac_wilson_EvenOdd.hpp:70-73)
+        return self._apply(OP_WILSON_HOP_OE, True, f)
+
+    def mult_oe_dag(self, f):  # Deo_.mult_dag (dirac_wilson_EvenOdd.hpp:75-78)
+        return self._apply(OP_WILSON_HOP_EO, True, f)
+
+    def mult_ee(self, f):
+        return np.array(f, dtype=np.float64, copy=True)
+
+    mult_oo = mult_ee_inv = mult_oo_inv = mult_ee
+
+    def getDeo(self):
+        return Dirac_Wilson(self.mass, self.u, "EO", self.ctx, self.prec)
+
+    def getDoe(self):
+        return Dirac_Wilson(self.mass, self.u, "OE", self.ctx, self.prec)
+
+
+class Dirac_Clover(_Dirac):
+    """Dirac_Clover(Dw, csw, u): Wilson plus clover, full lattice
+    (lib/Dirac_ops/dirac_clover.hpp:57-69).  Unlike the reference it does not
+    take ownership of (or delete) Dw; it only reads its mass."""
+
+    op = OP_CLOVER_FULL
+
+    def __init__(self, Dw, csw, u, ctx=None, prec="double"):
+        super().__init__(Dw.getMass(), u, ctx or getattr(Dw, "ctx", None), prec)
+        self.csw = float(csw)
+        self.ctx.check(self.ctx._lib.iro_clover_setup(self.ctx.h, self.mass, self.csw),
+                       "iro_clover_setup")
+
+    def fsize(self) -> int:
+        return 24 * self.ctx.V
+
+    def update_internal_state(self):
+        super().update_internal_state()
+        self.ctx.check(self.ctx._lib.iro_clover_setup(self.ctx.h, self.mass, self.csw),
+                       "iro_clover_setup")
+
+
+class Dirac_Clover_EvenOdd(Dirac_Clover):
+    """The even-odd Schur complement of Dirac_Clover, A_ee - kappa^2 H_eo A_oo^-1 H_oe,
+    on even half fields.  The reference has no e/o clover operator."""
+
+    op = OP_CLOVER_SCHUR_EE
+
+    def __init__(self, mass, csw, u, ctx=None, prec="double"):
+        _Dirac.__init__(self, mass, u, ctx, prec)
+        self.csw = float(csw)
+        self.ctx.check(self.ctx._lib.iro_clover_setup(self.ctx.h, self.mass, self.csw),
+                       "iro_clover_setup")
+
+    def fsize(self) -> int:
+        return 12 * self.ctx.V
+
+
+class Fopr_DdagD:
+    """D^dagger D (lib/Fopr/fopr.h:146-153)."""
+
+    def __init__(self, D):
+        self.D = D
+
+    def mult(self, f):
+        return self.D.mult_dag(self.D.mult(f))
+
+    def mult_dag(self, f):
+        return self.mult(f)
+
+    def func(self, x):
+        return x
+
+    def fsize(self):
+        return self.D.fsize()
+
+
+# ---- solvers -----------------------------------------------------------------------
+
+@dataclass
+class SolverOutput:
+    """lib/Solver/solver.hpp:16-22."""
+
+    diff: float
+    Iterations: int
+    timing: float
+    Msg: str
+    reliable_updates: int = 0
+    operator_applies: int = 0
+
+    def print(self, Msg2: str = ""):
+        print(f" {self.Msg} {Msg2}\n  Iterations = {self.Iterations}\n  Residual   = "
+              f"{self.diff:.6e}\n  Timing     = {self.timing:.3f} ms")
+
+
+_SOLVER_OPS = (OP_WILSON_FULL, OP_WILSON_SCHUR_EE, OP_CLOVER_FULL, OP_CLOVER_SCHUR_EE)
+
+
+class Solver_CG:
+    """Solver_CG(prec, MaxIter, Fopr_DdagD(D)) (lib/Solver/solver_CG.hpp:28-31).
+
+    ``prec`` is the squared relative residual target (GoalPrecision).
+    ``inner`` selects the reference's FP64 CG ("double") or the reliable-update
+    mixed-precision CG with FP32 ("single") or FP16 ("half") inner storage."""
+
+    def __init__(self, prec: float, MaxIter: int, fopr: Fopr_DdagD, inner="double",
+                 delta: float = 0.1, use_graph: bool = True):
+        if not isinstance(fopr, Fopr_DdagD) or fopr.D.op not in _SOLVER_OPS:
+            raise IroError(BAD_ARG, "Solver_CG needs Fopr_DdagD of a full or Schur operator")
+        self.fopr = fopr
+        self.params = CGParams(float(prec), int(MaxIter), _PREC[inner], float(delta),
+                               int(bool(use_graph)))
+
+    def check_DdagD(self) -> bool:
+        return True
+
+    def solve_many(self, b: np.ndarray, nrhs: int):
+        """Solves nrhs right-hand sides together (one link load serves all).
+        Returns (x, [SolverOutput]) without raising on non-convergence."""
+        D = self.fopr.D
+        D.ctx.upload_gauge(D.u)
+        b = _f64(b, D.fsize() * nrhs, "source")
+        x = np.empty_like(b)
+        outs = (SolverOut * nrhs)()
+        rc = D.ctx._lib.iro_cg_solve(D.ctx.h, D.op, D.mass, D.csw, ctypes.byref(self.params),
+                                     _ptr(b), _ptr(x), nrhs, outs)
+        if rc not in (OK, NOT_CONVERGED):
+            D.ctx.check(rc, "iro_cg_solve")
+        res = [SolverOutput(o.diff, o.iterations, o.timing_ms, "CG solver", o.reliable_updates,
+                            o.operator_applies) for o in outs]
+        return x, res, rc
+
+    def solve(self, xq: np.ndarray, b: np.ndarray) -> SolverOutput:
+        """Solver_CG::solve(Field& xq, const Field& b) (solver_CG.cpp:29-80)."""
+        x, res, rc = self.solve_many(b, 1)
+        if rc == NOT_CONVERGED:
+            raise ConvergenceError(rc, "CG solver not converged")
+        xq[...] = x.reshape(xq.shape)
+        return res[0]
+
+
+class MultiShiftSolver_CG:
+    """MultiShiftSolver_CG(Fopr_DdagD(D), stop_cond, Niter)
+    (lib/Solver/multiShiftSolver_CG.hpp:61-65), FP64."""
+
+    def __init__(self, fopr: Fopr_DdagD, stop_cond: float, Niter: int):
+        if not isinstance(fopr, Fopr_DdagD) or fopr.D.op not in _SOLVER_OPS:
+            raise IroError(BAD_ARG, "MultiShiftSolver_CG needs Fopr_DdagD of a full or Schur operator")
+        self.fopr = fopr
+        self.prec = float(stop_cond)
+        self.niter = int(Niter)
+
+    def solve(self, xq: list, b: np.ndarray, shifts) -> SolverOutput:
+        """solve(vector_Field& x, const Field& b, const vector_double& shifts,
+        double& diff, int& Nconv) (multiShiftSolver_CG.cpp:95-185).  The
+        returned SolverOutput carries .diff and .Nconv; xq[i] are filled."""
+        D = self.fopr.D
+        D.ctx.upload_gauge(D.u)
+        n = D.fsize()
+        b = _f64(b, n, "source")
+        sh = _f64(shifts)
+        x = np.empty(n * sh.size)
+        o = SolverOut()
+        nconv = ctypes.c_int(-1)
+        rc = D.ctx._lib.iro_multishift_cg_solve(D.ctx.h, D.op, D.mass, D.csw, _ptr(b), sh.size,
+                                                _ptr(sh), _ptr(x), self.prec, self.niter,
+                                                ctypes.byref(o), ctypes.byref(nconv))
+        D.ctx.check(rc, "iro_multishift_cg_solve")
+        x = x.reshape(sh.size, n)
+        for i in range(sh.size):
+            if i < len(xq):
+                xq[i][...] = x[i]
+            else:
+                xq.append(x[i].copy())
+        out = SolverOutput(o.diff, o.iterations, o.timing_ms, "Multishift CG solver", 0,
+                           o.operator_applies)
+        out.Nconv = nconv.value
+        return out

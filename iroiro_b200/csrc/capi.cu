@@ -1,0 +1,656 @@
+// C ABI of the B200 fermion-solve library: contexts, resident gauge and
+// clover data, boundary conversion of host fields, operator composition and
+// the Krylov solvers.  See include/iroiro_b200.h for the contract of each
+// entry point and the reference interface it replaces.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "internal.h"
+#include "iroiro_b200.h"
+
+using namespace iro;
+
+struct iro_field {
+  iro_ctx* ctx;
+  DevField f;
+};
+
+struct iro_ctx {
+  int L[4];
+  Geom g;
+  int64_t V, Vh;
+  int device;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  int sms = 148;
+  int max_blocks = 148 * 8;
+
+  // gauge
+  bool has_gauge = false;
+  int recon = 12;
+  double* raw = nullptr;  // Format_G, FP64, on the device
+  GaugeArrays ga{};
+  unsigned long long* d_maxdev = nullptr;
+
+  // clover
+  bool has_clover = false;
+  double cl_kc = 0.0;  // kappa*csw the clover was built for
+  void* clA[3][2] = {};
+  void* clAinv[3][2] = {};
+  int* d_singular = nullptr;
+
+  // boundary staging
+  double* stage = nullptr;
+  size_t stage_bytes = 0;
+
+  // reduction scratch and solver state
+  double* partials = nullptr;
+  unsigned* counter = nullptr;
+  double* redout = nullptr;
+  void* state = nullptr;  // CGState[16] or MSState
+  int* done = nullptr;    // [16]
+  void* h_pinned = nullptr;  // host mirror of state + done
+
+  std::map<std::tuple<int, int, int, int>, DevField> ws;
+};
+
+namespace {
+
+constexpr int kMaxRhs = 16;
+constexpr size_t kPartialsPerBlock = 64;
+
+int fail(iro_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(iro_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, e == cudaErrorMemoryAllocation ? IRO_OUT_OF_MEMORY : IRO_CUDA_ERROR,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e__ = (call);                           \
+    if (e__ != cudaSuccess) return cuda_fail(c, e__, #call); \
+  } while (0)
+
+double kappa_of(double mass) { return 0.5 / (4.0 + mass); }
+
+int alloc_field(iro_ctx* c, int subset, int prec, int nrhs, DevField& f) {
+  f.subset = subset;
+  f.prec = prec;
+  f.nrhs = nrhs;
+  f.Vh = c->Vh;
+  const int np = subset == 2 ? 2 : 1;
+  f.bytes_data = size_t(np) * c->Vh * nrhs * spinor_nchunk(prec) * 16;
+  f.bytes_norm = prec == PREC_HALF ? size_t(np) * c->Vh * nrhs * sizeof(float) : 0;
+  f.data = nullptr;
+  f.norm = nullptr;
+  cudaError_t e = cudaMalloc(&f.data, f.bytes_data);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(field)");
+  if (f.bytes_norm) {
+    e = cudaMalloc(reinterpret_cast<void**>(&f.norm), f.bytes_norm);
+    if (e != cudaSuccess) {
+      cudaFree(f.data);
+      return cuda_fail(c, e, "cudaMalloc(norm)");
+    }
+  }
+  return IRO_OK;
+}
+
+void free_field(DevField& f) {
+  if (f.data) cudaFree(f.data);
+  if (f.norm) cudaFree(f.norm);
+  f.data = nullptr;
+  f.norm = nullptr;
+}
+
+// workspace field (cached per subset, precision, nrhs and slot)
+DevField* ws(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc) {
+  auto key = std::make_tuple(subset, prec, nrhs, slot);
+  auto it = c->ws.find(key);
+  if (it != c->ws.end()) return &it->second;
+  DevField f;
+  *rc = alloc_field(c, subset, prec, nrhs, f);
+  if (*rc != IRO_OK) return nullptr;
+  return &(c->ws[key] = f);
+}
+
+int ensure_stage(iro_ctx* c, size_t bytes) {
+  if (c->stage_bytes >= bytes) return IRO_OK;
+  if (c->stage) cudaFree(c->stage);
+  c->stage = nullptr;
+  c->stage_bytes = 0;
+  CK(cudaMalloc(&c->stage, bytes));
+  c->stage_bytes = bytes;
+  return IRO_OK;
+}
+
+Reduce make_reduce(iro_ctx* c, int stage, int max_iter) {
+  Reduce r;
+  r.partials = c->partials;
+  r.counter = c->counter;
+  r.out = c->redout;
+  r.stage = stage;
+  r.state = c->state;
+  r.done = c->done;
+  r.max_iter = max_iter;
+  return r;
+}
+
+GaugePtr gauge_ptr(iro_ctx* c, int prec) {
+  GaugePtr g;
+  g.Vh = c->Vh;
+  g.b = nullptr;
+  if (prec == PREC_DOUBLE)
+    g.a = c->recon == 12 ? static_cast<const void*>(c->ga.d12) : static_cast<const void*>(c->ga.d18);
+  else if (prec == PREC_SINGLE)
+    g.a = c->ga.s12;
+  else {
+    g.a = c->ga.h12a;
+    g.b = c->ga.h12b;
+  }
+  return g;
+}
+
+bool is_clover(int op) {
+  return op == IRO_OP_CLOVER_FULL || op == IRO_OP_CLOVER_SCHUR_EE || op == IRO_OP_CLOVER_HOP_OE_INV;
+}
+bool is_full(int op) { return op == IRO_OP_WILSON_FULL || op == IRO_OP_CLOVER_FULL; }
+bool op_valid(int op) { return op >= IRO_OP_WILSON_FULL && op <= IRO_OP_CLOVER_HOP_OE_INV; }
+
+int input_subset(int op) {
+  switch (op) {
+    case IRO_OP_WILSON_HOP_EO: return 1;
+    case IRO_OP_WILSON_HOP_OE:
+    case IRO_OP_CLOVER_HOP_OE_INV: return 0;
+    case IRO_OP_WILSON_SCHUR_EE:
+    case IRO_OP_CLOVER_SCHUR_EE: return 0;
+    default: return 2;
+  }
+}
+int output_subset(int op) {
+  switch (op) {
+    case IRO_OP_WILSON_HOP_EO: return 0;
+    case IRO_OP_WILSON_HOP_OE:
+    case IRO_OP_CLOVER_HOP_OE_INV: return 1;
+    case IRO_OP_WILSON_SCHUR_EE:
+    case IRO_OP_CLOVER_SCHUR_EE: return 0;
+    default: return 2;
+  }
+}
+
+int clover_build(iro_ctx* c, double kc);
+
+int ensure_clover(iro_ctx* c, double mass, double csw) {
+  const double kc = kappa_of(mass) * csw;
+  if (c->has_clover && c->cl_kc == kc) return IRO_OK;
+  return clover_build(c, kc);
+}
+
+CloverPtr clover_ptr(iro_ctx* c, int prec, int p, bool inverse) {
+  CloverPtr cp;
+  cp.data = inverse ? c->clAinv[prec][p] : c->clA[prec][p];
+  cp.Vh = c->Vh;
+  return cp;
+}
+
+HopLaunch base_launch(iro_ctx* c, int prec, bool dag, int nrhs) {
+  HopLaunch L{};
+  L.g = c->g;
+  L.nparity = 1;
+  L.nrhs = nrhs;
+  L.gauge = gauge_ptr(c, prec);
+  L.recon = prec == PREC_DOUBLE ? c->recon : 12;
+  L.prec = prec;
+  L.dag = dag;
+  L.max_blocks = c->max_blocks;
+  L.skip = nullptr;
+  L.red_mask = 0;
+  return L;
+}
+
+// out = op(in) on device fields.  `red`/`red_mask`, when given, attach a
+// reduction to the last kernel of the operator (|out|^2, |xin|^2, (xin,out)),
+// and `skip` lets converged right-hand sides be left untouched.
+int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in,
+              DevField& out, const Reduce* red, int red_mask, const int* skip) {
+  if (!c->has_gauge) return fail(c, IRO_NO_GAUGE, "no gauge field uploaded");
+  if (!op_valid(op)) return fail(c, IRO_BAD_ARG, "unknown operator");
+  if (in.prec != out.prec || in.nrhs != out.nrhs)
+    return fail(c, IRO_BAD_ARG, "operator fields differ in precision or nrhs");
+  if ((in.subset != input_subset(op) && !(in.subset == 2 && input_subset(op) != 2)) ||
+      (out.subset != output_subset(op) && !(out.subset == 2 && output_subset(op) != 2)))
+    return fail(c, IRO_BAD_ARG, "field subset does not match the operator");
+  if (in.data == out.data) return fail(c, IRO_BAD_ARG, "in and out must differ");
+  const int prec = in.prec;
+  const int nrhs = in.nrhs;
+  if (prec != PREC_DOUBLE && c->recon != 12)
+    return fail(c, IRO_BAD_ARG, "single/half precision need an SU(3) gauge field");
+  if (is_clover(op)) {
+    int rc = ensure_clover(c, mass, csw);
+    if (rc) return rc;
+  }
+  const double k = kappa_of(mass);
+  HopLaunch L = base_launch(c, prec, dag, nrhs);
+  L.skip = skip;
+  cudaStream_t st = c->stream;
+  switch (op) {
+    case IRO_OP_WILSON_HOP_EO:
+    case IRO_OP_WILSON_HOP_OE: {
+      const int pout = op == IRO_OP_WILSON_HOP_EO ? 0 : 1;
+      L.p0 = pout;
+      L.in[0] = in.half(1 - pout);
+      L.out[0] = out.half(pout);
+      L.epi = EPI_SCALE;
+      L.scale = -k;
+      if (red) { L.red = *red; L.red_mask = red_mask; }
+      CK(launch_hop(L, st));
+    } break;
+    case IRO_OP_CLOVER_HOP_OE_INV: {
+      L.p0 = 1;
+      L.in[0] = in.half(0);
+      L.out[0] = out.half(1);
+      L.epi = EPI_SCALE_CLOV;
+      L.clov[0] = clover_ptr(c, prec, 1, true);
+      L.scale = -k;
+      if (red) { L.red = *red; L.red_mask = red_mask; }
+      CK(launch_hop(L, st));
+    } break;
+    case IRO_OP_WILSON_SCHUR_EE:
+    case IRO_OP_CLOVER_SCHUR_EE: {
+      int rc = IRO_OK;
+      DevField* t = ws(c, 1, prec, nrhs, 0, &rc);
+      if (!t) return rc;
+      const bool cl = op == IRO_OP_CLOVER_SCHUR_EE;
+      // t_o = [A_oo^-1] (-kappa H_oe f_e)
+      L.p0 = 1;
+      L.in[0] = in.half(0);
+      L.out[0] = t->half(1);
+      L.epi = cl ? EPI_SCALE_CLOV : EPI_SCALE;
+      if (cl) L.clov[0] = clover_ptr(c, prec, 1, true);
+      L.scale = -k;
+      CK(launch_hop(L, st));
+      // out_e = [A_ee] f_e + kappa H_eo t_o  =  f - Deo(Doe f)
+      HopLaunch L2 = base_launch(c, prec, dag, nrhs);
+      L2.skip = skip;
+      L2.p0 = 0;
+      L2.in[0] = t->half(1);
+      L2.out[0] = out.half(0);
+      L2.xin[0] = in.half(0);
+      L2.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
+      if (cl) L2.clov[0] = clover_ptr(c, prec, 0, false);
+      L2.scale = k;
+      if (red) { L2.red = *red; L2.red_mask = red_mask; }
+      CK(launch_hop(L2, st));
+    } break;
+    case IRO_OP_WILSON_FULL:
+    case IRO_OP_CLOVER_FULL: {
+      const bool cl = op == IRO_OP_CLOVER_FULL;
+      L.p0 = 0;
+      L.nparity = 2;
+      for (int y = 0; y < 2; ++y) {
+        L.in[y] = in.half(1 - y);
+        L.out[y] = out.half(y);
+        L.xin[y] = in.half(y);
+        if (cl) L.clov[y] = clover_ptr(c, prec, y, false);
+      }
+      L.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
+      L.scale = -k;
+      if (red) { L.red = *red; L.red_mask = red_mask; }
+      CK(launch_hop(L, st));
+    } break;
+  }
+  return IRO_OK;
+}
+
+int clover_build(iro_ctx* c, double kc) {
+  if (!c->has_gauge) return fail(c, IRO_NO_GAUGE, "no gauge field uploaded");
+  if (!c->clA[0][0]) {
+    const size_t bytes[3] = {size_t(36) * 16, size_t(18) * 16, size_t(9) * 16};
+    for (int pr = 0; pr < 3; ++pr)
+      for (int p = 0; p < 2; ++p) {
+        CK(cudaMalloc(&c->clA[pr][p], bytes[pr] * c->Vh));
+        CK(cudaMalloc(&c->clAinv[pr][p], bytes[pr] * c->Vh));
+      }
+  }
+  CloverArrays ca;
+  for (int pr = 0; pr < 3; ++pr)
+    for (int p = 0; p < 2; ++p) {
+      ca.A[pr][p] = c->clA[pr][p];
+      ca.Ainv[pr][p] = c->clAinv[pr][p];
+    }
+  CK(cudaMemsetAsync(c->d_singular, 0, sizeof(int), c->stream));
+  CK(launch_clover_build(c->g, c->raw, kc, ca, c->d_singular, c->stream));
+  int singular = 0;
+  CK(cudaMemcpyAsync(&singular, c->d_singular, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (singular) return fail(c, IRO_BAD_ARG, "clover block not invertible");
+  c->has_clover = true;
+  c->cl_kc = kc;
+  return IRO_OK;
+}
+
+// host Format_F (nrhs fields) -> device field
+int import_host(iro_ctx* c, const double* host, int host_layout_full, DevField& f) {
+  const int64_t host_sites = host_layout_full ? c->V : c->Vh;
+  const size_t bytes = size_t(host_sites) * 24 * sizeof(double) * f.nrhs;
+  int rc = ensure_stage(c, bytes);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->stage, host, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (f.subset == 2) {
+    for (int p = 0; p < 2; ++p)
+      CK(launch_import_spinor(c->g, c->stage, 0, p, host_sites, f.nrhs, f.prec, f.half(p), c->stream));
+  } else {
+    CK(launch_import_spinor(c->g, c->stage, host_layout_full ? 0 : 1, f.subset, host_sites, f.nrhs,
+                            f.prec, f.half(f.subset), c->stream));
+  }
+  return IRO_OK;
+}
+
+int export_host(iro_ctx* c, const DevField& f, int host_layout_full, double* host) {
+  const int64_t host_sites = host_layout_full ? c->V : c->Vh;
+  const size_t bytes = size_t(host_sites) * 24 * sizeof(double) * f.nrhs;
+  int rc = ensure_stage(c, bytes);
+  if (rc) return rc;
+  if (f.subset == 2) {
+    for (int p = 0; p < 2; ++p)
+      CK(launch_export_spinor(c->g, c->stage, 0, p, host_sites, f.nrhs, f.prec, f.half(p), c->stream));
+  } else {
+    CK(launch_export_spinor(c->g, c->stage, host_layout_full ? 0 : 1, f.subset, host_sites, f.nrhs,
+                            f.prec, f.half(f.subset), c->stream));
+  }
+  CK(cudaMemcpyAsync(host, c->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return IRO_OK;
+}
+
+// sum |v|^2 per rhs (and |w|^2) into host arrays
+int norms_host(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
+               std::vector<double>* nw) {
+  Reduce r = make_reduce(c, ST_NONE, 0);
+  nv.assign(v.nrhs, 0.0);
+  if (nw) nw->assign(v.nrhs, 0.0);
+  std::vector<double> tmp(2 * v.nrhs);
+  SpinorPtr wp;
+  if (w) wp = w->all();
+  CK(launch_norms(v.prec, v.sites(), v.nrhs, v.all(), w ? &wp : nullptr, r, c->max_blocks, c->stream));
+  CK(cudaMemcpyAsync(tmp.data(), c->redout, sizeof(double) * 2 * v.nrhs, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < v.nrhs; ++k) {
+    nv[k] = tmp[k];
+    if (nw) (*nw)[k] = tmp[v.nrhs + k];
+  }
+  return IRO_OK;
+}
+
+// v = a x + b y over the whole field
+int axpby_dev(iro_ctx* c, double a, const DevField& x, double b, const DevField& y, DevField& v) {
+  CK(launch_axpby(v.prec, v.sites(), v.nrhs, a, x.all(), b, y.all(), v.all(), c->stream));
+  return IRO_OK;
+}
+
+int convert_dev(iro_ctx* c, const DevField& in, DevField& out) {
+  CK(launch_convert(in.prec, in.all(), out.prec, out.all(), out.sites(), out.nrhs, c->stream));
+  return IRO_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+int iro_ctx_create(const int L[4], int device, iro_ctx** out) {
+  if (!out || !L) return IRO_BAD_ARG;
+  *out = nullptr;
+  for (int d = 0; d < 4; ++d)
+    if (L[d] < 2 || (L[d] & 1)) return IRO_BAD_ARG;
+  const int64_t V = int64_t(L[0]) * L[1] * L[2] * L[3];
+  if (V / 2 > int64_t(1) << 30) return IRO_BAD_ARG;
+  std::unique_ptr<iro_ctx> c(new iro_ctx());
+  for (int d = 0; d < 4; ++d) c->L[d] = L[d];
+  c->V = V;
+  c->Vh = V / 2;
+  c->g.L[0] = L[0]; c->g.L[1] = L[1]; c->g.L[2] = L[2]; c->g.L[3] = L[3];
+  c->g.Lxh = L[0] / 2;
+  c->g.Vh = int(c->Vh);
+  c->g.sy = c->g.Lxh;
+  c->g.sz = c->g.Lxh * L[1];
+  c->g.st = c->g.Lxh * L[1] * L[2];
+  c->device = device;
+  iro_ctx* cp = c.get();
+  {
+    iro_ctx* c = cp;
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    c->sms = prop.multiProcessorCount;
+    c->max_blocks = c->sms * 8;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+    CK(cudaMalloc(&c->partials, sizeof(double) * kPartialsPerBlock * c->max_blocks * 2));
+    CK(cudaMalloc(&c->counter, sizeof(unsigned)));
+    CK(cudaMemset(c->counter, 0, sizeof(unsigned)));
+    CK(cudaMalloc(&c->redout, sizeof(double) * kPartialsPerBlock));
+    CK(cudaMalloc(&c->state, sizeof(MSState) > sizeof(CGState) * kMaxRhs ? sizeof(MSState) : sizeof(CGState) * kMaxRhs));
+    CK(cudaMalloc(&c->done, sizeof(int) * 64));
+    CK(cudaMemset(c->done, 0, sizeof(int) * 64));
+    CK(cudaMallocHost(&c->h_pinned, 4096 + sizeof(MSState)));
+    CK(cudaMalloc(&c->d_maxdev, sizeof(unsigned long long)));
+    CK(cudaMalloc(&c->d_singular, sizeof(int)));
+    clover_init_tables();
+    CK(cudaGetLastError());
+  }
+  *out = c.release();
+  return IRO_OK;
+}
+
+int iro_ctx_destroy(iro_ctx* c) {
+  if (!c) return IRO_BAD_ARG;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->ws) free_field(kv.second);
+  void* ptrs[] = {c->raw, c->ga.d12, c->ga.d18, c->ga.s12, c->ga.h12a, c->ga.h12b, c->d_maxdev,
+                  c->d_singular, c->stage, c->partials, c->counter, c->redout, c->state, c->done};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int pr = 0; pr < 3; ++pr)
+    for (int p = 0; p < 2; ++p) {
+      if (c->clA[pr][p]) cudaFree(c->clA[pr][p]);
+      if (c->clAinv[pr][p]) cudaFree(c->clAinv[pr][p]);
+    }
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return IRO_OK;
+}
+
+const char* iro_last_error(const iro_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void* iro_ctx_get_stream(const iro_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int iro_ctx_set_stream(iro_ctx* c, void* stream) {
+  if (!c) return IRO_BAD_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->stream = static_cast<cudaStream_t>(stream);
+  c->own_stream = false;
+  return IRO_OK;
+}
+
+int iro_gauge_upload(iro_ctx* c, const double* u) {
+  if (!c || !u) return fail(c, IRO_BAD_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  const size_t raw_bytes = size_t(18) * 4 * c->V * sizeof(double);
+  if (!c->raw) {
+    CK(cudaMalloc(&c->raw, raw_bytes));
+    CK(cudaMalloc(&c->ga.d12, size_t(2) * 4 * 6 * c->Vh * sizeof(double2)));
+    CK(cudaMalloc(&c->ga.d18, size_t(2) * 4 * 9 * c->Vh * sizeof(double2)));
+    CK(cudaMalloc(&c->ga.s12, size_t(2) * 4 * 3 * c->Vh * sizeof(float4)));
+    CK(cudaMalloc(&c->ga.h12a, size_t(2) * 4 * c->Vh * sizeof(uint4)));
+    CK(cudaMalloc(&c->ga.h12b, size_t(2) * 4 * c->Vh * sizeof(uint2)));
+  }
+  CK(cudaMemcpyAsync(c->raw, u, raw_bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_maxdev, 0, sizeof(unsigned long long), c->stream));
+  CK(launch_import_gauge(c->g, c->raw, c->ga, c->d_maxdev, c->stream));
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_maxdev, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double dev;
+  std::memcpy(&dev, &bits, sizeof(dev));
+  c->recon = (dev <= 1e-12) ? 12 : 18;
+  c->has_gauge = true;
+  c->has_clover = false;
+  return IRO_OK;
+}
+
+int iro_clover_setup(iro_ctx* c, double mass, double csw) {
+  if (!c) return IRO_BAD_ARG;
+  CK(cudaSetDevice(c->device));
+  return clover_build(c, kappa_of(mass) * csw);
+}
+
+int iro_field_strength(iro_ctx* c, int mu, int nu, double* out) {
+  if (!c || !out || mu < 0 || mu > 3 || nu < 0 || nu > 3 || mu == nu)
+    return fail(c, IRO_BAD_ARG, "bad field-strength arguments");
+  if (!c->has_gauge) return fail(c, IRO_NO_GAUGE, "no gauge field uploaded");
+  CK(cudaSetDevice(c->device));
+  const size_t bytes = size_t(18) * c->V * sizeof(double);
+  int rc = ensure_stage(c, bytes);
+  if (rc) return rc;
+  CK(launch_field_strength(c->g, c->raw, mu, nu, c->stage, c->stream));
+  CK(cudaMemcpyAsync(out, c->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return IRO_OK;
+}
+
+int iro_dirac_apply(iro_ctx* c, int op, double mass, double csw, int dagger, int prec,
+                    const double* in, double* out, int nrhs) {
+  if (!c || !in || !out || nrhs < 1 || nrhs > kMaxRhs || prec < 0 || prec > 2 || !op_valid(op))
+    return fail(c, IRO_BAD_ARG, "bad operator arguments");
+  CK(cudaSetDevice(c->device));
+  int rc = IRO_OK;
+  const int si = input_subset(op), so = output_subset(op);
+  DevField* fi = ws(c, si, prec, nrhs, 10, &rc);
+  if (!fi) return rc;
+  DevField* fo = ws(c, so, prec, nrhs, 11, &rc);
+  if (!fo) return rc;
+  rc = import_host(c, in, is_full(op), *fi);
+  if (rc) return rc;
+  rc = apply_dev(c, op, mass, csw, dagger != 0, *fi, *fo, nullptr, 0, nullptr);
+  if (rc) return rc;
+  return export_host(c, *fo, is_full(op), out);
+}
+
+int iro_gamma5(iro_ctx* c, const double* in, double* out, int64_t nsites) {
+  if (!c || !in || !out || nsites < 0) return fail(c, IRO_BAD_ARG, "bad gamma5 arguments");
+  CK(cudaSetDevice(c->device));
+  const size_t bytes = size_t(nsites) * 24 * sizeof(double);
+  int rc = ensure_stage(c, bytes);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->stage, in, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_gamma5_aos(c->stage, nsites, c->stream));
+  CK(cudaMemcpyAsync(out, c->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return IRO_OK;
+}
+
+int iro_field_create(iro_ctx* c, int subset, int prec, int nrhs, iro_field** f) {
+  if (!c || !f || subset < 0 || subset > 2 || prec < 0 || prec > 2 || nrhs < 1 || nrhs > kMaxRhs)
+    return fail(c, IRO_BAD_ARG, "bad field arguments");
+  CK(cudaSetDevice(c->device));
+  std::unique_ptr<iro_field> h(new iro_field());
+  h->ctx = c;
+  int rc = alloc_field(c, subset, prec, nrhs, h->f);
+  if (rc) return rc;
+  CK(cudaMemset(h->f.data, 0, h->f.bytes_data));
+  if (h->f.norm) CK(cudaMemset(h->f.norm, 0, h->f.bytes_norm));
+  *f = h.release();
+  return IRO_OK;
+}
+
+int iro_field_destroy(iro_field* f) {
+  if (!f) return IRO_BAD_ARG;
+  cudaSetDevice(f->ctx->device);
+  free_field(f->f);
+  delete f;
+  return IRO_OK;
+}
+
+int iro_field_upload(iro_ctx* c, iro_field* f, const double* host) {
+  if (!c || !f || !host) return fail(c, IRO_BAD_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  return import_host(c, host, f->f.subset == 2, f->f);
+}
+
+int iro_field_download(iro_ctx* c, const iro_field* f, double* host) {
+  if (!c || !f || !host) return fail(c, IRO_BAD_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  return export_host(c, f->f, f->f.subset == 2, host);
+}
+
+int iro_dirac_apply_field(iro_ctx* c, int op, double mass, double csw, int dagger,
+                          const iro_field* in, iro_field* out) {
+  if (!c || !in || !out) return fail(c, IRO_BAD_ARG, "null argument");
+  return apply_dev(c, op, mass, csw, dagger != 0, in->f, out->f, nullptr, 0, nullptr);
+}
+
+// ---- CG ------------------------------------------------------------------------------
+int iro_cg_solve(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+                 const double* b, double* x, int nrhs, iro_solver_out* out);
+
+int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double csw, const double* b,
+                            int nshift, const double* shifts, double* x, double precision,
+                            int max_iter, iro_solver_out* out, int* nconv);
+
+}  // extern "C"
+
+// The solvers live in solvers.cu; these helpers are shared with it.
+namespace iro {
+namespace host {
+int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in, DevField& out,
+          const Reduce* red, int red_mask, const int* skip) {
+  return apply_dev(c, op, mass, csw, dag, in, out, red, red_mask, skip);
+}
+DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc) {
+  return ws(c, subset, prec, nrhs, slot, rc);
+}
+int import_field(iro_ctx* c, const double* host, bool full, DevField& f) {
+  return import_host(c, host, full ? 1 : 0, f);
+}
+int export_field(iro_ctx* c, const DevField& f, bool full, double* host) {
+  return export_host(c, f, full ? 1 : 0, host);
+}
+int norms(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
+          std::vector<double>* nw) {
+  return norms_host(c, v, w, nv, nw);
+}
+int axpby(iro_ctx* c, double a, const DevField& x, double b, const DevField& y, DevField& v) {
+  return axpby_dev(c, a, x, b, y, v);
+}
+int convert(iro_ctx* c, const DevField& in, DevField& out) { return convert_dev(c, in, out); }
+Reduce reduce(iro_ctx* c, int stage, int max_iter) { return make_reduce(c, stage, max_iter); }
+int set_error(iro_ctx* c, int code, const std::string& msg) { return fail(c, code, msg); }
+int cuda_error(iro_ctx* c, cudaError_t e, const char* where) { return cuda_fail(c, e, where); }
+cudaStream_t stream(iro_ctx* c) { return c->stream; }
+int max_blocks(iro_ctx* c) { return c->max_blocks; }
+int64_t vh(iro_ctx* c) { return c->Vh; }
+void* state(iro_ctx* c) { return c->state; }
+int* done(iro_ctx* c) { return c->done; }
+void* pinned(iro_ctx* c) { return c->h_pinned; }
+int device(iro_ctx* c) { return c->device; }
+bool op_is_full(int op) { return is_full(op); }
+int op_subset(int op) { return input_subset(op); }
+bool op_ok(int op) { return op_valid(op); }
+}  // namespace host
+}  // namespace iro

@@ -1,0 +1,208 @@
+// The Wilson(-clover) hopping stencil for sm_100a.
+//
+// One thread computes one output site of one right-hand side:
+//   acc = sum_mu (1 - g_mu) U_mu(x) psi(x+mu) + (1 + g_mu) U_mu(x-mu)^dag psi(x-mu)
+// in the direction order x+,x-,y+,y-,z+,z-,t+,t- of Dirac_Wilson::mult_offdiag
+// (lib/Dirac_ops/dirac_wilson.cpp:107-113), with each neighbour first
+// projected to a half spinor (two colour vectors), multiplied by the link and
+// reconstructed, as the reference's improved kernel does per direction
+// (lib/Dirac_ops/dirac_wilson_improved.code:5-648).  The dagger operator
+// gamma5 D gamma5 (dirac_wilson.cpp:34-36) is the same stencil with the two
+// projectors exchanged, since gamma5 (1 -+ g_mu) gamma5 = (1 +- g_mu).
+//
+// The epilogue fuses what follows the stencil in the reference's operators:
+// the -kappa scale, the identity/clover diagonal term (f - kappa H f, or
+// A f - kappa H f), the clover inverse of the Schur complement, and the
+// FP64 norm/dot reductions a Krylov solver needs next.  Reductions are
+// deterministic: a fixed tree inside each block, per-block partials in global
+// scratch, and the last block to finish (ticket counter) summing the partials
+// in block order and running the solver's scalar update.
+#pragma once
+
+#include "common.cuh"
+#include "solver_scalars.cuh"
+
+namespace iro {
+
+// projector (1 - S*gamma_mu) applied to psi -> half spinor h[0..2]=h0, h[3..5]=h1
+// gamma matrices of GammaMatrix (lib/Dirac_ops/wilsonLikeUtils.cpp:9-40).
+template <int MU, int S, typename R>
+__device__ __forceinline__ void project(const Cx<R> f[12], Cx<R> h[6]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const Cx<R> f0 = f[c], f1 = f[3 + c], f2 = f[6 + c], f3 = f[9 + c];
+    if (MU == 0) {  // h0 = f0 + S i f3, h1 = f1 + S i f2
+      h[c] = (S > 0) ? f0 + mul_i(f3) : f0 - mul_i(f3);
+      h[3 + c] = (S > 0) ? f1 + mul_i(f2) : f1 - mul_i(f2);
+    } else if (MU == 1) {  // h0 = f0 + S f3, h1 = f1 - S f2
+      h[c] = (S > 0) ? f0 + f3 : f0 - f3;
+      h[3 + c] = (S > 0) ? f1 - f2 : f1 + f2;
+    } else if (MU == 2) {  // h0 = f0 + S i f2, h1 = f1 - S i f3
+      h[c] = (S > 0) ? f0 + mul_i(f2) : f0 - mul_i(f2);
+      h[3 + c] = (S > 0) ? f1 - mul_i(f3) : f1 + mul_i(f3);
+    } else {  // t: S=+1 keeps 2*f2, 2*f3; S=-1 keeps 2*f0, 2*f1
+      h[c] = (S > 0) ? R(2) * f2 : R(2) * f0;
+      h[3 + c] = (S > 0) ? R(2) * f3 : R(2) * f1;
+    }
+  }
+}
+
+// acc += (1 - S*gamma_mu) reconstructed from the multiplied half spinor g
+template <int MU, int S, typename R>
+__device__ __forceinline__ void reconstruct(Cx<R> acc[12], const Cx<R> g[6]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const Cx<R> g0 = g[c], g1 = g[3 + c];
+    if (MU == 3) {
+      if (S > 0) {
+        acc[6 + c] = acc[6 + c] + g0;
+        acc[9 + c] = acc[9 + c] + g1;
+      } else {
+        acc[c] = acc[c] + g0;
+        acc[3 + c] = acc[3 + c] + g1;
+      }
+      continue;
+    }
+    acc[c] = acc[c] + g0;
+    acc[3 + c] = acc[3 + c] + g1;
+    if (MU == 0) {  // [h0, h1, -S i h1, -S i h0]
+      acc[6 + c] = (S > 0) ? acc[6 + c] + mul_mi(g1) : acc[6 + c] + mul_i(g1);
+      acc[9 + c] = (S > 0) ? acc[9 + c] + mul_mi(g0) : acc[9 + c] + mul_i(g0);
+    } else if (MU == 1) {  // [h0, h1, -S h1, S h0]
+      acc[6 + c] = (S > 0) ? acc[6 + c] - g1 : acc[6 + c] + g1;
+      acc[9 + c] = (S > 0) ? acc[9 + c] + g0 : acc[9 + c] - g0;
+    } else {  // MU==2: [h0, h1, -S i h0, S i h1]
+      acc[6 + c] = (S > 0) ? acc[6 + c] + mul_mi(g0) : acc[6 + c] + mul_i(g0);
+      acc[9 + c] = (S > 0) ? acc[9 + c] + mul_i(g1) : acc[9 + c] + mul_mi(g1);
+    }
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void su3_mul(const Su3<R>& U, const Cx<R> h[6], Cx<R> g[6]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    g[a] = U.e[a][0] * h[0] + U.e[a][1] * h[1] + U.e[a][2] * h[2];
+    g[3 + a] = U.e[a][0] * h[3] + U.e[a][1] * h[4] + U.e[a][2] * h[5];
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void su3_dag_mul(const Su3<R>& U, const Cx<R> h[6], Cx<R> g[6]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    g[a] = cj_mul(U.e[0][a], h[0]) + cj_mul(U.e[1][a], h[1]) + cj_mul(U.e[2][a], h[2]);
+    g[3 + a] = cj_mul(U.e[0][a], h[3]) + cj_mul(U.e[1][a], h[4]) + cj_mul(U.e[2][a], h[5]);
+  }
+}
+
+// Forward (x+mu) and backward (x-mu) contributions of direction MU.
+template <int MU, bool DAG, int SP, int GP, int RECON>
+__device__ __forceinline__ void hop_dir(const GaugePtr& gauge, const SpinorPtr& in, int p,
+                                        int64_t hs, const int nb[8], int nrhs, int r,
+                                        Cx<typename SpinorIO<SP>::Real> acc[12]) {
+  using R = typename SpinorIO<SP>::Real;
+  Cx<R> f[12], h[6], g[6];
+  // forward: (1 - g_mu) U_mu(x) psi(x+mu)   [dagger: (1 + g_mu)]
+  {
+    Su3<R> U;
+    GaugeIO<GP, RECON>::load(gauge, p, MU, hs, U);
+    SpinorIO<SP>::load(in, int64_t(nb[2 * MU]) * nrhs + r, f);
+    constexpr int S = DAG ? -1 : 1;
+    project<MU, S, R>(f, h);
+    su3_mul(U, h, g);
+    reconstruct<MU, S, R>(acc, g);
+  }
+  // backward: (1 + g_mu) U_mu(x-mu)^dag psi(x-mu)   [dagger: (1 - g_mu)]
+  {
+    Su3<R> U;
+    GaugeIO<GP, RECON>::load(gauge, 1 - p, MU, nb[2 * MU + 1], U);
+    SpinorIO<SP>::load(in, int64_t(nb[2 * MU + 1]) * nrhs + r, f);
+    constexpr int S = DAG ? 1 : -1;
+    project<MU, S, R>(f, h);
+    su3_dag_mul(U, h, g);
+    reconstruct<MU, S, R>(acc, g);
+  }
+}
+
+struct HopParams {
+  Geom g;
+  int p0;  // parity of the output sites handled by blockIdx.y == 0
+  int nrhs;
+  SpinorPtr in[2], out[2], xin[2];  // indexed by blockIdx.y
+  GaugePtr gauge;
+  CloverPtr clov[2];
+  double scale;
+  int red_mask;
+  Reduce red;
+  const int* skip;  // per-rhs converged flags, or null
+};
+
+template <int SP, int GP, int RECON, bool DAG, int EPI, int CP>
+__global__ void __launch_bounds__(256) hop_kernel(HopParams P) {
+  using R = typename SpinorIO<SP>::Real;
+  const int yi = blockIdx.y;
+  const int p = P.p0 ^ yi;
+  const int nrhs = P.nrhs;
+  const int64_t nthreads = int64_t(P.g.Vh) * nrhs;
+  double red[3] = {0.0, 0.0, 0.0};
+  for (int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; tid < nthreads;
+       tid += int64_t(gridDim.x) * blockDim.x) {
+    const int hs = int(tid / nrhs);
+    const int r = int(tid - int64_t(hs) * nrhs);
+    if (P.skip && P.skip[r]) continue;
+    const Coord c = coord_of(P.g, hs, p);
+    int nb[8];
+    neighbours(P.g, c, hs, nb);
+    Cx<R> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = {R(0), R(0)};
+    hop_dir<0, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    hop_dir<1, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    hop_dir<2, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    hop_dir<3, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    const R sc = R(P.scale);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
+    if (EPI == EPI_SCALE_CLOV) {
+      CloverBlock<R> B[2];
+      CloverIO<CP>::load(P.clov[yi], hs, B);
+      clover_apply(B, acc);
+    }
+    Cx<R> xv[12];
+    if (EPI == EPI_XPAY || EPI == EPI_XPAY_CLOV) {
+      SpinorIO<SP>::load(P.xin[yi], tid, xv);
+      Cx<R> ax[12];
+#pragma unroll
+      for (int k = 0; k < 12; ++k) ax[k] = xv[k];
+      if (EPI == EPI_XPAY_CLOV) {
+        CloverBlock<R> B[2];
+        CloverIO<CP>::load(P.clov[yi], hs, B);
+        clover_apply(B, ax);
+      }
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = ax[k] + acc[k];
+    }
+    SpinorIO<SP>::store(P.out[yi], tid, acc);
+    if (P.red_mask) {
+      double o2 = 0.0, x2 = 0.0, xo = 0.0;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        const double ar = acc[k].re, ai = acc[k].im;
+        o2 += ar * ar + ai * ai;
+        if (EPI == EPI_XPAY || EPI == EPI_XPAY_CLOV) {
+          const double xr = xv[k].re, xi = xv[k].im;
+          x2 += xr * xr + xi * xi;
+          xo += xr * ar + xi * ai;
+        }
+      }
+      red[0] += o2;
+      red[1] += x2;
+      red[2] += xo;
+    }
+  }
+  if (P.red_mask) block_reduce_finish<3>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,
+                                         gridDim.x * gridDim.y);
+}
+
+}  // namespace iro

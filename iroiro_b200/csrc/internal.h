@@ -1,0 +1,136 @@
+// Host-side interface between the C ABI layer and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "solver_scalars.cuh"
+
+namespace iro {
+
+// A device spinor field of one parity (or both, for full-lattice fields: the
+// even half followed by the odd half), nrhs right-hand sides.
+struct DevField {
+  int subset;  // 0 even, 1 odd, 2 full
+  int prec;
+  int nrhs;
+  int64_t Vh;
+  void* data;   // chunks
+  float* norm;  // FP16 norms
+  size_t bytes_data, bytes_norm;
+  // pointer to the half of parity p (p must be contained in the subset)
+  SpinorPtr half(int p) const;
+  // the whole field as one vector of sites() sites
+  SpinorPtr all() const;
+  int64_t sites() const { return (subset == 2 ? 2 : 1) * Vh; }
+};
+
+int spinor_chunk_bytes(int prec);  // bytes of one chunk element
+int spinor_nchunk(int prec);
+
+struct LaunchCfg {
+  int block;  // nrhs * 2^k, at most 256
+  int grid;
+};
+LaunchCfg launch_cfg(int64_t vh, int nrhs, int max_blocks);
+
+// ---- stencil ---------------------------------------------------------------
+struct HopLaunch {
+  Geom g;
+  int p0;     // output parity of grid row 0
+  int nparity;  // 1 or 2 (both parities in one launch)
+  int nrhs;
+  SpinorPtr in[2], out[2], xin[2];
+  GaugePtr gauge;
+  int recon;
+  CloverPtr clov[2];
+  int prec;
+  bool dag;
+  int epi;
+  double scale;
+  int red_mask;
+  Reduce red;
+  const int* skip;
+  int max_blocks;
+};
+cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st);
+
+// ---- linear algebra on fields ------------------------------------------------
+// v = a*x + b*y for nrhs fields of one parity (scalars uniform)
+cudaError_t launch_axpby(int prec, int64_t Vh, int nrhs, double a, SpinorPtr x, double b,
+                         SpinorPtr y, SpinorPtr v, cudaStream_t st);
+// precision conversion of one parity
+cudaError_t launch_convert(int pin, SpinorPtr in, int pout, SpinorPtr out, int64_t Vh, int nrhs,
+                           cudaStream_t st);
+// sum |v|^2 (k=0) and, if w given, |w|^2 (k=1) per rhs with a stage update
+cudaError_t launch_norms(int prec, int64_t Vh, int nrhs, SpinorPtr v, const SpinorPtr* w,
+                         const Reduce& red, int max_blocks, cudaStream_t st);
+// CG: r = b - s, p = r; reduce |r|^2, |b|^2 (stage ST_CG_INIT)
+cudaError_t launch_cg_init(int prec, int64_t Vh, int nrhs, SpinorPtr b, SpinorPtr s, SpinorPtr r,
+                           SpinorPtr p, const Reduce& red, int max_blocks, cudaStream_t st);
+// CG: x += alpha p; r -= alpha s; reduce |r|^2 (stage ST_CG_BETA)
+cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr r, SpinorPtr p,
+                         SpinorPtr s, const CGState* state, const Reduce& red, int max_blocks,
+                         cudaStream_t st);
+// CG: p = beta p + r
+cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r,
+                        const CGState* state, const int* done, cudaStream_t st);
+
+// Multishift (FP64): x0 -= beta p0; r += beta (s + sigma0 p0); reduce |r|^2
+cudaError_t launch_ms_xr(int64_t Vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
+                         const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st);
+// p0 = alpha p0 + r; x_k -= betas_k p_k; p_k = alphas_k p_k + zeta_k r; reduce |p_k|^2
+struct MSFields {
+  SpinorPtr x[MAXSHIFT], p[MAXSHIFT];
+};
+cudaError_t launch_ms_p(int64_t Vh, int nshift, const MSFields& f, SpinorPtr r, const MSState* m,
+                        const Reduce& red, int max_blocks, cudaStream_t st);
+
+// ---- mixed precision (reliable updates), masked by mask[rhs] != 0 ----------------
+cudaError_t launch_mx_merge(int plo, int64_t sites, int nrhs, SpinorPtr x64, SpinorPtr xlo,
+                            const int* mask, cudaStream_t st);
+cudaError_t launch_mx_residual(int plo, int64_t sites, int nrhs, SpinorPtr b, SpinorPtr s64,
+                               SpinorPtr r64, SpinorPtr rlo, const int* mask, const Reduce& red,
+                               int max_blocks, cudaStream_t st);
+cudaError_t launch_mx_p(int plo, int64_t sites, int nrhs, SpinorPtr p, SpinorPtr r,
+                        const CGState* state, const int* mask, cudaStream_t st);
+
+// ---- boundary conversion ---------------------------------------------------------
+// host Format_F doubles (already on the device in `stage`) <-> device field.
+// layout 0: full lexicographic lattice; 1: half field of parity p (hs order).
+// nrhs consecutive host fields of `host_sites` sites each.
+cudaError_t launch_import_spinor(const Geom& g, const double* stage, int layout, int p,
+                                 int64_t host_sites, int nrhs, int prec, SpinorPtr out,
+                                 cudaStream_t st);
+cudaError_t launch_export_spinor(const Geom& g, double* stage, int layout, int p,
+                                 int64_t host_sites, int nrhs, int prec, SpinorPtr in,
+                                 cudaStream_t st);
+// gamma5 on a Format_F staging buffer in place
+cudaError_t launch_gamma5_aos(double* stage, int64_t nsites, cudaStream_t st);
+
+// Format_G doubles on the device -> link arrays.  Also returns (in *maxdev)
+// the largest deviation of row 2 from conj(row0 x row1) and of the first two
+// rows from orthonormality.
+struct GaugeArrays {
+  double2* d12;  // [2][4][6][Vh]
+  double2* d18;  // [2][4][9][Vh]
+  float4* s12;   // [2][4][3][Vh]
+  uint4* h12a;   // [2][4][Vh]
+  uint2* h12b;   // [2][4][Vh]
+};
+cudaError_t launch_import_gauge(const Geom& g, const double* raw, GaugeArrays ga,
+                                unsigned long long* maxdev_bits, cudaStream_t st);
+
+// ---- clover ------------------------------------------------------------------------
+struct CloverArrays {
+  void* A[3][2];     // [prec][parity]
+  void* Ainv[3][2];
+};
+cudaError_t launch_clover_build(const Geom& g, const double* raw, double kappa_csw,
+                                CloverArrays ca, int* singular, cudaStream_t st);
+cudaError_t launch_field_strength(const Geom& g, const double* raw, int mu, int nu, double* out,
+                                  cudaStream_t st);
+void clover_init_tables();
+
+}  // namespace iro

@@ -1,0 +1,893 @@
+// Kernels of the B200 fermion-solve library other than the stencil body:
+// launch dispatch of the stencil, fused linear algebra of the solvers, the
+// boundary conversions between the reference's host layouts and the device
+// layouts, and the clover set-up.
+#include <cstring>
+
+#include "dslash.cuh"
+#include "internal.h"
+
+namespace iro {
+
+// ---- fields ------------------------------------------------------------------
+int spinor_chunk_bytes(int prec) { return 16; }
+int spinor_nchunk(int prec) {
+  return prec == PREC_DOUBLE ? 12 : (prec == PREC_SINGLE ? 6 : 3);
+}
+
+SpinorPtr DevField::half(int p) const {
+  // full fields interleave the parities inside each chunk: [chunk][p][Vh*nrhs]
+  SpinorPtr s;
+  const int64_t per = Vh * nrhs;
+  if (subset == 2) {
+    s.data = static_cast<char*>(data) + p * per * 16;
+    s.norm = norm ? norm + p * per : nullptr;
+    s.stride = 2 * per;
+  } else {
+    s.data = data;
+    s.norm = norm;
+    s.stride = per;
+  }
+  return s;
+}
+
+SpinorPtr DevField::all() const {
+  SpinorPtr s;
+  s.data = data;
+  s.norm = norm;
+  s.stride = (subset == 2 ? 2 : 1) * Vh * nrhs;
+  return s;
+}
+
+LaunchCfg launch_cfg(int64_t vh, int nrhs, int max_blocks) {
+  int spb = 1;
+  while (nrhs * spb * 2 <= 256) spb *= 2;
+  LaunchCfg c;
+  c.block = nrhs * spb;
+  int64_t need = (vh * nrhs + c.block - 1) / c.block;
+  c.grid = int(need < max_blocks ? need : max_blocks);
+  if (c.grid < 1) c.grid = 1;
+  return c;
+}
+
+// ---- stencil dispatch ------------------------------------------------------------
+// one translation unit per storage precision (dslash_{double,single,half}.cu)
+cudaError_t launch_hop_double(const HopLaunch& L, cudaStream_t st);
+cudaError_t launch_hop_single(const HopLaunch& L, cudaStream_t st);
+cudaError_t launch_hop_half(const HopLaunch& L, cudaStream_t st);
+
+cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st) {
+  switch (L.prec) {
+    case PREC_DOUBLE: return launch_hop_double(L, st);
+    case PREC_SINGLE: return launch_hop_single(L, st);
+    case PREC_HALF: return launch_hop_half(L, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// ---- linear algebra ------------------------------------------------------------
+template <typename RA, typename RB>
+__device__ __forceinline__ void cvt12(const Cx<RA> a[12], Cx<RB> b[12]) {
+#pragma unroll
+  for (int k = 0; k < 12; ++k) b[k] = {RB(a[k].re), RB(a[k].im)};
+}
+
+template <int SP>
+__global__ void axpby_kernel(int64_t n, double a, SpinorPtr x, double b, SpinorPtr y, SpinorPtr v) {
+  using R = typename SpinorIO<SP>::Real;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<R> xv[12], yv[12];
+    SpinorIO<SP>::load(x, i, xv);
+    if (b != 0.0) SpinorIO<SP>::load(y, i, yv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      xv[k] = R(a) * xv[k];
+      if (b != 0.0) xv[k] = xv[k] + R(b) * yv[k];
+    }
+    SpinorIO<SP>::store(v, i, xv);
+  }
+}
+
+cudaError_t launch_axpby(int prec, int64_t Vh, int nrhs, double a, SpinorPtr x, double b,
+                         SpinorPtr y, SpinorPtr v, cudaStream_t st) {
+  const int64_t n = Vh * nrhs;
+  const int blk = 256;
+  int grid = int((n + blk - 1) / blk);
+  if (grid > 148 * 16) grid = 148 * 16;
+  switch (prec) {
+    case PREC_DOUBLE: axpby_kernel<PREC_DOUBLE><<<grid, blk, 0, st>>>(n, a, x, b, y, v); break;
+    case PREC_SINGLE: axpby_kernel<PREC_SINGLE><<<grid, blk, 0, st>>>(n, a, x, b, y, v); break;
+    default: axpby_kernel<PREC_HALF><<<grid, blk, 0, st>>>(n, a, x, b, y, v); break;
+  }
+  return cudaGetLastError();
+}
+
+template <int PI, int PO>
+__global__ void convert_kernel(int64_t n, SpinorPtr in, SpinorPtr out) {
+  using RI = typename SpinorIO<PI>::Real;
+  using RO = typename SpinorIO<PO>::Real;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<RI> a[12];
+    Cx<RO> b[12];
+    SpinorIO<PI>::load(in, i, a);
+    cvt12(a, b);
+    SpinorIO<PO>::store(out, i, b);
+  }
+}
+
+cudaError_t launch_convert(int pin, SpinorPtr in, int pout, SpinorPtr out, int64_t Vh, int nrhs,
+                           cudaStream_t st) {
+  const int64_t n = Vh * nrhs;
+  const int blk = 256;
+  int grid = int((n + blk - 1) / blk);
+  if (grid > 148 * 16) grid = 148 * 16;
+#define IRO_CVT(A, B) \
+  if (pin == A && pout == B) { convert_kernel<A, B><<<grid, blk, 0, st>>>(n, in, out); return cudaGetLastError(); }
+  IRO_CVT(PREC_DOUBLE, PREC_DOUBLE)
+  IRO_CVT(PREC_DOUBLE, PREC_SINGLE)
+  IRO_CVT(PREC_DOUBLE, PREC_HALF)
+  IRO_CVT(PREC_SINGLE, PREC_DOUBLE)
+  IRO_CVT(PREC_SINGLE, PREC_SINGLE)
+  IRO_CVT(PREC_SINGLE, PREC_HALF)
+  IRO_CVT(PREC_HALF, PREC_DOUBLE)
+  IRO_CVT(PREC_HALF, PREC_SINGLE)
+  IRO_CVT(PREC_HALF, PREC_HALF)
+#undef IRO_CVT
+  return cudaErrorInvalidValue;
+}
+
+template <int SP, bool TWO>
+__global__ void __launch_bounds__(256) norms_kernel(int64_t vh, int nrhs, SpinorPtr v, SpinorPtr w, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
+  const int64_t n = vh * nrhs;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<R> a[12];
+    SpinorIO<SP>::load(v, i, a);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[0] += double(a[k].re) * a[k].re + double(a[k].im) * a[k].im;
+    if (TWO) {
+      SpinorIO<SP>::load(w, i, a);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[1] += double(a[k].re) * a[k].re + double(a[k].im) * a[k].im;
+    }
+  }
+  block_reduce_finish<2>(red, acc, nrhs, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_norms(int prec, int64_t Vh, int nrhs, SpinorPtr v, const SpinorPtr* w,
+                         const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, nrhs, max_blocks);
+  SpinorPtr ww = w ? *w : v;
+#define IRO_NORMS(P)                                                                          \
+  if (prec == P) {                                                                            \
+    if (w) norms_kernel<P, true><<<c.grid, c.block, 0, st>>>(Vh, nrhs, v, ww, red);            \
+    else norms_kernel<P, false><<<c.grid, c.block, 0, st>>>(Vh, nrhs, v, ww, red);             \
+    return cudaGetLastError();                                                                \
+  }
+  IRO_NORMS(PREC_DOUBLE)
+  IRO_NORMS(PREC_SINGLE)
+  IRO_NORMS(PREC_HALF)
+#undef IRO_NORMS
+  return cudaErrorInvalidValue;
+}
+
+// Solver_CG::solve start (solver_CG.cpp:40-47): r = b - A x, p = r, rr = (r,r)
+template <int SP>
+__global__ void __launch_bounds__(256) cg_init_kernel(int64_t vh, int nrhs, SpinorPtr b, SpinorPtr s, SpinorPtr r,
+                               SpinorPtr p, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
+  const int64_t n = vh * nrhs;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<R> bv[12], sv[12];
+    SpinorIO<SP>::load(b, i, bv);
+    SpinorIO<SP>::load(s, i, sv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      acc[1] += double(bv[k].re) * bv[k].re + double(bv[k].im) * bv[k].im;
+      sv[k] = bv[k] - sv[k];
+      acc[0] += double(sv[k].re) * sv[k].re + double(sv[k].im) * sv[k].im;
+    }
+    SpinorIO<SP>::store(r, i, sv);
+    SpinorIO<SP>::store(p, i, sv);
+  }
+  block_reduce_finish<2>(red, acc, nrhs, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_cg_init(int prec, int64_t Vh, int nrhs, SpinorPtr b, SpinorPtr s, SpinorPtr r,
+                           SpinorPtr p, const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, nrhs, max_blocks);
+  switch (prec) {
+    case PREC_DOUBLE: cg_init_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(Vh, nrhs, b, s, r, p, red); break;
+    case PREC_SINGLE: cg_init_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(Vh, nrhs, b, s, r, p, red); break;
+    default: cg_init_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(Vh, nrhs, b, s, r, p, red); break;
+  }
+  return cudaGetLastError();
+}
+
+// solve_step (solver_CG.cpp:131-147): x += cr p; r -= cr s; rr = (r,r)
+template <int SP>
+__global__ void __launch_bounds__(256) cg_xr_kernel(int64_t vh, int nrhs, SpinorPtr x, SpinorPtr r, SpinorPtr p,
+                             SpinorPtr s, const CGState* state, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
+  const int64_t n = vh * nrhs;
+  double acc = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int rhs = int(i % nrhs);
+    if (red.done[rhs]) continue;
+    const double a = state[rhs].alpha;
+    Cx<R> xv[12], rv[12], pv[12], sv[12];
+    SpinorIO<SP>::load(x, i, xv);
+    SpinorIO<SP>::load(r, i, rv);
+    SpinorIO<SP>::load(p, i, pv);
+    SpinorIO<SP>::load(s, i, sv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      xv[k] = xv[k] + R(a) * pv[k];
+      rv[k] = rv[k] - R(a) * sv[k];
+      acc += double(rv[k].re) * rv[k].re + double(rv[k].im) * rv[k].im;
+    }
+    SpinorIO<SP>::store(x, i, xv);
+    SpinorIO<SP>::store(r, i, rv);
+  }
+  block_reduce_finish<1>(red, &acc, nrhs, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr r, SpinorPtr p,
+                         SpinorPtr s, const CGState* state, const Reduce& red, int max_blocks,
+                         cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, nrhs, max_blocks);
+  switch (prec) {
+    case PREC_DOUBLE: cg_xr_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(Vh, nrhs, x, r, p, s, state, red); break;
+    case PREC_SINGLE: cg_xr_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(Vh, nrhs, x, r, p, s, state, red); break;
+    default: cg_xr_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(Vh, nrhs, x, r, p, s, state, red); break;
+  }
+  return cudaGetLastError();
+}
+
+// p = p*(rr/rrp) + r (solver_CG.cpp:150-153)
+template <int SP>
+__global__ void cg_p_kernel(int64_t vh, int nrhs, SpinorPtr p, SpinorPtr r, const CGState* state,
+                            const int* done) {
+  using R = typename SpinorIO<SP>::Real;
+  const int64_t n = vh * nrhs;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int rhs = int(i % nrhs);
+    if (done[rhs]) continue;
+    const double b = state[rhs].beta;
+    Cx<R> pv[12], rv[12];
+    SpinorIO<SP>::load(p, i, pv);
+    SpinorIO<SP>::load(r, i, rv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) pv[k] = R(b) * pv[k] + rv[k];
+    SpinorIO<SP>::store(p, i, pv);
+  }
+}
+
+cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r,
+                        const CGState* state, const int* done, cudaStream_t st) {
+  const int64_t n = Vh * nrhs;
+  const int blk = 256;
+  int grid = int((n + blk - 1) / blk);
+  if (grid > 148 * 16) grid = 148 * 16;
+  switch (prec) {
+    case PREC_DOUBLE: cg_p_kernel<PREC_DOUBLE><<<grid, blk, 0, st>>>(Vh, nrhs, p, r, state, done); break;
+    case PREC_SINGLE: cg_p_kernel<PREC_SINGLE><<<grid, blk, 0, st>>>(Vh, nrhs, p, r, state, done); break;
+    default: cg_p_kernel<PREC_HALF><<<grid, blk, 0, st>>>(Vh, nrhs, p, r, state, done); break;
+  }
+  return cudaGetLastError();
+}
+
+// ---- multishift (FP64) -------------------------------------------------------------
+// multiShiftSolver_CG.cpp:49-59: x0 -= beta p0; r += beta s, s = A p0 + sigma0 p0
+__global__ void __launch_bounds__(256) ms_xr_kernel(int64_t vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
+                             const MSState* m, Reduce red) {
+  double acc = 0.0;
+  if (!red.done[0]) {
+    const double beta = m->beta, s0 = m->sigma0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
+         i += int64_t(gridDim.x) * blockDim.x) {
+      Cx<double> xv[12], rv[12], pv[12], sv[12];
+      SpinorIO<PREC_DOUBLE>::load(x0, i, xv);
+      SpinorIO<PREC_DOUBLE>::load(r, i, rv);
+      SpinorIO<PREC_DOUBLE>::load(p0, i, pv);
+      SpinorIO<PREC_DOUBLE>::load(s, i, sv);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        sv[k] = sv[k] + s0 * pv[k];
+        xv[k] = xv[k] - beta * pv[k];
+        rv[k] = rv[k] + beta * sv[k];
+        acc += rv[k].re * rv[k].re + rv[k].im * rv[k].im;
+      }
+      SpinorIO<PREC_DOUBLE>::store(x0, i, xv);
+      SpinorIO<PREC_DOUBLE>::store(r, i, rv);
+    }
+  }
+  block_reduce_finish<1>(red, &acc, 1, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_ms_xr(int64_t Vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
+                         const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, 1, max_blocks);
+  ms_xr_kernel<<<c.grid, c.block, 0, st>>>(Vh, x0, r, p0, s, m, red);
+  return cudaGetLastError();
+}
+
+// multiShiftSolver_CG.cpp:61-83: all shifts' x and p updated in one pass
+__global__ void __launch_bounds__(256) ms_p_kernel(int64_t vh, MSFields f, SpinorPtr r, const MSState* m, Reduce red) {
+  double acc[MAXSHIFT];
+#pragma unroll
+  for (int k = 0; k < MAXSHIFT; ++k) acc[k] = 0.0;
+  if (!red.done[0]) {
+    const int ns2 = m->nshift2;
+    const double alpha = m->alpha;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
+         i += int64_t(gridDim.x) * blockDim.x) {
+      Cx<double> rv[12], pv[12], xv[12];
+      SpinorIO<PREC_DOUBLE>::load(r, i, rv);
+      SpinorIO<PREC_DOUBLE>::load(f.p[0], i, pv);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) pv[k] = alpha * pv[k] + rv[k];
+      SpinorIO<PREC_DOUBLE>::store(f.p[0], i, pv);
+#pragma unroll
+      for (int sh = 1; sh < MAXSHIFT; ++sh) {
+        if (sh >= ns2) break;
+        const double bs = m->betas[sh], as = m->alphas[sh], z = m->zeta[sh];
+        SpinorIO<PREC_DOUBLE>::load(f.p[sh], i, pv);
+        SpinorIO<PREC_DOUBLE>::load(f.x[sh], i, xv);
+        double a2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+          xv[k] = xv[k] - bs * pv[k];
+          pv[k] = as * pv[k] + z * rv[k];
+          a2 += pv[k].re * pv[k].re + pv[k].im * pv[k].im;
+        }
+        acc[sh] += a2;
+        SpinorIO<PREC_DOUBLE>::store(f.x[sh], i, xv);
+        SpinorIO<PREC_DOUBLE>::store(f.p[sh], i, pv);
+      }
+    }
+  }
+  block_reduce_finish<MAXSHIFT>(red, acc, 1, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_ms_p(int64_t Vh, int nshift, const MSFields& f, SpinorPtr r, const MSState* m,
+                        const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, 1, max_blocks);
+  ms_p_kernel<<<c.grid, c.block, 0, st>>>(Vh, f, r, m, red);
+  return cudaGetLastError();
+}
+
+// ---- boundary conversion ------------------------------------------------------------
+__device__ __forceinline__ int64_t host_site(const Geom& g, int layout, int p, int hs) {
+  if (layout == 1) return hs;
+  const Coord c = coord_of(g, hs, p);
+  return int64_t(c.x) + int64_t(g.L[0]) * c.row;
+}
+
+template <int SP>
+__global__ void import_kernel(Geom g, const double* stage, int layout, int p, int64_t host_sites,
+                              int nrhs, SpinorPtr out) {
+  using R = typename SpinorIO<SP>::Real;
+  const int64_t n = int64_t(g.Vh) * nrhs;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int hs = int(i / nrhs);
+    const int r = int(i - int64_t(hs) * nrhs);
+    const double* src = stage + (int64_t(r) * host_sites + host_site(g, layout, p, hs)) * 24;
+    Cx<R> v[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) v[k] = {R(src[2 * k]), R(src[2 * k + 1])};
+    SpinorIO<SP>::store(out, i, v);
+  }
+}
+
+template <int SP>
+__global__ void export_kernel(Geom g, double* stage, int layout, int p, int64_t host_sites,
+                              int nrhs, SpinorPtr in) {
+  using R = typename SpinorIO<SP>::Real;
+  const int64_t n = int64_t(g.Vh) * nrhs;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int hs = int(i / nrhs);
+    const int r = int(i - int64_t(hs) * nrhs);
+    double* dst = stage + (int64_t(r) * host_sites + host_site(g, layout, p, hs)) * 24;
+    Cx<R> v[12];
+    SpinorIO<SP>::load(in, i, v);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      dst[2 * k] = double(v[k].re);
+      dst[2 * k + 1] = double(v[k].im);
+    }
+  }
+}
+
+static int grid_for(int64_t n, int blk) {
+  int64_t g = (n + blk - 1) / blk;
+  return int(g > 148 * 32 ? 148 * 32 : (g < 1 ? 1 : g));
+}
+
+cudaError_t launch_import_spinor(const Geom& g, const double* stage, int layout, int p,
+                                 int64_t host_sites, int nrhs, int prec, SpinorPtr out,
+                                 cudaStream_t st) {
+  const int grid = grid_for(int64_t(g.Vh) * nrhs, 256);
+  switch (prec) {
+    case PREC_DOUBLE: import_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out); break;
+    case PREC_SINGLE: import_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out); break;
+    default: import_kernel<PREC_HALF><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_spinor(const Geom& g, double* stage, int layout, int p,
+                                 int64_t host_sites, int nrhs, int prec, SpinorPtr in,
+                                 cudaStream_t st) {
+  const int grid = grid_for(int64_t(g.Vh) * nrhs, 256);
+  switch (prec) {
+    case PREC_DOUBLE: export_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in); break;
+    case PREC_SINGLE: export_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in); break;
+    default: export_kernel<PREC_HALF><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in); break;
+  }
+  return cudaGetLastError();
+}
+
+// GammaMatrix::gamma5core (lib/Dirac_ops/wilsonLikeUtils.cpp:42-49): spins 0<->2, 1<->3
+__global__ void gamma5_aos_kernel(double* f, int64_t nsites) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nsites * 6;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t site = i / 6;
+    const int k = int(i - site * 6);  // complex k of spins 0,1 (k = c + 3*s)
+    double2* p = reinterpret_cast<double2*>(f + site * 24);
+    double2 a = p[k], b = p[k + 6];
+    p[k] = b;
+    p[k + 6] = a;
+  }
+}
+
+cudaError_t launch_gamma5_aos(double* stage, int64_t nsites, cudaStream_t st) {
+  gamma5_aos_kernel<<<grid_for(nsites * 6, 256), 256, 0, st>>>(stage, nsites);
+  return cudaGetLastError();
+}
+
+// ---- gauge import -------------------------------------------------------------------
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double v) {
+  atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+__global__ void import_gauge_kernel(Geom g, const double* raw, GaugeArrays ga,
+                                    unsigned long long* maxdev) {
+  const int64_t Vh = g.Vh;
+  const int64_t V = 2 * Vh;
+  const int64_t n = 2 * 4 * Vh;
+  double dev = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t hs = i % Vh;
+    const int mu = int((i / Vh) % 4);
+    const int p = int(i / (4 * Vh));
+    const Coord c = coord_of(g, int(hs), p);
+    const int64_t site = int64_t(c.x) + int64_t(g.L[0]) * c.row;
+    const double* u = raw + 18 * (site + V * mu);
+    Su3<double> U;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) U.e[a][b] = {u[2 * (3 * a + b)], u[2 * (3 * a + b) + 1]};
+    const int64_t base = int64_t(p * 4 + mu);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ga.d12[(base * 6 + k) * Vh + hs] = make_double2(U.e[k / 3][k % 3].re, U.e[k / 3][k % 3].im);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ga.d18[(base * 9 + k) * Vh + hs] = make_double2(U.e[k / 3][k % 3].re, U.e[k / 3][k % 3].im);
+    ga.s12[(base * 3 + 0) * Vh + hs] = make_float4(U.e[0][0].re, U.e[0][0].im, U.e[0][1].re, U.e[0][1].im);
+    ga.s12[(base * 3 + 1) * Vh + hs] = make_float4(U.e[0][2].re, U.e[0][2].im, U.e[1][0].re, U.e[1][0].im);
+    ga.s12[(base * 3 + 2) * Vh + hs] = make_float4(U.e[1][1].re, U.e[1][1].im, U.e[1][2].re, U.e[1][2].im);
+    uint4 ha;
+    ha.x = pack_h2(float(U.e[0][0].re), float(U.e[0][0].im));
+    ha.y = pack_h2(float(U.e[0][1].re), float(U.e[0][1].im));
+    ha.z = pack_h2(float(U.e[0][2].re), float(U.e[0][2].im));
+    ha.w = pack_h2(float(U.e[1][0].re), float(U.e[1][0].im));
+    uint2 hb;
+    hb.x = pack_h2(float(U.e[1][1].re), float(U.e[1][1].im));
+    hb.y = pack_h2(float(U.e[1][2].re), float(U.e[1][2].im));
+    ga.h12a[base * Vh + hs] = ha;
+    ga.h12b[base * Vh + hs] = hb;
+    // SU(3) check: rows 0,1 orthonormal and row 2 = conj(row0 x row1)
+    Su3<double> W = U;
+    reconstruct_row2(W);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      dev = fmax(dev, fabs(W.e[2][b].re - U.e[2][b].re));
+      dev = fmax(dev, fabs(W.e[2][b].im - U.e[2][b].im));
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int a2 = 0; a2 < 2; ++a2) {
+        Cx<double> s = {0.0, 0.0};
+#pragma unroll
+        for (int b = 0; b < 3; ++b) s = s + cj_mul(U.e[a][b], U.e[a2][b]);
+        dev = fmax(dev, fabs(s.re - (a == a2 ? 1.0 : 0.0)));
+        dev = fmax(dev, fabs(s.im));
+      }
+  }
+  dev = warp_max(dev);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxdev, dev);
+}
+
+cudaError_t launch_import_gauge(const Geom& g, const double* raw, GaugeArrays ga,
+                                unsigned long long* maxdev_bits, cudaStream_t st) {
+  import_gauge_kernel<<<grid_for(int64_t(8) * g.Vh, 256), 256, 0, st>>>(g, raw, ga, maxdev_bits);
+  return cudaGetLastError();
+}
+
+// ---- clover set-up (FP64) -------------------------------------------------------------
+// Spin matrices i*sigma_{mu nu} of Dirac_Clover::isigma_{23,31,12,41,42,43}
+// (lib/Dirac_ops/dirac_clover.cpp:221-329) reduced to the two chirality
+// blocks: s_pm[k][a][b] = S_k[a][b] +- S_k[a][b+2] for a,b in {0,1}.
+__constant__ double2 c_spm[2][6][2][2];
+
+struct M3d {
+  Cx<double> e[3][3];
+};
+
+__device__ __forceinline__ M3d m3_load(const double* raw, int64_t V, int64_t site, int mu) {
+  M3d m;
+  const double* u = raw + 18 * (site + V * mu);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) m.e[a][b] = {u[2 * (3 * a + b)], u[2 * (3 * a + b) + 1]};
+  return m;
+}
+__device__ __forceinline__ M3d m3_mul(const M3d& x, const M3d& y) {
+  M3d r;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) r.e[a][b] = x.e[a][0] * y.e[0][b] + x.e[a][1] * y.e[1][b] + x.e[a][2] * y.e[2][b];
+  return r;
+}
+__device__ __forceinline__ M3d m3_dag(const M3d& x) {
+  M3d r;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) r.e[a][b] = conjx(x.e[b][a]);
+  return r;
+}
+__device__ __forceinline__ M3d m3_ah(const M3d& x) {
+  M3d r;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) r.e[a][b] = 0.5 * (x.e[a][b] - conjx(x.e[b][a]));
+  return r;
+}
+
+__device__ __forceinline__ int64_t lex_shift(const Geom& g, int64_t site, int dir, int sgn) {
+  int c[4];
+  int64_t r = site;
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    c[d] = int(r % g.L[d]);
+    r /= g.L[d];
+  }
+  c[dir] = (c[dir] + sgn + g.L[dir]) % g.L[dir];
+  return c[0] + int64_t(g.L[0]) * (c[1] + int64_t(g.L[1]) * (c[2] + int64_t(g.L[2]) * c[3]));
+}
+
+// v(x) = Vup(x)^dag - Vdn(x)^dag (staples.cpp:596-597, 641-643)
+__device__ M3d leaves(const Geom& g, const double* raw, int64_t V, int64_t x, int mu, int nu) {
+  const int64_t xn = lex_shift(g, x, nu, 1), xm = lex_shift(g, x, mu, 1);
+  M3d up = m3_mul(m3_mul(m3_load(raw, V, x, nu), m3_load(raw, V, xn, mu)), m3_dag(m3_load(raw, V, xm, nu)));
+  const int64_t y = lex_shift(g, x, nu, -1), ym = lex_shift(g, y, mu, 1);
+  M3d dn = m3_mul(m3_mul(m3_dag(m3_load(raw, V, y, nu)), m3_load(raw, V, y, mu)), m3_load(raw, V, ym, nu));
+  M3d a = m3_dag(up), b = m3_dag(dn), v;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) v.e[i][j] = a.e[i][j] - b.e[i][j];
+  return v;
+}
+
+// Staples::fieldStrength (lib/Measurements/GaugeM/staples.cpp:587-666)
+__device__ M3d field_strength_at(const Geom& g, const double* raw, int64_t V, int64_t x, int mu, int nu) {
+  const int64_t xm = lex_shift(g, x, mu, -1);
+  M3d f1 = m3_ah(m3_mul(m3_load(raw, V, x, mu), leaves(g, raw, V, x, mu, nu)));
+  M3d f2 = m3_ah(m3_mul(leaves(g, raw, V, xm, mu, nu), m3_load(raw, V, xm, mu)));
+  M3d f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) f.e[i][j] = f1.e[i][j] + f2.e[i][j];
+  // traceless anti-Hermitian part (anti_hermite_traceless, sunMatUtils.cpp:50-55), x 0.25
+  const double imtr = (f.e[0][0].im + f.e[1][1].im + f.e[2][2].im) / 3.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) f.e[i][i].im -= imtr;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) f.e[i][j] = 0.25 * f.e[i][j];
+  return f;
+}
+
+__global__ void field_strength_kernel(Geom g, const double* raw, int mu, int nu, double* out) {
+  const int64_t V = 2 * int64_t(g.Vh);
+  for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < V;
+       x += int64_t(gridDim.x) * blockDim.x) {
+    M3d f = field_strength_at(g, raw, V, x, mu, nu);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        out[18 * x + 2 * (3 * i + j)] = f.e[i][j].re;
+        out[18 * x + 2 * (3 * i + j) + 1] = f.e[i][j].im;
+      }
+  }
+}
+
+cudaError_t launch_field_strength(const Geom& g, const double* raw, int mu, int nu, double* out,
+                                  cudaStream_t st) {
+  field_strength_kernel<<<grid_for(2 * int64_t(g.Vh), 128), 128, 0, st>>>(g, raw, mu, nu, out);
+  return cudaGetLastError();
+}
+
+// complex 6x6 inverse by Gauss-Jordan elimination with partial pivoting
+__device__ bool inv6(Cx<double> a[6][6], Cx<double> inv[6][6]) {
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) inv[i][j] = {i == j ? 1.0 : 0.0, 0.0};
+  for (int c = 0; c < 6; ++c) {
+    int piv = c;
+    double best = a[c][c].re * a[c][c].re + a[c][c].im * a[c][c].im;
+    for (int r = c + 1; r < 6; ++r) {
+      const double m = a[r][c].re * a[r][c].re + a[r][c].im * a[r][c].im;
+      if (m > best) {
+        best = m;
+        piv = r;
+      }
+    }
+    if (!(best > 0.0)) return false;
+    if (piv != c)
+      for (int j = 0; j < 6; ++j) {
+        Cx<double> t = a[c][j]; a[c][j] = a[piv][j]; a[piv][j] = t;
+        t = inv[c][j]; inv[c][j] = inv[piv][j]; inv[piv][j] = t;
+      }
+    const double den = a[c][c].re * a[c][c].re + a[c][c].im * a[c][c].im;
+    const Cx<double> rp = {a[c][c].re / den, -a[c][c].im / den};
+    for (int j = 0; j < 6; ++j) {
+      a[c][j] = a[c][j] * rp;
+      inv[c][j] = inv[c][j] * rp;
+    }
+    for (int r = 0; r < 6; ++r) {
+      if (r == c) continue;
+      const Cx<double> f = a[r][c];
+      for (int j = 0; j < 6; ++j) {
+        a[r][j] = a[r][j] - f * a[c][j];
+        inv[r][j] = inv[r][j] - f * inv[c][j];
+      }
+    }
+  }
+  return true;
+}
+
+__device__ void store_block(const CloverArrays& ca, bool inverse, int p, int64_t Vh, int64_t hs,
+                            int blk, Cx<double> m[6][6]) {
+  // Hermitian parts: real diagonal and upper triangle (averaged with the lower)
+  double v[36];
+  for (int i = 0; i < 6; ++i) v[i] = m[i][i].re;
+  for (int i = 0; i < 6; ++i)
+    for (int j = i + 1; j < 6; ++j) {
+      const int k = tri(i, j);
+      v[6 + 2 * k] = 0.5 * (m[i][j].re + m[j][i].re);
+      v[7 + 2 * k] = 0.5 * (m[i][j].im - m[j][i].im);
+    }
+  void* const* arr = inverse ? ca.Ainv[0] : ca.A[0];
+  double2* d = static_cast<double2*>(arr[p]);
+  for (int k = 0; k < 18; ++k) d[(blk * 18 + k) * Vh + hs] = make_double2(v[2 * k], v[2 * k + 1]);
+  float* fptr = reinterpret_cast<float*>(static_cast<float4*>((inverse ? ca.Ainv[1] : ca.A[1])[p]));
+  // FP32: 18 float4 chunks over both blocks, values v_all[36*blk + j]
+  for (int q = 0; q < 9; ++q) {
+    float4 f4 = make_float4(float(v[4 * q]), float(v[4 * q + 1]), float(v[4 * q + 2]), float(v[4 * q + 3]));
+    reinterpret_cast<float4*>(fptr)[(blk * 9 + q) * Vh + hs] = f4;
+  }
+  uint4* h = static_cast<uint4*>((inverse ? ca.Ainv[2] : ca.A[2])[p]);
+  // FP16: 9 chunks of 8 halves over both blocks: block 0 owns values 0..35,
+  // block 1 36..71; chunk 4 straddles the two blocks (values 32..39).
+  // Written per half-word pair so the two blocks can be stored independently.
+  unsigned short* hs16 = reinterpret_cast<unsigned short*>(h);
+  for (int j = 0; j < 36; ++j) {
+    const int gidx = 36 * blk + j;
+    const int q = gidx / 8, w = gidx % 8;
+    __half hv = __float2half_rn(float(v[j]));
+    hs16[((int64_t(q) * Vh + hs) * 8) + w] = *reinterpret_cast<unsigned short*>(&hv);
+  }
+}
+
+__global__ void clover_build_kernel(Geom g, const double* raw, double kc, CloverArrays ca, int* singular) {
+  const int64_t Vh = g.Vh;
+  const int64_t V = 2 * Vh;
+  const int PAIRS[6][2] = {{1, 2}, {2, 0}, {0, 1}, {3, 0}, {3, 1}, {3, 2}};
+  for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < V;
+       x += int64_t(gridDim.x) * blockDim.x) {
+    int c4[4];
+    int64_t rr = x;
+    for (int d = 0; d < 4; ++d) {
+      c4[d] = int(rr % g.L[d]);
+      rr /= g.L[d];
+    }
+    const int p = (c4[0] + c4[1] + c4[2] + c4[3]) & 1;
+    const int64_t hs = x >> 1;
+    Cx<double> B[2][6][6];
+    for (int s = 0; s < 2; ++s)
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) B[s][i][j] = {i == j ? 1.0 : 0.0, 0.0};
+    for (int k = 0; k < 6; ++k) {
+      const M3d F = field_strength_at(g, raw, V, x, PAIRS[k][0], PAIRS[k][1]);
+      for (int s = 0; s < 2; ++s)
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) {
+            const double2 sv = c_spm[s][k][a][b];
+            if (sv.x == 0.0 && sv.y == 0.0) continue;
+            const Cx<double> sc = {-kc * sv.x, -kc * sv.y};
+            for (int i = 0; i < 3; ++i)
+              for (int j = 0; j < 3; ++j) B[s][a * 3 + i][b * 3 + j] = B[s][a * 3 + i][b * 3 + j] + sc * F.e[i][j];
+          }
+    }
+    for (int s = 0; s < 2; ++s) {
+      Cx<double> inv[6][6], work[6][6];
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) work[i][j] = B[s][i][j];
+      if (!inv6(work, inv)) atomicExch(singular, 1);
+      store_block(ca, false, p, Vh, hs, s, B[s]);
+      store_block(ca, true, p, Vh, hs, s, inv);
+    }
+  }
+}
+
+cudaError_t launch_clover_build(const Geom& g, const double* raw, double kappa_csw,
+                                CloverArrays ca, int* singular, cudaStream_t st) {
+  clover_build_kernel<<<grid_for(2 * int64_t(g.Vh), 64), 64, 0, st>>>(g, raw, kappa_csw, ca, singular);
+  return cudaGetLastError();
+}
+
+void clover_init_tables() {
+  // S_k[s_out][s_in] as (re, im), from Dirac_Clover::isigma_* (dirac_clover.cpp:221-329)
+  double S[6][4][4][2];
+  std::memset(S, 0, sizeof(S));
+  auto set = [&](int k, int a, int b, double re, double im) {
+    S[k][a][b][0] = re;
+    S[k][a][b][1] = im;
+  };
+  // isigma_23: w0 = i v1, w1 = i v0, w2 = i v3, w3 = i v2
+  set(0, 0, 1, 0, 1); set(0, 1, 0, 0, 1); set(0, 2, 3, 0, 1); set(0, 3, 2, 0, 1);
+  // isigma_31: w0 = v1, w1 = -v0, w2 = v3, w3 = -v2
+  set(1, 0, 1, 1, 0); set(1, 1, 0, -1, 0); set(1, 2, 3, 1, 0); set(1, 3, 2, -1, 0);
+  // isigma_12: w0 = i v0, w1 = -i v1, w2 = i v2, w3 = -i v3
+  set(2, 0, 0, 0, 1); set(2, 1, 1, 0, -1); set(2, 2, 2, 0, 1); set(2, 3, 3, 0, -1);
+  // isigma_41: w0 = -i v3, w1 = -i v2, w2 = -i v1, w3 = -i v0
+  set(3, 0, 3, 0, -1); set(3, 1, 2, 0, -1); set(3, 2, 1, 0, -1); set(3, 3, 0, 0, -1);
+  // isigma_42: w0 = -v3, w1 = v2, w2 = -v1, w3 = v0
+  set(4, 0, 3, -1, 0); set(4, 1, 2, 1, 0); set(4, 2, 1, -1, 0); set(4, 3, 0, 1, 0);
+  // isigma_43: w0 = -i v2, w1 = i v3, w2 = -i v0, w3 = i v1
+  set(5, 0, 2, 0, -1); set(5, 1, 3, 0, 1); set(5, 2, 0, 0, -1); set(5, 3, 1, 0, 1);
+  double2 spm[2][6][2][2];
+  for (int s = 0; s < 2; ++s)
+    for (int k = 0; k < 6; ++k)
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          const double sg = s == 0 ? 1.0 : -1.0;
+          spm[s][k][a][b].x = S[k][a][b][0] + sg * S[k][a][b + 2][0];
+          spm[s][k][a][b].y = S[k][a][b][1] + sg * S[k][a][b + 2][1];
+        }
+  cudaMemcpyToSymbol(c_spm, spm, sizeof(spm));
+}
+
+}  // namespace iro
+
+namespace iro {
+
+// ---- mixed-precision reliable updates -------------------------------------------------
+// x64 += xlo; xlo = 0   for right-hand sides with mask[r] != 0
+template <int PL>
+__global__ void mx_merge_kernel(int64_t n, int nrhs, SpinorPtr x64, SpinorPtr xlo, const int* mask) {
+  using RL = typename SpinorIO<PL>::Real;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    if (!mask[i % nrhs]) continue;
+    Cx<double> a[12];
+    Cx<RL> l[12];
+    SpinorIO<PREC_DOUBLE>::load(x64, i, a);
+    SpinorIO<PL>::load(xlo, i, l);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      a[k] = a[k] + Cx<double>{double(l[k].re), double(l[k].im)};
+      l[k] = {RL(0), RL(0)};
+    }
+    SpinorIO<PREC_DOUBLE>::store(x64, i, a);
+    SpinorIO<PL>::store(xlo, i, l);
+  }
+}
+
+// r64 = b - s64; rlo = r64; reduce |r64|^2   for mask[r] != 0
+template <int PL>
+__global__ void __launch_bounds__(256) mx_residual_kernel(int64_t n, int nrhs, SpinorPtr b, SpinorPtr s64, SpinorPtr r64,
+                                   SpinorPtr rlo, const int* mask, Reduce red) {
+  using RL = typename SpinorIO<PL>::Real;
+  double acc = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    if (!mask[i % nrhs]) continue;
+    Cx<double> bv[12], sv[12];
+    Cx<RL> l[12];
+    SpinorIO<PREC_DOUBLE>::load(b, i, bv);
+    SpinorIO<PREC_DOUBLE>::load(s64, i, sv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      sv[k] = bv[k] - sv[k];
+      acc += sv[k].re * sv[k].re + sv[k].im * sv[k].im;
+      l[k] = {RL(sv[k].re), RL(sv[k].im)};
+    }
+    SpinorIO<PREC_DOUBLE>::store(r64, i, sv);
+    SpinorIO<PL>::store(rlo, i, l);
+  }
+  block_reduce_finish<1>(red, &acc, nrhs, blockIdx.x, gridDim.x);
+}
+
+// p = beta p + r   for mask[r] != 0
+template <int PL>
+__global__ void mx_p_kernel(int64_t n, int nrhs, SpinorPtr p, SpinorPtr r, const CGState* state,
+                            const int* mask) {
+  using RL = typename SpinorIO<PL>::Real;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int rhs = int(i % nrhs);
+    if (!mask[rhs]) continue;
+    const RL beta = RL(state[rhs].beta);
+    Cx<RL> pv[12], rv[12];
+    SpinorIO<PL>::load(p, i, pv);
+    SpinorIO<PL>::load(r, i, rv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) pv[k] = beta * pv[k] + rv[k];
+    SpinorIO<PL>::store(p, i, pv);
+  }
+}
+
+cudaError_t launch_mx_merge(int plo, int64_t sites, int nrhs, SpinorPtr x64, SpinorPtr xlo,
+                            const int* mask, cudaStream_t st) {
+  const int64_t n = sites * nrhs;
+  const int grid = grid_for(n, 256);
+  if (plo == PREC_SINGLE) mx_merge_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(n, nrhs, x64, xlo, mask);
+  else if (plo == PREC_HALF) mx_merge_kernel<PREC_HALF><<<grid, 256, 0, st>>>(n, nrhs, x64, xlo, mask);
+  else mx_merge_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(n, nrhs, x64, xlo, mask);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mx_residual(int plo, int64_t sites, int nrhs, SpinorPtr b, SpinorPtr s64,
+                               SpinorPtr r64, SpinorPtr rlo, const int* mask, const Reduce& red,
+                               int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(sites, nrhs, max_blocks);
+  const int64_t n = sites * nrhs;
+  if (plo == PREC_SINGLE) mx_residual_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(n, nrhs, b, s64, r64, rlo, mask, red);
+  else if (plo == PREC_HALF) mx_residual_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(n, nrhs, b, s64, r64, rlo, mask, red);
+  else mx_residual_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(n, nrhs, b, s64, r64, rlo, mask, red);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mx_p(int plo, int64_t sites, int nrhs, SpinorPtr p, SpinorPtr r,
+                        const CGState* state, const int* mask, cudaStream_t st) {
+  const int64_t n = sites * nrhs;
+  const int grid = grid_for(n, 256);
+  if (plo == PREC_SINGLE) mx_p_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(n, nrhs, p, r, state, mask);
+  else if (plo == PREC_HALF) mx_p_kernel<PREC_HALF><<<grid, 256, 0, st>>>(n, nrhs, p, r, state, mask);
+  else mx_p_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(n, nrhs, p, r, state, mask);
+  return cudaGetLastError();
+}
+
+}  // namespace iro

@@ -1,0 +1,217 @@
+// FP64 reductions and the Krylov solvers' scalar recurrences, kept on the
+// device so that an iteration needs no host round trip.
+//
+// A kernel that reduces hands its per-thread partial sums to
+// block_reduce_finish(): a fixed-order tree inside the block, one partial per
+// block in global scratch, and the last block to arrive (ticket counter)
+// sums the partials in block order -- deterministic run to run -- and then
+// applies the solver stage's scalar update (alpha, beta, convergence flags,
+// multishift zeta recurrences).
+#pragma once
+
+#include "common.cuh"
+
+namespace iro {
+
+// Per right-hand side CG state (Solver_CG::solve_step, lib/Solver/solver_CG.cpp:82-160).
+struct CGState {
+  double rr;       // (r,r)
+  double rr_prev;  // (r,r) of the previous iteration
+  double pap;      // (p,Ap)
+  double alpha;    // rr/pap
+  double beta;     // rr/rr_prev
+  double target;   // GoalPrecision * |b|^2
+  double maxrr;    // (r,r) at the last reliable update (mixed precision)
+  double delta2;   // reliable-update trigger delta^2; 0 for plain CG
+  int iter;        // iterations completed
+  int conv_iter;   // 0-based index of the converging iteration, -1 before
+};
+
+// done[] flag values
+enum { RUNNING = 0, CONVERGED = 1, STOPPED = 2, PAUSED = 3 };
+
+// Multishift CG state (MultiShiftSolver_CG::solve_step,
+// lib/Solver/multiShiftSolver_CG.cpp:34-93); shift arrays have MAXSHIFT slots.
+constexpr int MAXSHIFT = 16;
+struct MSState {
+  double rr, rrp, pap, alpha, beta, alphap, betap, snorm, prec, sigma0;
+  int nshift, nshift2, iter, conv_iter;
+  double csh2[MAXSHIFT], zeta1[MAXSHIFT], zeta2[MAXSHIFT], zeta[MAXSHIFT];
+  double betas[MAXSHIFT], alphas[MAXSHIFT], pp[MAXSHIFT];
+};
+
+enum Stage {
+  ST_NONE = 0,
+  ST_CG_ALPHA = 1,  // totals[0] = (p,Ap)            -> alpha
+  ST_CG_BETA = 2,   // totals[0] = (r,r)             -> beta, convergence
+  ST_MS_ALPHA = 3,  // totals[0]=|Mp|^2, [1]=|p|^2   -> pap incl. sigma0, beta
+  ST_MS_R = 4,      // totals[0] = (r,r)             -> alpha, zeta recurrences
+  ST_MS_PP = 5,     // totals[k] = |p_k|^2 (k>=1)    -> pruning, convergence
+  ST_CG_INIT = 6    // totals[0] = (r,r), [1] = |b|^2 -> rr, target
+};
+
+struct Reduce {
+  double* partials;   // [blocks][nred*nrhs] scratch
+  unsigned* counter;  // ticket, returned to zero by the last block
+  double* out;        // [nred*nrhs] totals
+  int stage;
+  void* state;   // CGState[nrhs] or MSState
+  int* done;     // per-rhs converged flags (CG)
+  int max_iter;  // CG: iterations after which a right-hand side stops
+};
+
+__device__ inline void stage_update(const Reduce& R, const double* tot, int nred, int nrhs) {
+  switch (R.stage) {
+    case ST_CG_ALPHA: {
+      CGState* s = static_cast<CGState*>(R.state);
+      for (int r = 0; r < nrhs; ++r) {
+        if (R.done[r]) continue;
+        s[r].pap = tot[r];
+        s[r].alpha = s[r].rr / s[r].pap;
+      }
+    } break;
+    case ST_CG_BETA: {
+      CGState* s = static_cast<CGState*>(R.state);
+      for (int r = 0; r < nrhs; ++r) {
+        if (R.done[r]) continue;
+        s[r].rr_prev = s[r].rr;
+        s[r].rr = tot[r];
+        const int it = s[r].iter;
+        s[r].iter = it + 1;
+        if (s[r].delta2 > 0.0) {
+          // mixed precision: pause for an FP64 residual recomputation when
+          // |r| fell by delta since the last one, or looks converged;
+          // convergence is declared on the true residual only
+          if (s[r].rr < s[r].delta2 * s[r].maxrr || s[r].rr < s[r].target) {
+            R.done[r] = PAUSED;
+            continue;
+          }
+        } else if (s[r].rr < s[r].target) {
+          s[r].beta = s[r].rr / s[r].rr_prev;
+          s[r].conv_iter = it;
+          R.done[r] = CONVERGED;
+          continue;
+        }
+        s[r].beta = s[r].rr / s[r].rr_prev;
+        if (s[r].iter >= R.max_iter) R.done[r] = STOPPED;
+      }
+    } break;
+    case ST_MS_ALPHA: {
+      MSState* m = static_cast<MSState*>(R.state);
+      if (R.done[0]) break;
+      // s = A p0 + sigma0 p0 (multiShiftSolver_CG.cpp:49-50); (s,p0) =
+      // |M p0|^2 + sigma0 |p0|^2
+      m->pap = tot[0] + m->sigma0 * tot[1];
+      m->rrp = m->rr;
+      m->beta = -m->rrp / m->pap;
+    } break;
+    case ST_MS_R: {
+      MSState* m = static_cast<MSState*>(R.state);
+      if (R.done[0]) break;
+      m->rr = tot[0];
+      m->alpha = m->rr / m->rrp;
+      m->pp[0] = m->rr;
+      const double alphah = 1.0 + m->alphap * m->beta / m->betap;
+      for (int k = 1; k < m->nshift2; ++k) {
+        double zeta = (alphah - m->csh2[k] * m->beta) / m->zeta1[k] + (1.0 - alphah) / m->zeta2[k];
+        zeta = 1.0 / zeta;
+        const double zr = zeta / m->zeta1[k];
+        m->betas[k] = m->beta * zr;
+        m->alphas[k] = m->alpha * zr * zr;
+        m->zeta[k] = zeta;
+      }
+    } break;
+    case ST_MS_PP: {
+      MSState* m = static_cast<MSState*>(R.state);
+      if (R.done[0]) break;
+      for (int k = 1; k < m->nshift2; ++k) {
+        m->pp[k] = tot[k] * m->snorm;
+        m->zeta2[k] = m->zeta1[k];
+        m->zeta1[k] = m->zeta[k];
+      }
+      for (int k = m->nshift2 - 1; k >= 0; --k) {
+        if (m->pp[k] > m->prec) {
+          m->nshift2 = k + 1;
+          break;
+        }
+      }
+      m->alphap = m->alpha;
+      m->betap = m->beta;
+      const int it = m->iter;
+      m->iter = it + 1;
+      if (m->rr * m->snorm < m->prec) {
+        m->conv_iter = it;
+        R.done[0] = 1;
+      } else if (m->iter >= R.max_iter) {
+        R.done[0] = 2;
+      }
+    } break;
+    case ST_CG_INIT: {
+      CGState* s = static_cast<CGState*>(R.state);
+      for (int r = 0; r < nrhs; ++r) {
+        s[r].rr = tot[r];
+        s[r].maxrr = tot[r];
+        s[r].target *= tot[nrhs + r];  // GoalPrecision * |b|^2
+        s[r].iter = 0;
+        s[r].conv_iter = -1;
+        R.done[r] = (R.max_iter <= 0) ? STOPPED : RUNNING;
+      }
+    } break;
+    default:
+      break;
+  }
+}
+
+// Block size must be nrhs * 2^k (so each thread keeps one right-hand side
+// across a grid-stride loop whose stride is a multiple of nrhs).
+template <int NRED>
+__device__ void block_reduce_finish(const Reduce& R, const double* v, int nrhs, int bid, int nblk) {
+  __shared__ double sm[NRED][256];
+  __shared__ bool last;
+  const int t = threadIdx.x;
+  const int n = blockDim.x;
+#pragma unroll
+  for (int k = 0; k < NRED; ++k) sm[k][t] = v[k];
+  __syncthreads();
+  for (int s = (n / nrhs) / 2; s > 0; s >>= 1) {
+    if (t < s * nrhs) {
+#pragma unroll
+      for (int k = 0; k < NRED; ++k) sm[k][t] += sm[k][t + s * nrhs];
+    }
+    __syncthreads();
+  }
+  const int nv = NRED * nrhs;
+  if (t < nrhs) {
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) R.partials[int64_t(bid) * nv + k * nrhs + t] = sm[k][t];
+  }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) last = (atomicAdd(R.counter, 1u) == unsigned(nblk - 1));
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double tot[NRED * 16];
+  int p2 = 1;
+  while (p2 < n) p2 <<= 1;
+  for (int q = 0; q < nv; ++q) {
+    double s = 0.0;
+    for (int b = t; b < nblk; b += n) s += __ldcg(R.partials + int64_t(b) * nv + q);
+    sm[0][t] = s;
+    __syncthreads();
+    for (int h = p2 / 2; h > 0; h >>= 1) {
+      if (t < h && t + h < n) sm[0][t] += sm[0][t + h];
+      __syncthreads();
+    }
+    if (t == 0) tot[q] = sm[0][0];
+    __syncthreads();
+  }
+  if (t == 0) {
+    for (int q = 0; q < nv; ++q) R.out[q] = tot[q];
+    *R.counter = 0u;
+    stage_update(R, tot, NRED, nrhs);
+    __threadfence();
+  }
+}
+
+}  // namespace iro

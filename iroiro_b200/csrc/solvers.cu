@@ -1,0 +1,471 @@
+// Krylov solvers on the device: the reference's FP64 CG and multishift CG,
+// and the mixed-precision reliable-update CG.  The iteration scalars live on
+// the device (solver_scalars.cuh); the host only launches a chunk of
+// iterations (optionally as one CUDA graph) and polls the convergence flags
+// between chunks.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "iroiro_b200.h"
+
+namespace iro {
+namespace host {
+int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in, DevField& out,
+          const Reduce* red, int red_mask, const int* skip);
+DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
+int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
+int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
+int norms(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
+          std::vector<double>* nw);
+int axpby(iro_ctx* c, double a, const DevField& x, double b, const DevField& y, DevField& v);
+int convert(iro_ctx* c, const DevField& in, DevField& out);
+Reduce reduce(iro_ctx* c, int stage, int max_iter);
+int set_error(iro_ctx* c, int code, const std::string& msg);
+int cuda_error(iro_ctx* c, cudaError_t e, const char* where);
+cudaStream_t stream(iro_ctx* c);
+int max_blocks(iro_ctx* c);
+int64_t vh(iro_ctx* c);
+void* state(iro_ctx* c);
+int* done(iro_ctx* c);
+void* pinned(iro_ctx* c);
+int device(iro_ctx* c);
+bool op_is_full(int op);
+int op_subset(int op);
+bool op_ok(int op);
+}  // namespace host
+}  // namespace iro
+
+using namespace iro;
+using namespace iro::host;
+
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t e__ = (call);                                \
+    if (e__ != cudaSuccess) return cuda_error(c, e__, #call); \
+  } while (0)
+#define RC(call)              \
+  do {                        \
+    int r__ = (call);         \
+    if (r__ != IRO_OK) return r__; \
+  } while (0)
+
+namespace {
+
+constexpr int kChunk = 8;  // iterations launched between host polls
+
+bool solver_op_ok(int op) {
+  return op == IRO_OP_WILSON_FULL || op == IRO_OP_WILSON_SCHUR_EE || op == IRO_OP_CLOVER_FULL ||
+         op == IRO_OP_CLOVER_SCHUR_EE;
+}
+
+// Runs `body` (which enqueues `n` iterations) repeatedly until every
+// right-hand side has left the iteration (done flag set) or max_iter is hit.
+// With use_graph the chunk is captured once as a CUDA graph and replayed.
+template <typename F>
+int iterate(iro_ctx* c, int nrhs, int max_iter, bool use_graph, F body) {
+  cudaStream_t st = stream(c);
+  int* hdone = static_cast<int*>(pinned(c));
+  cudaGraphExec_t exec = nullptr;
+  if (use_graph) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = body(kChunk);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaGraphInstantiate");
+  }
+  int launched = 0;
+  int rc = IRO_OK;
+  while (launched < max_iter) {
+    if (exec) {
+      cudaError_t e = cudaGraphLaunch(exec, st);
+      if (e != cudaSuccess) {
+        rc = cuda_error(c, e, "cudaGraphLaunch");
+        break;
+      }
+    } else {
+      rc = body(kChunk);
+      if (rc) break;
+    }
+    launched += kChunk;
+    cudaError_t e = cudaMemcpyAsync(hdone, done(c), sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      rc = cuda_error(c, e, "poll");
+      break;
+    }
+    bool all = true;
+    for (int r = 0; r < nrhs; ++r) all = all && hdone[r] != 0;
+    if (all) break;
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  return rc;
+}
+
+// FP64 CG on D^dag D, Solver_CG::solve (lib/Solver/solver_CG.cpp:29-80).
+int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+              const double* b, double* x, int nrhs, iro_solver_out* out) {
+  const int sub = op_subset(op);
+  const bool full = op_is_full(op);
+  int rc = IRO_OK;
+  DevField* B = workspace(c, sub, PREC_DOUBLE, nrhs, 20, &rc); if (!B) return rc;
+  DevField* X = workspace(c, sub, PREC_DOUBLE, nrhs, 21, &rc); if (!X) return rc;
+  DevField* R = workspace(c, sub, PREC_DOUBLE, nrhs, 22, &rc); if (!R) return rc;
+  DevField* P = workspace(c, sub, PREC_DOUBLE, nrhs, 23, &rc); if (!P) return rc;
+  DevField* S = workspace(c, sub, PREC_DOUBLE, nrhs, 24, &rc); if (!S) return rc;
+  DevField* Q = workspace(c, sub, PREC_DOUBLE, nrhs, 25, &rc); if (!Q) return rc;
+  cudaStream_t st = stream(c);
+  RC(import_field(c, b, full, *B));
+  RC(axpby(c, 1.0, *B, 0.0, *B, *X));  // x0 = b (solver_CG.cpp:40)
+  // CG state: target = GoalPrecision (scaled by |b|^2 in the init stage)
+  std::vector<CGState> s0(nrhs);
+  for (auto& s : s0) {
+    std::memset(&s, 0, sizeof(s));
+    s.target = prm->precision;
+    s.conv_iter = -1;
+  }
+  CK(cudaMemcpyAsync(state(c), s0.data(), sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
+  // r = b - A x, p = r, rr = (r,r)
+  RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  Reduce rinit = reduce(c, ST_CG_INIT, prm->max_iter);
+  CK(launch_cg_init(PREC_DOUBLE, B->sites(), nrhs, B->all(), S->all(), R->all(), P->all(), rinit,
+                    max_blocks(c), st));
+  const int* skip = done(c);
+  Reduce ralpha = reduce(c, ST_CG_ALPHA, prm->max_iter);
+  Reduce rbeta = reduce(c, ST_CG_BETA, prm->max_iter);
+  auto body = [&](int n) -> int {
+    for (int i = 0; i < n; ++i) {
+      // s = D^dag (D p), (p, s) = |D p|^2
+      RC(apply(c, op, mass, csw, false, *P, *Q, &ralpha, RED_OUT2, skip));
+      RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
+      CK(launch_cg_xr(PREC_DOUBLE, X->sites(), nrhs, X->all(), R->all(), P->all(), S->all(),
+                      static_cast<const CGState*>(state(c)), rbeta, max_blocks(c), st));
+      CK(launch_cg_p(PREC_DOUBLE, P->sites(), nrhs, P->all(), R->all(),
+                     static_cast<const CGState*>(state(c)), done(c), st));
+    }
+    return IRO_OK;
+  };
+  RC(iterate(c, nrhs, prm->max_iter, prm->use_graph != 0, body));
+  // true residual |A x - b| / |b| (solver_CG.cpp:69-71)
+  RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  RC(axpby(c, 1.0, *S, -1.0, *B, *R));
+  std::vector<double> rn, bn;
+  RC(norms(c, *R, B, rn, &bn));
+  std::vector<CGState> s1(nrhs);
+  CK(cudaMemcpyAsync(s1.data(), state(c), sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  RC(export_field(c, *X, full, x));
+  int status = IRO_OK;
+  for (int r = 0; r < nrhs; ++r) {
+    out[r].diff = std::sqrt(rn[r] / bn[r]);
+    out[r].iterations = s1[r].conv_iter;
+    out[r].reliable_updates = 0;
+    out[r].operator_applies = s1[r].iter + 2;
+    if (s1[r].conv_iter < 0) status = IRO_NOT_CONVERGED;
+  }
+  if (status) set_error(c, status, "CG solver not converged");
+  return status;
+}
+
+}  // namespace
+
+int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+             const double* b, double* x, int nrhs, iro_solver_out* out);
+
+extern "C" int iro_cg_solve(iro_ctx* c, int op, double mass, double csw,
+                            const iro_cg_params* prm, const double* b, double* x, int nrhs,
+                            iro_solver_out* out) {
+  if (!c || !prm || !b || !x || !out || nrhs < 1 || nrhs > 16 || !solver_op_ok(op) ||
+      prm->inner_prec < 0 || prm->inner_prec > 2 || !(prm->precision > 0.0))
+    return set_error(c, IRO_BAD_ARG, "bad CG arguments");
+  CK(cudaSetDevice(device(c)));
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = prm->inner_prec == PREC_DOUBLE ? cg_double(c, op, mass, csw, prm, b, x, nrhs, out)
+                                          : cg_mixed(c, op, mass, csw, prm, b, x, nrhs, out);
+  auto t1 = std::chrono::steady_clock::now();
+  const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  for (int r = 0; r < nrhs; ++r) out[r].timing_ms = ms;
+  return rc;
+}
+
+// ---- multishift CG ---------------------------------------------------------------------
+// MultiShiftSolver_CG::solve (lib/Solver/multiShiftSolver_CG.cpp:95-185) in FP64.
+extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double csw,
+                                       const double* b, int nshift, const double* shifts,
+                                       double* x, double precision, int max_iter,
+                                       iro_solver_out* out, int* nconv) {
+  if (!c || !b || !shifts || !x || !out || !nconv || nshift < 1 || nshift > MAXSHIFT ||
+      !solver_op_ok(op) || !(precision > 0.0))
+    return set_error(c, IRO_BAD_ARG, "bad multishift arguments");
+  CK(cudaSetDevice(device(c)));
+  auto t0 = std::chrono::steady_clock::now();
+  const int sub = op_subset(op);
+  const bool full = op_is_full(op);
+  int rc = IRO_OK;
+  DevField* B = workspace(c, sub, PREC_DOUBLE, 1, 30, &rc); if (!B) return rc;
+  DevField* R = workspace(c, sub, PREC_DOUBLE, 1, 31, &rc); if (!R) return rc;
+  DevField* S = workspace(c, sub, PREC_DOUBLE, 1, 32, &rc); if (!S) return rc;
+  DevField* Q = workspace(c, sub, PREC_DOUBLE, 1, 33, &rc); if (!Q) return rc;
+  std::vector<DevField*> XS(nshift), PS(nshift);
+  for (int k = 0; k < nshift; ++k) {
+    XS[k] = workspace(c, sub, PREC_DOUBLE, 1, 40 + k, &rc); if (!XS[k]) return rc;
+    PS[k] = workspace(c, sub, PREC_DOUBLE, 1, 40 + MAXSHIFT + k, &rc); if (!PS[k]) return rc;
+  }
+  cudaStream_t st = stream(c);
+  RC(import_field(c, b, full, *B));
+  std::vector<double> bn;
+  RC(norms(c, *B, nullptr, bn, nullptr));
+  // solve_init (multiShiftSolver_CG.cpp:10-32): p_i = b, x_i = 0, r = b
+  for (int k = 0; k < nshift; ++k) {
+    RC(axpby(c, 1.0, *B, 0.0, *B, *PS[k]));
+    RC(axpby(c, 0.0, *B, 0.0, *B, *XS[k]));
+  }
+  RC(axpby(c, 1.0, *B, 0.0, *B, *R));
+  MSState m;
+  std::memset(&m, 0, sizeof(m));
+  m.rr = bn[0];
+  m.alphap = 0.0;
+  m.betap = 1.0;
+  m.snorm = 1.0 / bn[0];
+  m.prec = precision;
+  m.sigma0 = shifts[0];
+  m.nshift = nshift;
+  m.nshift2 = nshift;
+  m.conv_iter = -1;
+  for (int k = 0; k < nshift; ++k) {
+    m.csh2[k] = shifts[k] - shifts[0];
+    m.zeta1[k] = m.zeta2[k] = 1.0;
+  }
+  int zero = 0;
+  CK(cudaMemcpyAsync(state(c), &m, sizeof(m), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(done(c), &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+  MSFields f;
+  for (int k = 0; k < MAXSHIFT; ++k) {
+    f.x[k] = XS[k < nshift ? k : 0]->all();
+    f.p[k] = PS[k < nshift ? k : 0]->all();
+  }
+  const MSState* dm = static_cast<const MSState*>(state(c));
+  Reduce ralpha = reduce(c, ST_MS_ALPHA, max_iter);
+  Reduce rr = reduce(c, ST_MS_R, max_iter);
+  Reduce rpp = reduce(c, ST_MS_PP, max_iter);
+  const int* skip = done(c);
+  auto body = [&](int n) -> int {
+    for (int i = 0; i < n; ++i) {
+      RC(apply(c, op, mass, csw, false, *PS[0], *Q, &ralpha, RED_OUT2 | RED_X2, skip));
+      RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
+      CK(launch_ms_xr(B->sites(), XS[0]->all(), R->all(), PS[0]->all(), S->all(), dm, rr,
+                      max_blocks(c), st));
+      CK(launch_ms_p(B->sites(), nshift, f, R->all(), dm, rpp, max_blocks(c), st));
+    }
+    return IRO_OK;
+  };
+  RC(iterate(c, 1, max_iter, true, body));
+  CK(cudaMemcpyAsync(&m, state(c), sizeof(m), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  // true residuals of every shift (multiShiftSolver_CG.cpp:166-177)
+  double dmax = -1.0;
+  for (int k = 0; k < nshift; ++k) {
+    RC(apply(c, op, mass, csw, false, *XS[k], *Q, nullptr, 0, nullptr));
+    RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+    RC(axpby(c, 1.0, *S, shifts[k], *XS[k], *S));
+    RC(axpby(c, 1.0, *S, -1.0, *B, *S));
+    std::vector<double> sn;
+    RC(norms(c, *S, nullptr, sn, nullptr));
+    const double d1 = sn[0] / bn[0];
+    if (d1 > dmax) dmax = d1;
+    const size_t nfield = size_t(24) * size_t(full ? 2 * vh(c) : vh(c));
+    RC(export_field(c, *XS[k], full, x + size_t(k) * nfield));
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  out->diff = std::sqrt(dmax);
+  out->iterations = m.conv_iter;
+  out->timing_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  out->reliable_updates = 0;
+  out->operator_applies = m.iter + nshift;
+  *nconv = m.conv_iter;
+  if (m.conv_iter < 0) return set_error(c, IRO_NOT_CONVERGED, "Not converged.");
+  return IRO_OK;
+}
+
+// ---- mixed-precision reliable-update CG ----------------------------------------------
+// Inner CG iterations run on FP32 or FP16 storage with FP32 arithmetic; the
+// solution is accumulated in FP64 and, whenever the iterated residual has
+// fallen by `delta` since the last recomputation (or looks converged), the
+// residual is recomputed in FP64 as r = b - A x and the iteration continues
+// from it (reliable updates: Sleijpen & van der Vorst, "Reliable updated
+// residuals in hybrid Bi-CG methods", Computing 56 (1996); the FP32/FP16
+// variant follows Clark et al., "Solving lattice QCD systems of equations
+// using mixed precision solvers on GPUs", CPC 181 (2010)).  Convergence is
+// declared only on the FP64 true residual.  The starting guess is x0 = b as
+// in Solver_CG (solver_CG.cpp:40).
+int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+             const double* b, double* x, int nrhs, iro_solver_out* out) {
+  const int sub = op_subset(op);
+  const bool full = op_is_full(op);
+  const int pl = prm->inner_prec;
+  int rc = IRO_OK;
+  DevField* B = workspace(c, sub, PREC_DOUBLE, nrhs, 20, &rc); if (!B) return rc;
+  DevField* X = workspace(c, sub, PREC_DOUBLE, nrhs, 21, &rc); if (!X) return rc;
+  DevField* R = workspace(c, sub, PREC_DOUBLE, nrhs, 22, &rc); if (!R) return rc;
+  DevField* S = workspace(c, sub, PREC_DOUBLE, nrhs, 24, &rc); if (!S) return rc;
+  DevField* Q = workspace(c, sub, PREC_DOUBLE, nrhs, 25, &rc); if (!Q) return rc;
+  DevField* Xl = workspace(c, sub, pl, nrhs, 26, &rc); if (!Xl) return rc;
+  DevField* Rl = workspace(c, sub, pl, nrhs, 27, &rc); if (!Rl) return rc;
+  DevField* Pl = workspace(c, sub, pl, nrhs, 28, &rc); if (!Pl) return rc;
+  DevField* Sl = workspace(c, sub, pl, nrhs, 29, &rc); if (!Sl) return rc;
+  DevField* Ql = workspace(c, sub, pl, nrhs, 19, &rc); if (!Ql) return rc;
+  cudaStream_t st = stream(c);
+  int* dmask = done(c) + 32;
+  int* hpin = static_cast<int*>(pinned(c));
+  const double delta = prm->delta > 0.0 ? prm->delta : 0.1;
+
+  RC(import_field(c, b, full, *B));
+  RC(axpby(c, 1.0, *B, 0.0, *B, *X));
+  std::vector<CGState> hs(nrhs);
+  for (auto& s : hs) {
+    std::memset(&s, 0, sizeof(s));
+    s.target = prm->precision;
+    s.delta2 = delta * delta;
+    s.conv_iter = -1;
+  }
+  CK(cudaMemcpyAsync(state(c), hs.data(), sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
+  // FP64 r = b - A x; low-precision r, p; x_lo = 0
+  RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  Reduce rinit = reduce(c, ST_CG_INIT, prm->max_iter);
+  CK(launch_cg_init(PREC_DOUBLE, B->sites(), nrhs, B->all(), S->all(), R->all(), Q->all(), rinit,
+                    max_blocks(c), st));
+  RC(convert(c, *R, *Rl));
+  RC(convert(c, *R, *Pl));
+  RC(axpby(c, 0.0, *Rl, 0.0, *Rl, *Xl));
+
+  const int* skip = done(c);
+  Reduce ralpha = reduce(c, ST_CG_ALPHA, prm->max_iter);
+  Reduce rbeta = reduce(c, ST_CG_BETA, prm->max_iter);
+  Reduce rnone = reduce(c, ST_NONE, 0);
+  auto body = [&](int n) -> int {
+    for (int i = 0; i < n; ++i) {
+      RC(apply(c, op, mass, csw, false, *Pl, *Ql, &ralpha, RED_OUT2, skip));
+      RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, skip));
+      CK(launch_cg_xr(pl, Xl->sites(), nrhs, Xl->all(), Rl->all(), Pl->all(), Sl->all(),
+                      static_cast<const CGState*>(state(c)), rbeta, max_blocks(c), st));
+      CK(launch_cg_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(),
+                     static_cast<const CGState*>(state(c)), done(c), st));
+    }
+    return IRO_OK;
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (prm->use_graph) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int brc = body(kChunk);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (brc) return brc;
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaGraphInstantiate");
+  }
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() { if (e) cudaGraphExecDestroy(e); }
+  } guard{exec};
+
+  std::vector<int> updates(nrhs, 0);
+  std::vector<int> hdone(nrhs), mask(nrhs);
+  for (;;) {
+    // inner iterations until some right-hand side pauses or all have left
+    for (;;) {
+      if (exec) CK(cudaGraphLaunch(exec, st));
+      else RC(body(kChunk));
+      CK(cudaMemcpyAsync(hpin, done(c), sizeof(int) * nrhs, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      bool any_pause = false, all_left = true;
+      for (int r = 0; r < nrhs; ++r) {
+        any_pause = any_pause || hpin[r] == PAUSED;
+        all_left = all_left && hpin[r] != RUNNING;
+      }
+      if (any_pause || all_left) break;
+    }
+    bool any_pause = false;
+    for (int r = 0; r < nrhs; ++r) {
+      hdone[r] = hpin[r];
+      mask[r] = hdone[r] == PAUSED ? 1 : 0;
+      any_pause = any_pause || mask[r];
+    }
+    if (!any_pause) break;
+    // reliable update of the paused right-hand sides: x += x_lo, r = b - A x
+    CK(cudaMemcpyAsync(dmask, mask.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+    CK(launch_mx_merge(pl, X->sites(), nrhs, X->all(), Xl->all(), dmask, st));
+    RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+    RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+    CK(launch_mx_residual(pl, B->sites(), nrhs, B->all(), S->all(), R->all(), Rl->all(), dmask,
+                          rnone, max_blocks(c), st));
+    std::vector<double> rr(nrhs);
+    CK(cudaMemcpyAsync(hs.data(), state(c), sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // the reduction's totals are in the context's output slot
+    {
+      Reduce tmp = rnone;
+      CK(cudaMemcpyAsync(rr.data(), tmp.out, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+    for (int r = 0; r < nrhs; ++r) {
+      if (!mask[r]) continue;
+      ++updates[r];
+      CGState& s = hs[r];
+      s.rr = rr[r];
+      s.maxrr = rr[r];
+      s.beta = s.rr / s.rr_prev;
+      if (s.rr < s.target) {
+        s.conv_iter = s.iter - 1;
+        hdone[r] = CONVERGED;
+        mask[r] = 0;
+      } else if (s.iter >= prm->max_iter) {
+        hdone[r] = STOPPED;
+        mask[r] = 0;
+      } else {
+        hdone[r] = RUNNING;
+      }
+    }
+    CK(cudaMemcpyAsync(state(c), hs.data(), sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dmask, mask.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+    CK(launch_mx_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(),
+                   static_cast<const CGState*>(state(c)), dmask, st));
+    CK(cudaMemcpyAsync(done(c), hdone.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+    bool all_left = true;
+    for (int r = 0; r < nrhs; ++r) all_left = all_left && hdone[r] != RUNNING;
+    if (all_left) break;
+  }
+  // fold any remaining low-precision correction in, then the FP64 true residual
+  std::vector<int> ones(nrhs, 1);
+  CK(cudaMemcpyAsync(dmask, ones.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+  CK(launch_mx_merge(pl, X->sites(), nrhs, X->all(), Xl->all(), dmask, st));
+  RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  RC(axpby(c, 1.0, *S, -1.0, *B, *R));
+  std::vector<double> rn, bn;
+  RC(norms(c, *R, B, rn, &bn));
+  CK(cudaMemcpyAsync(hs.data(), state(c), sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  RC(export_field(c, *X, full, x));
+  int status = IRO_OK;
+  for (int r = 0; r < nrhs; ++r) {
+    out[r].diff = std::sqrt(rn[r] / bn[r]);
+    out[r].iterations = hs[r].conv_iter;
+    out[r].reliable_updates = updates[r];
+    out[r].operator_applies = hs[r].iter + 2 * updates[r] + 2;
+    if (hs[r].conv_iter < 0) status = IRO_NOT_CONVERGED;
+  }
+  if (status) set_error(c, status, "mixed-precision CG not converged");
+  return status;
+}

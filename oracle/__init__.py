@@ -1,0 +1,226 @@
+"""CPU oracle for the fermion-solve hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may load this package, and only as the checker: the product
+(``iroiro_b200``) never imports it.
+
+Two implementations live here:
+
+* ``port()`` -- liboracle_port.so, a plain-C restatement (port/iro_oracle.c)
+  of the reference's Wilson/clover operators, CG and multishift CG, citing
+  the reference lines it follows.
+* ``ref()`` -- oracle/_ref/libiroiro_ref.so, the reference's own classes
+  compiled from its sources by oracle/Makefile (built only where the
+  reference tree is present; the built library travels with the repository
+  working copy).  It keeps the lattice in process-wide singletons, so one
+  process can serve one lattice size.
+
+The port is pinned against the reference through tests/golden/, which
+tests/golden/make_golden.py generates by running the reference library.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+PORT_LIB = HERE / "liboracle_port.so"
+REF_LIB = HERE / "_ref" / "libiroiro_ref.so"
+
+WILSON_FULL, WILSON_EO, CLOVER_FULL = 0, 1, 2
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.c_int
+_port = None
+_ref = None
+
+
+def build(ref: bool = False) -> None:
+    """make -C oracle port [ref]."""
+    targets = ["port"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def port() -> "Port":
+    global _port
+    if _port is None:
+        if not PORT_LIB.exists():
+            build()
+        _port = Port(ctypes.CDLL(str(PORT_LIB)))
+    return _port
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref() -> "Ref":
+    global _ref
+    if _ref is None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} not built (make -C oracle ref)")
+        _ref = Ref(ctypes.CDLL(str(REF_LIB)))
+    return _ref
+
+
+class Port:
+    """The C restatement; any lattice size per call."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        D, L4 = ctypes.c_double, ctypes.POINTER(ctypes.c_int)
+        lib.orc_gamma5.argtypes = [ctypes.c_long, _D, _D]
+        lib.orc_wilson_full.argtypes = [L4, _D, D, _I, _D, _D]
+        lib.orc_wilson_hop.argtypes = [L4, _D, D, _I, _I, _D, _D]
+        lib.orc_wilson_eo.argtypes = [L4, _D, D, _I, _D, _D]
+        lib.orc_field_strength.argtypes = [L4, _D, _I, _I, _D]
+        lib.orc_clover_full.argtypes = [L4, _D, D, D, _I, _D, _D]
+        lib.orc_cg.argtypes = [L4, _D, _I, D, D, _D, _D, D, _I, _D, ctypes.POINTER(_I)]
+        lib.orc_multishift.argtypes = [L4, _D, _I, D, D, _D, _I, _D, _D, D, _I, _D,
+                                       ctypes.POINTER(_I)]
+
+    @staticmethod
+    def _L(L):
+        return (ctypes.c_int * 4)(*[int(v) for v in L])
+
+    def gamma5(self, f):
+        f = np.ascontiguousarray(f, np.float64)
+        out = np.empty_like(f)
+        self.lib.orc_gamma5(f.size // 24, _p(f), _p(out))
+        return out
+
+    def wilson_full(self, L, u, mass, dag, f):
+        f = np.ascontiguousarray(f, np.float64)
+        out = np.empty_like(f)
+        self.lib.orc_wilson_full(self._L(L), _p(u), mass, int(dag), _p(f), _p(out))
+        return out
+
+    def wilson_hop(self, L, u, mass, eo, dag, f):
+        f = np.ascontiguousarray(f, np.float64)
+        out = np.empty_like(f)
+        self.lib.orc_wilson_hop(self._L(L), _p(u), mass, int(eo), int(dag), _p(f), _p(out))
+        return out
+
+    def wilson_eo(self, L, u, mass, dag, f):
+        f = np.ascontiguousarray(f, np.float64)
+        out = np.empty_like(f)
+        self.lib.orc_wilson_eo(self._L(L), _p(u), mass, int(dag), _p(f), _p(out))
+        return out
+
+    def field_strength(self, L, u, mu, nu):
+        out = np.empty(18 * int(np.prod(L)))
+        self.lib.orc_field_strength(self._L(L), _p(u), mu, nu, _p(out))
+        return out
+
+    def clover_full(self, L, u, mass, csw, dag, f):
+        f = np.ascontiguousarray(f, np.float64)
+        out = np.empty_like(f)
+        self.lib.orc_clover_full(self._L(L), _p(u), mass, csw, int(dag), _p(f), _p(out))
+        return out
+
+    def cg(self, L, u, op, mass, csw, b, prec, maxiter):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.empty_like(b)
+        diff = ctypes.c_double()
+        it = ctypes.c_int()
+        self.lib.orc_cg(self._L(L), _p(u), op, mass, csw, _p(b), _p(x), prec, maxiter,
+                        ctypes.byref(diff), ctypes.byref(it))
+        return x, it.value, diff.value
+
+    def multishift(self, L, u, op, mass, csw, b, shifts, prec, maxiter):
+        b = np.ascontiguousarray(b, np.float64)
+        sh = np.ascontiguousarray(shifts, np.float64)
+        x = np.empty(b.size * sh.size)
+        diff = ctypes.c_double()
+        nc = ctypes.c_int()
+        self.lib.orc_multishift(self._L(L), _p(u), op, mass, csw, _p(b), sh.size, _p(sh), _p(x),
+                                prec, maxiter, ctypes.byref(diff), ctypes.byref(nc))
+        return x.reshape(sh.size, b.size), nc.value, diff.value
+
+
+class Ref:
+    """The reference's own classes; one lattice per process (ref_init)."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        D = ctypes.c_double
+        lib.ref_init.argtypes = [_I, _I, _I, _I]
+        lib.ref_wilson_mult.argtypes = [_D, D, _I, _D, _D]
+        lib.ref_wilson_hop.argtypes = [_D, D, _I, _I, _D, _D]
+        lib.ref_wilson_eo_mult.argtypes = [_D, D, _I, _D, _D]
+        lib.ref_clover_mult.argtypes = [_D, D, D, _I, _D, _D]
+        lib.ref_field_strength.argtypes = [_D, _I, _I, _D]
+        lib.ref_cg_solve.argtypes = [_D, _I, D, D, _D, _D, D, _I, _D, ctypes.POINTER(_I), _D]
+        lib.ref_multishift_solve.argtypes = [_D, _I, D, D, _D, _I, _D, _D, D, _I, _D,
+                                             ctypes.POINTER(_I)]
+        lib.ref_eo_mult_throughput.argtypes = [_D, D, _D, _D, _I, _I, _D]
+        self.L = None
+
+    def init(self, L):
+        rc = self.lib.ref_init(*[int(v) for v in L])
+        if rc:
+            raise RuntimeError(f"reference already initialised with another lattice than {L}")
+        self.L = list(L)
+
+    def _chk(self, rc, what):
+        if rc:
+            raise RuntimeError(f"{what} returned {rc}")
+
+    def wilson_full(self, u, mass, dag, f):
+        out = np.empty_like(f)
+        self._chk(self.lib.ref_wilson_mult(_p(u), mass, int(dag), _p(f), _p(out)), "ref_wilson_mult")
+        return out
+
+    def wilson_hop(self, u, mass, eo, dag, f):
+        out = np.empty_like(f)
+        self._chk(self.lib.ref_wilson_hop(_p(u), mass, int(eo), int(dag), _p(f), _p(out)), "ref_wilson_hop")
+        return out
+
+    def wilson_eo(self, u, mass, dag, f):
+        out = np.empty_like(f)
+        self._chk(self.lib.ref_wilson_eo_mult(_p(u), mass, int(dag), _p(f), _p(out)), "ref_wilson_eo_mult")
+        return out
+
+    def clover_full(self, u, mass, csw, dag, f):
+        out = np.empty_like(f)
+        self._chk(self.lib.ref_clover_mult(_p(u), mass, csw, int(dag), _p(f), _p(out)), "ref_clover_mult")
+        return out
+
+    def field_strength(self, u, mu, nu):
+        out = np.empty(18 * int(np.prod(self.L)))
+        self._chk(self.lib.ref_field_strength(_p(u), mu, nu, _p(out)), "ref_field_strength")
+        return out
+
+    def cg(self, u, op, mass, csw, b, prec, maxiter):
+        x = np.empty_like(b)
+        diff = ctypes.c_double()
+        it = ctypes.c_int()
+        ms = ctypes.c_double()
+        self._chk(self.lib.ref_cg_solve(_p(u), op, mass, csw, _p(b), _p(x), prec, maxiter,
+                                        ctypes.byref(diff), ctypes.byref(it), ctypes.byref(ms)),
+                  "ref_cg_solve")
+        return x, it.value, diff.value, ms.value
+
+    def multishift(self, u, op, mass, csw, b, shifts, prec, maxiter):
+        sh = np.ascontiguousarray(shifts, np.float64)
+        x = np.empty(b.size * sh.size)
+        diff = ctypes.c_double()
+        nc = ctypes.c_int()
+        self._chk(self.lib.ref_multishift_solve(_p(u), op, mass, csw, _p(b), sh.size, _p(sh), _p(x),
+                                                prec, maxiter, ctypes.byref(diff), ctypes.byref(nc)),
+                  "ref_multishift_solve")
+        return x.reshape(sh.size, b.size), nc.value, diff.value
+
+    def eo_mult_throughput(self, u, mass, f, nthreads, reps):
+        out = np.empty_like(f)
+        secs = ctypes.c_double()
+        self._chk(self.lib.ref_eo_mult_throughput(_p(u), mass, _p(f), _p(out), nthreads, reps,
+                                                  ctypes.byref(secs)), "ref_eo_mult_throughput")
+        return out, secs.value

@@ -1,0 +1,152 @@
+"""Wilson and clover operators on the GPU against the reference.
+
+Against the golden fixtures (the reference's own outputs) at every storage
+precision, against the C oracle at 8^3x16, and through size-independent
+identities at 24^3x48 (gamma5-hermiticity, the even-odd block structure,
+multi-RHS = single-RHS, FP32 vs FP64)."""
+import numpy as np
+import pytest
+
+import iroiro_b200 as ib
+from conftest import TOL_FP16, TOL_FP32, TOL_FP64, load_golden, rel
+
+pytestmark = pytest.mark.gpu
+
+PREC_TOL = [("double", TOL_FP64), ("single", TOL_FP32), ("half", TOL_FP16)]
+PAIRS = [(1, 2), (2, 0), (0, 1), (3, 0), (3, 1), (3, 2)]
+
+
+@pytest.fixture(scope="module", params=["4x4x4x4", "6x2x4x4"])
+def g(request):
+    d = load_golden(request.param)
+    d["ctx"] = ib.context(d["L"])
+    d["ctx"].upload_gauge(d["u"], force=True)
+    return d
+
+
+@pytest.mark.parametrize("prec,tol", PREC_TOL)
+@pytest.mark.parametrize("dag", [0, 1])
+def test_wilson_vs_reference(g, prec, tol, dag):
+    c, m = g["ctx"], float(g["mass"])
+    c.upload_gauge(g["u"])
+    assert rel(c.apply(ib.OP_WILSON_FULL, m, 0, dag, g["f_full"], prec), g[f"wilson_full_{dag}"]) < tol
+    assert rel(c.apply(ib.OP_WILSON_HOP_EO, m, 0, dag, g["f_half"], prec), g[f"hop_eo_{dag}"]) < tol
+    assert rel(c.apply(ib.OP_WILSON_HOP_OE, m, 0, dag, g["f_half"], prec), g[f"hop_oe_{dag}"]) < tol
+    assert rel(c.apply(ib.OP_WILSON_SCHUR_EE, m, 0, dag, g["f_half"], prec), g[f"wilson_eo_{dag}"]) < tol
+
+
+@pytest.mark.parametrize("prec,tol", PREC_TOL)
+@pytest.mark.parametrize("dag", [0, 1])
+def test_clover_vs_reference(g, prec, tol, dag):
+    c, m, csw = g["ctx"], float(g["mass"]), float(g["csw"])
+    c.upload_gauge(g["u"])
+    out = c.apply(ib.OP_CLOVER_FULL, m, csw, dag, g["f_full"], prec)
+    assert rel(out, g[f"clover_full_{dag}"]) < tol
+
+
+def test_field_strength_vs_reference(g):
+    c = g["ctx"]
+    c.upload_gauge(g["u"])
+    for mu, nu in PAIRS:
+        assert rel(c.field_strength(mu, nu), g[f"F_{mu}{nu}"]) < TOL_FP64
+
+
+def test_gamma5(g):
+    c = g["ctx"]
+    f = g["f_full"]
+    out = c.gamma5(f).reshape(-1, 4, 6)
+    ff = f.reshape(-1, 4, 6)
+    assert np.array_equal(out[:, 0], ff[:, 2]) and np.array_equal(out[:, 3], ff[:, 1])
+
+
+def test_python_mirror_classes(g):
+    u, m = g["u"], float(g["mass"])
+    ctx = g["ctx"]
+    D = ib.Dirac_Wilson(m, u, ctx=ctx)
+    assert rel(D.mult(g["f_full"]), g["wilson_full_0"]) < TOL_FP64
+    E = ib.Dirac_Wilson_EvenOdd(m, u, ctx=ctx)
+    assert rel(E.mult_dag(g["f_half"]), g["wilson_eo_1"]) < TOL_FP64
+    assert rel(E.mult_eo(g["f_half"]), g["hop_eo_0"]) < TOL_FP64
+    assert rel(E.mult_oe_dag(g["f_half"]), g["hop_eo_1"]) < TOL_FP64
+    C = ib.Dirac_Clover(D, float(g["csw"]), u, ctx=ctx)
+    assert rel(C.mult(g["f_full"]), g["clover_full_0"]) < TOL_FP64
+
+
+@pytest.mark.parametrize("L", [[8, 8, 8, 16], [4, 6, 2, 8]])
+def test_vs_oracle_port(port, L):
+    u = ib.synth_gauge(L, 0.25, 31, True)
+    V = int(np.prod(L))
+    f = ib.synth_gaussian(V, 32)
+    h = ib.synth_gaussian(V // 2, 33)
+    c = ib.context(L)
+    c.upload_gauge(u, force=True)
+    m = 0.5 / 0.124 - 4
+    for dag in (0, 1):
+        assert rel(c.apply(ib.OP_WILSON_FULL, m, 0, dag, f), port.wilson_full(L, u, m, dag, f)) < TOL_FP64
+        assert rel(c.apply(ib.OP_WILSON_SCHUR_EE, m, 0, dag, h), port.wilson_eo(L, u, m, dag, h)) < TOL_FP64
+        assert rel(c.apply(ib.OP_CLOVER_FULL, m, 1.0, dag, f), port.clover_full(L, u, m, 1.0, dag, f)) < TOL_FP64
+
+
+@pytest.fixture(scope="module")
+def big():
+    L = [24, 24, 24, 48]
+    V = int(np.prod(L))
+    u = ib.synth_gauge(L, 0.2, 41, True)
+    c = ib.context(L)
+    c.upload_gauge(u, force=True)
+    return dict(L=L, V=V, u=u, c=c, m=0.5 / 0.12 - 4, f=ib.synth_gaussian(V, 42),
+                g=ib.synth_gaussian(V, 43), h=ib.synth_gaussian(V // 2, 44), k=ib.synth_gaussian(V // 2, 45))
+
+
+@pytest.mark.parametrize("op,full,csw", [(ib.OP_WILSON_FULL, True, 0.0), (ib.OP_CLOVER_FULL, True, 1.0),
+                                         (ib.OP_WILSON_SCHUR_EE, False, 0.0),
+                                         (ib.OP_CLOVER_SCHUR_EE, False, 1.0)])
+def test_gamma5_hermiticity_24c48(big, op, full, csw):
+    """<g, D f> = <D^dag g, f> with D^dag = gamma5 D gamma5."""
+    c, m = big["c"], big["m"]
+    f, gg = (big["f"], big["g"]) if full else (big["h"], big["k"])
+    a = np.dot(gg, c.apply(op, m, csw, 0, f))
+    b = np.dot(c.apply(op, m, csw, 1, gg), f)
+    assert abs(a - b) < 1e-12 * abs(a)
+
+
+def test_even_odd_blocks_24c48(big):
+    """The full operators restricted to even-site sources reproduce the e/o
+    blocks: D [f_e, 0] = [A_ee f_e, -kappa H_oe f_e]."""
+    c, m, L, V = big["c"], big["m"], big["L"], big["V"]
+    Vh = V // 2
+    h = big["h"]
+    # scatter the even half field to lexicographic sites: site = 2*hs + ((y+z+t)&1)
+    hs = np.arange(Vh)
+    row = hs // (L[0] // 2)
+    y = row % L[1]; z = (row // L[1]) % L[2]; t = row // (L[1] * L[2])
+    esite = 2 * hs + ((y + z + t) & 1)
+    osite = 2 * hs + ((y + z + t + 1) & 1)
+    full = np.zeros((V, 24))
+    full[esite] = h.reshape(Vh, 24)
+    out = c.apply(ib.OP_WILSON_FULL, m, 0, 0, full.ravel()).reshape(V, 24)
+    assert rel(out[esite].ravel(), h) < TOL_FP64
+    assert rel(out[osite].ravel(), c.apply(ib.OP_WILSON_HOP_OE, m, 0, 0, h)) < TOL_FP64
+
+
+@pytest.mark.parametrize("prec,tol", [("single", TOL_FP32), ("half", TOL_FP16)])
+def test_low_precision_24c48(big, prec, tol):
+    c, m = big["c"], big["m"]
+    for op, f, csw in ((ib.OP_WILSON_SCHUR_EE, big["h"], 0.0), (ib.OP_CLOVER_SCHUR_EE, big["h"], 1.0),
+                       (ib.OP_WILSON_FULL, big["f"], 0.0)):
+        ref = c.apply(op, m, csw, 0, f, "double")
+        assert rel(c.apply(op, m, csw, 0, f, prec), ref) < tol
+
+
+@pytest.mark.parametrize("prec", ["double", "single", "half"])
+def test_multi_rhs_equals_single(prec):
+    L = [8, 8, 8, 8]
+    V = int(np.prod(L))
+    c = ib.context(L)
+    c.upload_gauge(ib.synth_gauge(L, 0.2, 51, True), force=True)
+    m = 0.1
+    fs = np.stack([ib.synth_gaussian(V // 2, 60 + r) for r in range(12)])
+    blk = c.apply(ib.OP_CLOVER_SCHUR_EE, m, 1.0, 0, fs.ravel(), prec, nrhs=12).reshape(12, -1)
+    for r in range(12):
+        one = c.apply(ib.OP_CLOVER_SCHUR_EE, m, 1.0, 0, fs[r], prec)
+        assert np.array_equal(blk[r], one)

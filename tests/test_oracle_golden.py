@@ -1,0 +1,60 @@
+"""The C restatement of the hot path against the reference's own outputs.
+
+The golden fixtures were produced by the reference's classes compiled from
+its sources (tests/golden/make_golden.py); this pins the oracle that the GPU
+parity tests use at sizes beyond the fixtures."""
+import numpy as np
+import pytest
+
+from conftest import TOL_FP64, TOL_SOL, rel
+
+PAIRS = [(1, 2), (2, 0), (0, 1), (3, 0), (3, 1), (3, 2)]
+
+
+@pytest.mark.parametrize("dag", [0, 1])
+def test_wilson_ops(port, golden, dag):
+    g = golden
+    L, u, m = g["L"], g["u"], float(g["mass"])
+    assert rel(port.wilson_full(L, u, m, dag, g["f_full"]), g[f"wilson_full_{dag}"]) < TOL_FP64
+    assert rel(port.wilson_hop(L, u, m, 0, dag, g["f_half"]), g[f"hop_eo_{dag}"]) < TOL_FP64
+    assert rel(port.wilson_hop(L, u, m, 1, dag, g["f_half"]), g[f"hop_oe_{dag}"]) < TOL_FP64
+    assert rel(port.wilson_eo(L, u, m, dag, g["f_half"]), g[f"wilson_eo_{dag}"]) < TOL_FP64
+
+
+def test_field_strength(port, golden):
+    g = golden
+    for mu, nu in PAIRS:
+        assert rel(port.field_strength(g["L"], g["u"], mu, nu), g[f"F_{mu}{nu}"]) < TOL_FP64
+
+
+@pytest.mark.parametrize("dag", [0, 1])
+def test_clover(port, golden, dag):
+    g = golden
+    out = port.clover_full(g["L"], g["u"], float(g["mass"]), float(g["csw"]), dag, g["f_full"])
+    assert rel(out, g[f"clover_full_{dag}"]) < TOL_FP64
+
+
+def test_gamma5_involution(port, golden):
+    f = golden["f_full"]
+    assert np.array_equal(port.gamma5(port.gamma5(f)), f)
+
+
+@pytest.mark.parametrize("name,op,src", [("wilson_full", 0, "f_full"), ("wilson_eo", 1, "f_half"),
+                                         ("clover_full", 2, "f_full")])
+def test_cg(port, golden_full, name, op, src):
+    g = golden_full
+    x, it, diff = port.cg(g["L"], g["u"], op, float(g["mass"]), float(g["csw"]), g[src], 1e-20, 5000)
+    assert it == int(g[f"cg_{name}_iters"])
+    assert rel(x, g[f"cg_{name}_x"]) < TOL_SOL
+    assert abs(diff - float(g[f"cg_{name}_diff"])) < 5e-2 * float(g[f"cg_{name}_diff"])
+
+
+@pytest.mark.parametrize("name,op,src", [("wilson_full", 0, "f_full"), ("wilson_eo", 1, "f_half")])
+def test_multishift(port, golden_full, name, op, src):
+    g = golden_full
+    x, nc, diff = port.multishift(g["L"], g["u"], op, float(g["mass"]), 0.0, g[src], g["shifts"],
+                                  1e-20, 5000)
+    assert nc == int(g[f"ms_{name}_nconv"])
+    for k in range(len(g["shifts"])):
+        assert rel(x[k], g[f"ms_{name}_x"][k]) < TOL_SOL
+    assert abs(diff - float(g[f"ms_{name}_diff"])) < 5e-2 * float(g[f"ms_{name}_diff"])
