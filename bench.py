@@ -78,24 +78,45 @@ class Clocks:
         self.device = device
         self.proc = None
 
-    def start(self):
+    def start(self, wait_s: float = 15.0):
+        """Starts sampling every 100 ms and waits for the first sample, so that
+        the sampler's start-up does not fall inside the timed region."""
+        import threading
+        self.lines = []
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+        first = threading.Event()
+
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.perf_counter(), line))
+                first.set()
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        first.wait(wait_s)
+
+    def mark(self):
+        self.t_begin = time.perf_counter()
 
     def stop(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t_end = time.perf_counter()
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        t0 = getattr(self, "t_begin", 0.0)
+        inside = [ln for t, ln in self.lines if t0 <= t <= t_end + 0.15]
+        out = "".join(inside or [ln for _, ln in self.lines[-3:]])
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in out.strip().splitlines():
@@ -183,24 +204,25 @@ def run_reference(args, world, rank):
     ref = oracle.ref()
     ref.init(L)
     threads = cpu_cores()
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 2)):
         ref.eo_mult_throughput(u, MASS, f, threads, 1)
     t = 0.0
-    for _ in range(args.steps):
+    nsteps = max(1, min(args.steps, 20))  # bounded sample: a step takes ~1 s on the host
+    for _ in range(nsteps):
         _, s = ref.eo_mult_throughput(u, MASS, f, threads, 1)
         t += s
-    steps_bytes = (2 * BYTES_HOP + BYTES_XPAY) * (V // 2) * threads * args.steps
+    steps_bytes = (2 * BYTES_HOP + BYTES_XPAY) * (V // 2) * threads * nsteps
     val = steps_bytes / t / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GB/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
+        "n_gpus": args.gpus, "steps": nsteps, "warmup": min(args.warmup, 2),
+        "ms_per_step": round(1e3 * t / nsteps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "lattice": L, "kappa": KAPPA,
                    "sample": f"{threads} concurrent Dirac_Wilson_EvenOdd::mult per step"},
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": threads,
                          "kind": "reference",
-                         "sample": f"{threads} threads x 1 mult per step, {args.steps} steps"},
+                         "sample": f"{threads} threads x 1 mult per step, {nsteps} steps (at most 20: one step takes about a second)"},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -242,7 +264,8 @@ def run_ours(args, world, rank, local):
     u = ib.synth_gauge(L, EPS, SEED + rank, gauge_transform=True)
     h = ib.synth_gaussian(Vh, SEED + 100 + rank)
     ctx = ib.Context(L, local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload_gauge(u, force=True)
     lib = ctx._lib
@@ -269,6 +292,7 @@ def run_ours(args, world, rank, local):
     clocks.start()
     barrier(world)
     torch.cuda.synchronize()
+    clocks.mark()
     for s, e in ev:
         flush.zero_()
         s.record(stream)
@@ -376,6 +400,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": 24 * 8 * Vh,
                 "d2h_bytes_per_step": 24 * 8 * Vh, "ms_per_step": round(e2e_ms / args.steps, 3)},
         "gpu_launches": 2 * args.steps,
+        "autotune": ctx.autotune_report(),
         "clocks": ck,
         "variants": variants,
         "solve": solve,
@@ -388,7 +413,7 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-solve", action="store_true")

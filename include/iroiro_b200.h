@@ -95,6 +95,11 @@ const char* iro_last_error(const iro_ctx* ctx);
    context creates its own; set_stream makes it use the caller's. */
 void* iro_ctx_get_stream(const iro_ctx* ctx);
 int iro_ctx_set_stream(iro_ctx* ctx, void* stream);
+/* The stencil autotuner's choices so far, as a JSON array (one object per
+   tuned launch shape: precision, reconstruction, dagger, epilogue, nrhs,
+   parities -> kernel variant, block size, time per launch in ms).  The
+   reference has no autotuner. */
+int iro_autotune_report(const iro_ctx* ctx, char* buf, int len);
 
 /* ---- gauge and clover ---------------------------------------------------- */
 /* Uploads a Format_G gauge field (18*4*V doubles) and keeps it resident in

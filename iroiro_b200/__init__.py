@@ -92,6 +92,7 @@ def _declare(L):
         "iro_last_error": (ctypes.c_char_p, [_VP]),
         "iro_ctx_get_stream": (_VP, [_VP]),
         "iro_ctx_set_stream": (I, [_VP, _VP]),
+        "iro_autotune_report": (I, [_VP, ctypes.c_char_p, I]),
         "iro_gauge_upload": (I, [_VP, _D]),
         "iro_clover_setup": (I, [_VP, D, D]),
         "iro_field_strength": (I, [_VP, I, I, _D]),
@@ -211,6 +212,13 @@ class Context:
     @property
     def stream(self) -> int:
         return int(self._lib.iro_ctx_get_stream(self.h) or 0)
+
+    def autotune_report(self) -> list:
+        """The stencil autotuner's choices (one dict per tuned launch shape)."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(self._lib.iro_autotune_report(self.h, buf, len(buf)), "iro_autotune_report")
+        return json.loads(buf.value.decode())
 
     def set_stream(self, stream_handle: int):
         self.check(self._lib.iro_ctx_set_stream(self.h, _VP(stream_handle)), "set_stream")

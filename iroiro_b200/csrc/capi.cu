@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -60,6 +61,10 @@ struct iro_ctx {
   void* h_pinned = nullptr;  // host mirror of state + done
 
   std::map<std::tuple<int, int, int, int>, DevField> ws;
+
+  // stencil autotuner: (prec, recon, dag, epilogue, nrhs, nparity) -> (variant, block cap)
+  std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> tuned;
+  std::map<std::tuple<int, int, int, int, int, int>, float> tuned_ms;
 };
 
 namespace {
@@ -216,7 +221,71 @@ HopLaunch base_launch(iro_ctx* c, int prec, bool dag, int nrhs) {
   L.max_blocks = c->max_blocks;
   L.skip = nullptr;
   L.red_mask = 0;
+  L.variant = 0;
+  L.block_cap = 256;
   return L;
+}
+
+// Launches the stencil with the variant and block size the autotuner picked
+// for this (precision, reconstruction, dagger, epilogue, nrhs, parities).
+// An untuned shape is timed once in every candidate configuration on the
+// caller's own fields (without reductions, so solver state is untouched; the
+// launch is idempotent) before the real launch; during stream capture the
+// default configuration is used.  IRO_HOP_VARIANT="<variant>,<block>" fixes
+// the choice.
+int launch_tuned(iro_ctx* c, HopLaunch L) {
+  auto key = std::make_tuple(L.prec, L.recon, int(L.dag), L.epi, L.nrhs, L.nparity);
+  cudaStream_t st = c->stream;
+  static const char* forced = std::getenv("IRO_HOP_VARIANT");
+  auto it = c->tuned.find(key);
+  if (forced) {
+    int v = 0, b = 256;
+    std::sscanf(forced, "%d,%d", &v, &b);
+    c->tuned[key] = {v & 3, b};
+    it = c->tuned.find(key);
+  }
+  if (it == c->tuned.end()) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      L.variant = 0;
+      L.block_cap = 256;
+      CK(launch_hop(L, st));
+      return IRO_OK;
+    }
+    HopLaunch T = L;
+    T.red_mask = 0;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    std::pair<int, int> pick{0, 256};
+    for (int v = 0; v < 4; ++v)
+      for (int b : {256, 128}) {
+        T.variant = v;
+        T.block_cap = b;
+        CK(launch_hop(T, st));  // warm-up
+        CK(cudaEventRecord(e0, st));
+        for (int i = 0; i < 3; ++i) CK(launch_hop(T, st));
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          pick = {v, b};
+        }
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tuned[key] = pick;
+    c->tuned_ms[key] = best / 3;
+    it = c->tuned.find(key);
+  }
+  L.variant = it->second.first;
+  L.block_cap = it->second.second;
+  CK(launch_hop(L, st));
+  return IRO_OK;
 }
 
 // out = op(in) on device fields.  `red`/`red_mask`, when given, attach a
@@ -254,7 +323,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       L.epi = EPI_SCALE;
       L.scale = -k;
       if (red) { L.red = *red; L.red_mask = red_mask; }
-      CK(launch_hop(L, st));
+      { int rt = launch_tuned(c, L); if (rt) return rt; }
     } break;
     case IRO_OP_CLOVER_HOP_OE_INV: {
       L.p0 = 1;
@@ -264,7 +333,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       L.clov[0] = clover_ptr(c, prec, 1, true);
       L.scale = -k;
       if (red) { L.red = *red; L.red_mask = red_mask; }
-      CK(launch_hop(L, st));
+      { int rt = launch_tuned(c, L); if (rt) return rt; }
     } break;
     case IRO_OP_WILSON_SCHUR_EE:
     case IRO_OP_CLOVER_SCHUR_EE: {
@@ -279,7 +348,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       L.epi = cl ? EPI_SCALE_CLOV : EPI_SCALE;
       if (cl) L.clov[0] = clover_ptr(c, prec, 1, true);
       L.scale = -k;
-      CK(launch_hop(L, st));
+      { int rt = launch_tuned(c, L); if (rt) return rt; }
       // out_e = [A_ee] f_e + kappa H_eo t_o  =  f - Deo(Doe f)
       HopLaunch L2 = base_launch(c, prec, dag, nrhs);
       L2.skip = skip;
@@ -291,7 +360,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       if (cl) L2.clov[0] = clover_ptr(c, prec, 0, false);
       L2.scale = k;
       if (red) { L2.red = *red; L2.red_mask = red_mask; }
-      CK(launch_hop(L2, st));
+      { int rt = launch_tuned(c, L2); if (rt) return rt; }
     } break;
     case IRO_OP_WILSON_FULL:
     case IRO_OP_CLOVER_FULL: {
@@ -307,7 +376,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       L.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
       L.scale = -k;
       if (red) { L.red = *red; L.red_mask = red_mask; }
-      CK(launch_hop(L, st));
+      { int rt = launch_tuned(c, L); if (rt) return rt; }
     } break;
   }
   return IRO_OK;
@@ -476,6 +545,27 @@ int iro_ctx_destroy(iro_ctx* c) {
 }
 
 const char* iro_last_error(const iro_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int iro_autotune_report(const iro_ctx* c, char* buf, int len) {
+  if (!c || !buf || len < 3) return IRO_BAD_ARG;
+  std::string s = "[";
+  for (const auto& kv : c->tuned) {
+    const auto& k = kv.first;
+    char item[256];
+    auto ms = c->tuned_ms.find(k);
+    std::snprintf(item, sizeof(item),
+                  "%s{\"prec\":%d,\"recon\":%d,\"dag\":%d,\"epilogue\":%d,\"nrhs\":%d,"
+                  "\"parities\":%d,\"variant\":%d,\"block\":%d,\"ms\":%.5f}",
+                  s.size() > 1 ? "," : "", std::get<0>(k), std::get<1>(k), std::get<2>(k),
+                  std::get<3>(k), std::get<4>(k), std::get<5>(k), kv.second.first, kv.second.second,
+                  ms == c->tuned_ms.end() ? -1.0 : double(ms->second));
+    s += item;
+  }
+  s += "]";
+  if (int(s.size()) + 1 > len) return IRO_BAD_ARG;
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return IRO_OK;
+}
 
 void* iro_ctx_get_stream(const iro_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
 

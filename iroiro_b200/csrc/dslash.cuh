@@ -138,8 +138,11 @@ struct HopParams {
   const int* skip;  // per-rhs converged flags, or null
 };
 
-template <int SP, int GP, int RECON, bool DAG, int EPI, int CP>
-__global__ void __launch_bounds__(256) hop_kernel(HopParams P) {
+// VAR bit 0: at least two 256-thread blocks per SM (register cap 128);
+// VAR bit 1: the four directions as a rolled loop (no hoisting of one
+// direction's loads over another's, fewer live registers).
+template <int SP, int GP, int RECON, bool DAG, int EPI, int CP, int VAR>
+__global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_kernel(HopParams P) {
   using R = typename SpinorIO<SP>::Real;
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;
@@ -157,10 +160,22 @@ __global__ void __launch_bounds__(256) hop_kernel(HopParams P) {
     Cx<R> acc[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = {R(0), R(0)};
-    hop_dir<0, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
-    hop_dir<1, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
-    hop_dir<2, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
-    hop_dir<3, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    if (VAR & 2) {
+#pragma unroll 1
+      for (int mu = 0; mu < 4; ++mu) {
+        switch (mu) {
+          case 0: hop_dir<0, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc); break;
+          case 1: hop_dir<1, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc); break;
+          case 2: hop_dir<2, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc); break;
+          default: hop_dir<3, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc); break;
+        }
+      }
+    } else {
+      hop_dir<0, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      hop_dir<1, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      hop_dir<2, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      hop_dir<3, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    }
     const R sc = R(P.scale);
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];

@@ -7,7 +7,7 @@
 
 namespace iro {
 
-template <int SP, int GP, int RECON, bool DAG, int EPI>
+template <int SP, int GP, int RECON, bool DAG, int EPI, int VAR>
 static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   HopParams P;
   P.g = L.g;
@@ -24,19 +24,29 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   P.red_mask = L.red_mask;
   P.red = L.red;
   P.skip = L.skip;
-  LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks);
+  LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks, L.block_cap);
   dim3 grid(c.grid, L.nparity);
-  hop_kernel<SP, GP, RECON, DAG, EPI, SP><<<grid, c.block, 0, st>>>(P);
+  hop_kernel<SP, GP, RECON, DAG, EPI, SP, VAR><<<grid, c.block, 0, st>>>(P);
   return cudaGetLastError();
+}
+
+template <int SP, int GP, int RECON, bool DAG, int EPI>
+static cudaError_t hop_var(const HopLaunch& L, cudaStream_t st) {
+  switch (L.variant & 3) {
+    case 0: return hop_go<SP, GP, RECON, DAG, EPI, 0>(L, st);
+    case 1: return hop_go<SP, GP, RECON, DAG, EPI, 1>(L, st);
+    case 2: return hop_go<SP, GP, RECON, DAG, EPI, 2>(L, st);
+    default: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
+  }
 }
 
 template <int SP, int RECON, bool DAG>
 static cudaError_t hop_epi(const HopLaunch& L, cudaStream_t st) {
   switch (L.epi) {
-    case EPI_SCALE: return hop_go<SP, SP, RECON, DAG, EPI_SCALE>(L, st);
-    case EPI_SCALE_CLOV: return hop_go<SP, SP, RECON, DAG, EPI_SCALE_CLOV>(L, st);
-    case EPI_XPAY: return hop_go<SP, SP, RECON, DAG, EPI_XPAY>(L, st);
-    case EPI_XPAY_CLOV: return hop_go<SP, SP, RECON, DAG, EPI_XPAY_CLOV>(L, st);
+    case EPI_SCALE: return hop_var<SP, SP, RECON, DAG, EPI_SCALE>(L, st);
+    case EPI_SCALE_CLOV: return hop_var<SP, SP, RECON, DAG, EPI_SCALE_CLOV>(L, st);
+    case EPI_XPAY: return hop_var<SP, SP, RECON, DAG, EPI_XPAY>(L, st);
+    case EPI_XPAY_CLOV: return hop_var<SP, SP, RECON, DAG, EPI_XPAY_CLOV>(L, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -33,7 +33,7 @@ struct LaunchCfg {
   int block;  // nrhs * 2^k, at most 256
   int grid;
 };
-LaunchCfg launch_cfg(int64_t vh, int nrhs, int max_blocks);
+LaunchCfg launch_cfg(int64_t vh, int nrhs, int max_blocks, int block_cap = 256);
 
 // ---- stencil ---------------------------------------------------------------
 struct HopLaunch {
@@ -53,6 +53,8 @@ struct HopLaunch {
   Reduce red;
   const int* skip;
   int max_blocks;
+  int variant;    // kernel variant (see hop_kernel), chosen by the autotuner
+  int block_cap;  // largest block size (128 or 256), chosen by the autotuner
 };
 cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st);
 

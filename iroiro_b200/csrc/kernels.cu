@@ -39,9 +39,10 @@ SpinorPtr DevField::all() const {
   return s;
 }
 
-LaunchCfg launch_cfg(int64_t vh, int nrhs, int max_blocks) {
+LaunchCfg launch_cfg(int64_t vh, int nrhs, int max_blocks, int block_cap) {
   int spb = 1;
-  while (nrhs * spb * 2 <= 256) spb *= 2;
+  const int cap = block_cap < nrhs ? nrhs : (block_cap > 256 ? 256 : block_cap);
+  while (nrhs * spb * 2 <= cap) spb *= 2;
   LaunchCfg c;
   c.block = nrhs * spb;
   int64_t need = (vh * nrhs + c.block - 1) / c.block;

@@ -70,7 +70,8 @@ int iterate(iro_ctx* c, int nrhs, int max_iter, bool use_graph, F body) {
   cudaStream_t st = stream(c);
   int* hdone = static_cast<int*>(pinned(c));
   cudaGraphExec_t exec = nullptr;
-  if (use_graph) {
+  // the legacy default stream cannot be captured: run the chunk eagerly there
+  if (use_graph && st != nullptr) {
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = body(kChunk);
@@ -253,6 +254,9 @@ extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double c
     f.x[k] = XS[k < nshift ? k : 0]->all();
     f.p[k] = PS[k < nshift ? k : 0]->all();
   }
+  // autotune the two operator launches outside the graph capture (scratch Q, S only)
+  RC(apply(c, op, mass, csw, false, *PS[0], *Q, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
   const MSState* dm = static_cast<const MSState*>(state(c));
   Reduce ralpha = reduce(c, ST_MS_ALPHA, max_iter);
   Reduce rr = reduce(c, ST_MS_R, max_iter);
@@ -347,6 +351,9 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   RC(convert(c, *R, *Rl));
   RC(convert(c, *R, *Pl));
   RC(axpby(c, 0.0, *Rl, 0.0, *Rl, *Xl));
+  // autotune the low-precision operator launches outside the graph capture
+  RC(apply(c, op, mass, csw, false, *Pl, *Ql, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, nullptr));
 
   const int* skip = done(c);
   Reduce ralpha = reduce(c, ST_CG_ALPHA, prm->max_iter);
@@ -364,7 +371,7 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
     return IRO_OK;
   };
   cudaGraphExec_t exec = nullptr;
-  if (prm->use_graph) {
+  if (prm->use_graph && st != nullptr) {
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int brc = body(kChunk);
