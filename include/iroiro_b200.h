@@ -142,6 +142,12 @@ int iro_field_download(iro_ctx* ctx, const iro_field* f, double* host);
    of in/out must match the operator. */
 int iro_dirac_apply_field(iro_ctx* ctx, int op, double mass, double csw, int dagger,
                           const iro_field* in, iro_field* out);
+/* Field::norm(), sqrt(sum x^2) over every real component, one value per
+   right-hand side into out[nrhs] (include/field.h:74-78); FP64 accumulation. */
+int iro_field_norm(iro_ctx* ctx, const iro_field* f, double* out);
+/* Field::operator*, the real inner product sum a_i b_i, one value per
+   right-hand side (lib/Fields/field.inl:58-62); FP64 accumulation. */
+int iro_field_dot(iro_ctx* ctx, const iro_field* a, const iro_field* b, double* out);
 
 /* ---- solvers -------------------------------------------------------------- */
 /* Mirrors SolverOutput (lib/Solver/solver.hpp:16-22). */

@@ -103,6 +103,8 @@ def _declare(L):
         "iro_field_upload": (I, [_VP, _VP, _D]),
         "iro_field_download": (I, [_VP, _VP, _D]),
         "iro_dirac_apply_field": (I, [_VP, I, D, D, I, _VP, _VP]),
+        "iro_field_norm": (I, [_VP, _VP, _D]),
+        "iro_field_dot": (I, [_VP, _VP, _VP, _D]),
         "iro_cg_solve": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
                              ctypes.POINTER(SolverOut)]),
         "iro_multishift_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, I,
@@ -253,6 +255,58 @@ class Context:
         out = np.empty(18 * self.V)
         self.check(self._lib.iro_field_strength(self.h, mu, nu, _ptr(out)), "iro_field_strength")
         return out
+
+
+class DeviceField:
+    """A spinor field resident on the GPU (iro_field): subset 0 even half,
+    1 odd half, 2 full lattice; nrhs right-hand sides in the device layout
+    of `prec`.  upload/download convert from/to Format_F host arrays."""
+
+    def __init__(self, ctx: Context, subset: int, prec="double", nrhs: int = 1):
+        self.ctx, self.subset, self.prec, self.nrhs = ctx, subset, _PREC[prec], nrhs
+        h = _VP()
+        ctx.check(ctx._lib.iro_field_create(ctx.h, subset, self.prec, nrhs, ctypes.byref(h)),
+                  "iro_field_create")
+        self.h = h
+
+    @property
+    def size(self) -> int:
+        return (24 if self.subset == 2 else 12) * self.ctx.V * self.nrhs
+
+    def upload(self, f):
+        f = _f64(f, self.size, "spinor")
+        self.ctx.check(self.ctx._lib.iro_field_upload(self.ctx.h, self.h, _ptr(f)), "iro_field_upload")
+        return self
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.size)
+        self.ctx.check(self.ctx._lib.iro_field_download(self.ctx.h, self.h, _ptr(out)),
+                       "iro_field_download")
+        return out
+
+    def norm(self) -> np.ndarray:
+        """Field::norm() per right-hand side (include/field.h:74-78)."""
+        out = np.empty(self.nrhs)
+        self.ctx.check(self.ctx._lib.iro_field_norm(self.ctx.h, self.h, _ptr(out)), "iro_field_norm")
+        return out
+
+    def dot(self, other: "DeviceField") -> np.ndarray:
+        """Field::operator* per right-hand side (lib/Fields/field.inl:58-62)."""
+        out = np.empty(self.nrhs)
+        self.ctx.check(self.ctx._lib.iro_field_dot(self.ctx.h, self.h, other.h, _ptr(out)),
+                       "iro_field_dot")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._lib.iro_field_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _contexts: dict = {}

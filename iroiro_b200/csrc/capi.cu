@@ -695,6 +695,30 @@ int iro_dirac_apply_field(iro_ctx* c, int op, double mass, double csw, int dagge
   return apply_dev(c, op, mass, csw, dagger != 0, in->f, out->f, nullptr, 0, nullptr);
 }
 
+int iro_field_norm(iro_ctx* c, const iro_field* f, double* out) {
+  if (!c || !f || !out) return fail(c, IRO_BAD_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  std::vector<double> n2;
+  int rc = norms_host(c, f->f, nullptr, n2, nullptr);
+  if (rc) return rc;
+  for (int r = 0; r < f->f.nrhs; ++r) out[r] = std::sqrt(n2[r]);
+  return IRO_OK;
+}
+
+int iro_field_dot(iro_ctx* c, const iro_field* a, const iro_field* b, double* out) {
+  if (!c || !a || !b || !out) return fail(c, IRO_BAD_ARG, "null argument");
+  if (a->f.subset != b->f.subset || a->f.prec != b->f.prec || a->f.nrhs != b->f.nrhs)
+    return fail(c, IRO_BAD_ARG, "dot: fields differ in subset, precision or nrhs");
+  CK(cudaSetDevice(c->device));
+  Reduce r = make_reduce(c, ST_NONE, 0);
+  CK(launch_dot(a->f.prec, a->f.sites(), a->f.nrhs, a->f.all(), b->f.all(), r, c->max_blocks,
+                c->stream));
+  CK(cudaMemcpyAsync(out, c->redout, sizeof(double) * a->f.nrhs, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return IRO_OK;
+}
+
 // ---- CG ------------------------------------------------------------------------------
 int iro_cg_solve(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
                  const double* b, double* x, int nrhs, iro_solver_out* out);

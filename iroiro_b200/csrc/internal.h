@@ -68,6 +68,9 @@ cudaError_t launch_convert(int pin, SpinorPtr in, int pout, SpinorPtr out, int64
 // sum |v|^2 (k=0) and, if w given, |w|^2 (k=1) per rhs with a stage update
 cudaError_t launch_norms(int prec, int64_t Vh, int nrhs, SpinorPtr v, const SpinorPtr* w,
                          const Reduce& red, int max_blocks, cudaStream_t st);
+// sum_i a_i b_i (real parts) per rhs
+cudaError_t launch_dot(int prec, int64_t sites, int nrhs, SpinorPtr a, SpinorPtr b,
+                       const Reduce& red, int max_blocks, cudaStream_t st);
 // CG: r = b - s, p = r; reduce |r|^2, |b|^2 (stage ST_CG_INIT)
 cudaError_t launch_cg_init(int prec, int64_t Vh, int nrhs, SpinorPtr b, SpinorPtr s, SpinorPtr r,
                            SpinorPtr p, const Reduce& red, int max_blocks, cudaStream_t st);

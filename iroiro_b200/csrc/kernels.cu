@@ -891,4 +891,30 @@ cudaError_t launch_mx_p(int plo, int64_t sites, int nrhs, SpinorPtr p, SpinorPtr
   return cudaGetLastError();
 }
 
+// ---- Field::operator* (lib/Fields/field.inl:58-62): sum_i a_i b_i per rhs ------------
+template <int SP>
+__global__ void __launch_bounds__(256) dot_kernel(int64_t n, int nrhs, SpinorPtr a, SpinorPtr b, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
+  double acc = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<R> av[12], bv[12];
+    SpinorIO<SP>::load(a, i, av);
+    SpinorIO<SP>::load(b, i, bv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc += double(av[k].re) * bv[k].re + double(av[k].im) * bv[k].im;
+  }
+  block_reduce_finish<1>(red, &acc, nrhs, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_dot(int prec, int64_t sites, int nrhs, SpinorPtr a, SpinorPtr b,
+                       const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(sites, nrhs, max_blocks);
+  const int64_t n = sites * nrhs;
+  if (prec == PREC_SINGLE) dot_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(n, nrhs, a, b, red);
+  else if (prec == PREC_HALF) dot_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(n, nrhs, a, b, red);
+  else dot_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(n, nrhs, a, b, red);
+  return cudaGetLastError();
+}
+
 }  // namespace iro
