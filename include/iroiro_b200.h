@@ -149,6 +149,24 @@ int iro_field_norm(iro_ctx* ctx, const iro_field* f, double* out);
    right-hand side (lib/Fields/field.inl:58-62); FP64 accumulation. */
 int iro_field_dot(iro_ctx* ctx, const iro_field* a, const iro_field* b, double* out);
 
+/* Field norm without any device allocation.  No counterpart in the
+   reference: it exists for callers that cannot call cudaMalloc, for instance
+   a host code that owns all device memory through its own pool with a fixed
+   budget, or that must keep its device footprint constant after set-up (the
+   context API above allocates contexts, staging buffers and workspaces).
+   Computes sqrt(sum d_in[i]^2) over n doubles of a device array the caller
+   owns (a Format_F field has 24 doubles per site) and writes it to the
+   caller's device double *d_out, on `stream` (a cudaStream_t; NULL for the
+   legacy default stream), without synchronizing.  It works on the current
+   device.  Limit: n <= 67108864 doubles (2796202 sites), the capacity of the
+   fixed 64 KiB scratch; larger n returns IRO_BAD_ARG and launches nothing.
+   The scratch is one file-scope __device__ array per GPU, held until the
+   process exits and shared by every call: calls that overlap on the GPU
+   (different streams or threads at the same time) race and give wrong
+   results.  The first call on a device looks up the array's device address
+   (cudaGetSymbolAddress); make that first call before any stream capture. */
+int iro_norm_noalloc(const double* d_in, int64_t n, double* d_out, void* stream);
+
 /* ---- solvers -------------------------------------------------------------- */
 /* Mirrors SolverOutput (lib/Solver/solver.hpp:16-22). */
 typedef struct {

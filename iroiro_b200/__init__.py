@@ -105,6 +105,7 @@ def _declare(L):
         "iro_dirac_apply_field": (I, [_VP, I, D, D, I, _VP, _VP]),
         "iro_field_norm": (I, [_VP, _VP, _D]),
         "iro_field_dot": (I, [_VP, _VP, _VP, _D]),
+        "iro_norm_noalloc": (I, [_VP, ctypes.c_int64, _VP, _VP]),
         "iro_cg_solve": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
                              ctypes.POINTER(SolverOut)]),
         "iro_multishift_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, I,
