@@ -230,6 +230,80 @@ def run_reference(args, world, rank):
     return 0
 
 
+def timed_solves(ctx, D, b, nrhs, torch, inners=("double", "single", "half"), prec=1e-20):
+    """Wall time of iro_cg_solve_field to a 1e-10 FP64 true residual for the
+    reference's FP64 CG and the mixed-precision CG (device-resident fields)."""
+    import iroiro_b200 as ib
+    sub = 0 if D.op in (ib.OP_WILSON_SCHUR_EE, ib.OP_CLOVER_SCHUR_EE) else 2
+    B = ib.DeviceField(ctx, sub, "double", nrhs).upload(b)
+    X = ib.DeviceField(ctx, sub, "double", nrhs)
+    res = {}
+    for inner in inners:
+        slv = ib.Solver_CG(prec, 20000, ib.Fopr_DdagD(D), inner=inner)
+        slv.solve_field(B, X)  # warm-up: workspaces, autotuning, graph capture
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outs, rc = slv.solve_field(B, X)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[inner] = {"ms": round(dt * 1e3, 2), "iterations": max(o.Iterations for o in outs),
+                      "true_residual_max": max(o.diff for o in outs),
+                      "reliable_updates": max(o.reliable_updates for o in outs),
+                      "converged": rc == ib.OK}
+    if "double" in res:
+        for k in res:
+            if k != "double":
+                res[k]["speedup_vs_fp64_cg"] = round(res["double"]["ms"] / res[k]["ms"], 2)
+    B.close()
+    X.close()
+    return res
+
+
+def batched_solves(torch, device):
+    """Batched configuration: 32^3x64 even-odd Wilson, kappa=0.12; the 12
+    spin-colour point sources at one seeded site solved together (one
+    launch sequence, every link load shared by the 12 right-hand sides) in
+    mixed precision, against 12 sequential plain FP64 CG solves; and
+    multishift CG with 12 shifts 1e-4..10 on one Gaussian source."""
+    import iroiro_b200 as ib
+    Lb = [32, 32, 32, 64]
+    Vb = int(np.prod(Lb))
+    ctx = ib.Context(Lb, device)
+    s = torch.cuda.current_stream()
+    ctx.set_stream(s.cuda_stream)
+    u = ib.synth_gauge(Lb, EPS, SEED + 7, gauge_transform=False)
+    ctx.upload_gauge(u, force=True)
+    D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+    site = int(np.random.default_rng(SEED).integers(Vb // 2))
+    src = ib.synth_point_sources(Vb // 2, site)
+    out = {"op": "e/o Wilson Schur 32^3x64, kappa=0.12, 12 point sources at half-site %d" % site}
+    # plain FP64 CG, one source after the other (what Qprop does, qprop.cpp:14-24)
+    seq = timed_solves(ctx, D, src[0], 1, torch, inners=("double",))
+    out["fp64_cg_one_source_ms"] = seq["double"]["ms"]
+    out["fp64_cg_12_sequential_ms"] = round(12 * seq["double"]["ms"], 2)
+    out["fp64_cg_iterations"] = seq["double"]["iterations"]
+    blk = timed_solves(ctx, D, src.ravel(), 12, torch, inners=("double", "single", "half"))
+    for k, v in blk.items():
+        v.pop("speedup_vs_fp64_cg", None)
+        v["speedup_vs_12_fp64_cg"] = round(out["fp64_cg_12_sequential_ms"] / v["ms"], 2)
+    out["block12"] = blk
+    # multishift, 12 shifts geometrically spaced 1e-4..10, one Gaussian source
+    shifts = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
+    g = ib.synth_gaussian(Vb // 2, SEED + 9)
+    ms = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 20000)
+    xs = []
+    ms.solve(xs, g, shifts)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    o = ms.solve(xs, g, shifts)
+    torch.cuda.synchronize()
+    out["multishift12"] = {"ms": round((time.perf_counter() - t0) * 1e3, 2), "iterations": o.Nconv,
+                           "max_true_residual": o.diff}
+    out["autotune"] = ctx.autotune_report()
+    ctx.close()
+    return out
+
+
 def cpu_baseline_leg():
     """The reference's own e/o mult on the host cores, a bounded sample."""
     import oracle
@@ -293,12 +367,14 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     clocks.mark()
+    torch.cuda.profiler.start()  # ncu --profile-from-start off captures exactly this region
     for s, e in ev:
         flush.zero_()
         s.record(stream)
         step()
         e.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     barrier(world)
     ck = clocks.stop()
     t_ms = sum(s.elapsed_time(e) for s, e in ev)
@@ -360,23 +436,16 @@ def run_ours(args, world, rank, local):
         lib.iro_field_destroy(a)
         lib.iro_field_destroy(b)
 
-    # time to a 1e-10 FP64 true residual, e/o Wilson-clover, FP64 CG vs mixed precision
+    # time to a 1e-10 FP64 true residual, e/o Wilson-clover, FP64 CG vs mixed
+    # precision; fields resident on the device (iro_cg_solve_field)
     solve = {}
     if not args.no_solve:
         D = ib.Dirac_Clover_EvenOdd(MASS, CSW, u, ctx=ctx)
-        for inner in ("double", "single", "half"):
-            slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner)
-            slv.solve_many(h, 1)  # warm-up (workspace allocation, graph capture)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            x, outs, rc = slv.solve_many(h, 1)
-            dt = time.perf_counter() - t0
-            solve[inner] = {"ms": round(dt * 1e3, 2), "iterations": outs[0].Iterations,
-                            "true_residual": outs[0].diff,
-                            "reliable_updates": outs[0].reliable_updates}
-        base = solve["double"]["ms"]
-        for k in ("single", "half"):
-            solve[k]["speedup_vs_fp64_cg"] = round(base / solve[k]["ms"], 2)
+        solve = timed_solves(ctx, D, h, 1, torch)
+        solve["op"] = "e/o Wilson-clover Schur 24^3x48, kappa=0.12, csw=1.0, one Gaussian source"
+    batched = {}
+    if not args.no_solve and not args.no_batched:
+        batched = batched_solves(torch, local)
 
     lib.iro_field_destroy(fin)
     lib.iro_field_destroy(fout)
@@ -404,6 +473,7 @@ def run_ours(args, world, rank, local):
         "clocks": ck,
         "variants": variants,
         "solve": solve,
+        "batched": batched,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
@@ -418,6 +488,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     world, rank, local = (1, 0, 0) if args.impl == "reference" and _env_int("WORLD_SIZE", 1) == 1 \
         else ((_env_int("WORLD_SIZE", 1), _env_int("RANK", 0), _env_int("LOCAL_RANK", 0))

@@ -201,6 +201,12 @@ typedef struct {
 int iro_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
                  const double* b, double* x, int nrhs, iro_solver_out* out);
 
+/* iro_cg_solve on device-resident fields: b and x are FP64 fields of the
+   operator's subset (full lattice, or the even half for the Schur operators)
+   with the same nrhs; no host traffic. */
+int iro_cg_solve_field(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
+                       const iro_field* b, iro_field* x, iro_solver_out* out);
+
 /* MultiShiftSolver_CG::solve for (D^dagger D + sigma_i) x_i = b
    (lib/Solver/multiShiftSolver_CG.cpp:95-185) in FP64: x_i = 0 start,
    convergence on shift 0 only, pruning of converged shifts by

@@ -108,6 +108,8 @@ def _declare(L):
         "iro_norm_noalloc": (I, [_VP, ctypes.c_int64, _VP, _VP]),
         "iro_cg_solve": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
                              ctypes.POINTER(SolverOut)]),
+        "iro_cg_solve_field": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _VP, _VP,
+                                   ctypes.POINTER(SolverOut)]),
         "iro_multishift_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, I,
                                         ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
         "iro_synth_gauge": (I, [L4, D, ctypes.c_uint64, I, _D]),
@@ -541,6 +543,19 @@ class Solver_CG:
         res = [SolverOutput(o.diff, o.iterations, o.timing_ms, "CG solver", o.reliable_updates,
                             o.operator_applies) for o in outs]
         return x, res, rc
+
+    def solve_field(self, b: "DeviceField", x: "DeviceField"):
+        """Solves on device-resident FP64 fields (all right-hand sides of b
+        together), without host traffic.  Returns ([SolverOutput], status)."""
+        D = self.fopr.D
+        D.ctx.upload_gauge(D.u)
+        outs = (SolverOut * b.nrhs)()
+        rc = D.ctx._lib.iro_cg_solve_field(D.ctx.h, D.op, D.mass, D.csw, ctypes.byref(self.params),
+                                           b.h, x.h, outs)
+        if rc not in (OK, NOT_CONVERGED):
+            D.ctx.check(rc, "iro_cg_solve_field")
+        return [SolverOutput(o.diff, o.iterations, o.timing_ms, "CG solver", o.reliable_updates,
+                             o.operator_applies) for o in outs], rc
 
     def solve(self, xq: np.ndarray, b: np.ndarray) -> SolverOutput:
         """Solver_CG::solve(Field& xq, const Field& b) (solver_CG.cpp:29-80)."""

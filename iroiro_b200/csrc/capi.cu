@@ -763,6 +763,7 @@ void* state(iro_ctx* c) { return c->state; }
 int* done(iro_ctx* c) { return c->done; }
 void* pinned(iro_ctx* c) { return c->h_pinned; }
 int device(iro_ctx* c) { return c->device; }
+DevField* field_dev(iro_field* f) { return f ? &f->f : nullptr; }
 bool op_is_full(int op) { return is_full(op); }
 int op_subset(int op) { return input_subset(op); }
 bool op_ok(int op) { return op_valid(op); }

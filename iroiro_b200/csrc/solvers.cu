@@ -36,6 +36,7 @@ int device(iro_ctx* c);
 bool op_is_full(int op);
 int op_subset(int op);
 bool op_ok(int op);
+DevField* field_dev(iro_field* f);
 }  // namespace host
 }  // namespace iro
 
@@ -112,18 +113,15 @@ int iterate(iro_ctx* c, int nrhs, int max_iter, bool use_graph, F body) {
 
 // FP64 CG on D^dag D, Solver_CG::solve (lib/Solver/solver_CG.cpp:29-80).
 int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
-              const double* b, double* x, int nrhs, iro_solver_out* out) {
+              const DevField* B, DevField* X, int nrhs, iro_solver_out* out) {
   const int sub = op_subset(op);
   const bool full = op_is_full(op);
   int rc = IRO_OK;
-  DevField* B = workspace(c, sub, PREC_DOUBLE, nrhs, 20, &rc); if (!B) return rc;
-  DevField* X = workspace(c, sub, PREC_DOUBLE, nrhs, 21, &rc); if (!X) return rc;
   DevField* R = workspace(c, sub, PREC_DOUBLE, nrhs, 22, &rc); if (!R) return rc;
   DevField* P = workspace(c, sub, PREC_DOUBLE, nrhs, 23, &rc); if (!P) return rc;
   DevField* S = workspace(c, sub, PREC_DOUBLE, nrhs, 24, &rc); if (!S) return rc;
   DevField* Q = workspace(c, sub, PREC_DOUBLE, nrhs, 25, &rc); if (!Q) return rc;
   cudaStream_t st = stream(c);
-  RC(import_field(c, b, full, *B));
   RC(axpby(c, 1.0, *B, 0.0, *B, *X));  // x0 = b (solver_CG.cpp:40)
   // CG state: target = GoalPrecision (scaled by |b|^2 in the init stage)
   std::vector<CGState> s0(nrhs);
@@ -164,7 +162,6 @@ int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* 
   std::vector<CGState> s1(nrhs);
   CK(cudaMemcpyAsync(s1.data(), state(c), sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  RC(export_field(c, *X, full, x));
   int status = IRO_OK;
   for (int r = 0; r < nrhs; ++r) {
     out[r].diff = std::sqrt(rn[r] / bn[r]);
@@ -180,22 +177,53 @@ int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* 
 }  // namespace
 
 int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
-             const double* b, double* x, int nrhs, iro_solver_out* out);
+             const DevField* B, DevField* X, int nrhs, iro_solver_out* out);
 
-extern "C" int iro_cg_solve(iro_ctx* c, int op, double mass, double csw,
-                            const iro_cg_params* prm, const double* b, double* x, int nrhs,
-                            iro_solver_out* out) {
-  if (!c || !prm || !b || !x || !out || nrhs < 1 || nrhs > 16 || !solver_op_ok(op) ||
-      prm->inner_prec < 0 || prm->inner_prec > 2 || !(prm->precision > 0.0))
-    return set_error(c, IRO_BAD_ARG, "bad CG arguments");
-  CK(cudaSetDevice(device(c)));
+static int cg_any(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+                  const DevField* B, DevField* X, int nrhs, iro_solver_out* out) {
   auto t0 = std::chrono::steady_clock::now();
-  int rc = prm->inner_prec == PREC_DOUBLE ? cg_double(c, op, mass, csw, prm, b, x, nrhs, out)
-                                          : cg_mixed(c, op, mass, csw, prm, b, x, nrhs, out);
+  int rc = prm->inner_prec == PREC_DOUBLE ? cg_double(c, op, mass, csw, prm, B, X, nrhs, out)
+                                          : cg_mixed(c, op, mass, csw, prm, B, X, nrhs, out);
   auto t1 = std::chrono::steady_clock::now();
   const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   for (int r = 0; r < nrhs; ++r) out[r].timing_ms = ms;
   return rc;
+}
+
+static bool cg_args_ok(const iro_cg_params* prm, int op) {
+  return prm && solver_op_ok(op) && prm->inner_prec >= 0 && prm->inner_prec <= 2 &&
+         prm->precision > 0.0;
+}
+
+extern "C" int iro_cg_solve(iro_ctx* c, int op, double mass, double csw,
+                            const iro_cg_params* prm, const double* b, double* x, int nrhs,
+                            iro_solver_out* out) {
+  if (!c || !b || !x || !out || nrhs < 1 || nrhs > 16 || !cg_args_ok(prm, op))
+    return set_error(c, IRO_BAD_ARG, "bad CG arguments");
+  CK(cudaSetDevice(device(c)));
+  const int sub = op_subset(op);
+  const bool full = op_is_full(op);
+  int rc = IRO_OK;
+  DevField* B = workspace(c, sub, PREC_DOUBLE, nrhs, 20, &rc); if (!B) return rc;
+  DevField* X = workspace(c, sub, PREC_DOUBLE, nrhs, 21, &rc); if (!X) return rc;
+  RC(import_field(c, b, full, *B));
+  rc = cg_any(c, op, mass, csw, prm, B, X, nrhs, out);
+  if (rc != IRO_OK && rc != IRO_NOT_CONVERGED) return rc;
+  int rc2 = export_field(c, *X, full, x);
+  return rc2 ? rc2 : rc;
+}
+
+extern "C" int iro_cg_solve_field(iro_ctx* c, int op, double mass, double csw,
+                                  const iro_cg_params* prm, const iro_field* b, iro_field* x,
+                                  iro_solver_out* out) {
+  const DevField* B = field_dev(const_cast<iro_field*>(b));
+  DevField* X = field_dev(x);
+  if (!c || !B || !X || !out || !cg_args_ok(prm, op) || B->prec != PREC_DOUBLE ||
+      X->prec != PREC_DOUBLE || B->nrhs != X->nrhs || B->subset != op_subset(op) ||
+      X->subset != op_subset(op) || B->data == X->data)
+    return set_error(c, IRO_BAD_ARG, "bad CG field arguments");
+  CK(cudaSetDevice(device(c)));
+  return cg_any(c, op, mass, csw, prm, B, X, B->nrhs, out);
 }
 
 // ---- multishift CG ---------------------------------------------------------------------
@@ -312,13 +340,11 @@ extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double c
 // declared only on the FP64 true residual.  The starting guess is x0 = b as
 // in Solver_CG (solver_CG.cpp:40).
 int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
-             const double* b, double* x, int nrhs, iro_solver_out* out) {
+             const DevField* B, DevField* X, int nrhs, iro_solver_out* out) {
   const int sub = op_subset(op);
   const bool full = op_is_full(op);
   const int pl = prm->inner_prec;
   int rc = IRO_OK;
-  DevField* B = workspace(c, sub, PREC_DOUBLE, nrhs, 20, &rc); if (!B) return rc;
-  DevField* X = workspace(c, sub, PREC_DOUBLE, nrhs, 21, &rc); if (!X) return rc;
   DevField* R = workspace(c, sub, PREC_DOUBLE, nrhs, 22, &rc); if (!R) return rc;
   DevField* S = workspace(c, sub, PREC_DOUBLE, nrhs, 24, &rc); if (!S) return rc;
   DevField* Q = workspace(c, sub, PREC_DOUBLE, nrhs, 25, &rc); if (!Q) return rc;
@@ -332,7 +358,6 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   int* hpin = static_cast<int*>(pinned(c));
   const double delta = prm->delta > 0.0 ? prm->delta : 0.1;
 
-  RC(import_field(c, b, full, *B));
   RC(axpby(c, 1.0, *B, 0.0, *B, *X));
   std::vector<CGState> hs(nrhs);
   for (auto& s : hs) {
@@ -464,7 +489,6 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   RC(norms(c, *R, B, rn, &bn));
   CK(cudaMemcpyAsync(hs.data(), state(c), sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  RC(export_field(c, *X, full, x));
   int status = IRO_OK;
   for (int r = 0; r < nrhs; ++r) {
     out[r].diff = std::sqrt(rn[r] / bn[r]);
