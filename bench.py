@@ -480,6 +480,39 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def kernel_only(args):
+    """Profiling driver: `steps` applications of one operator on device
+    fields inside a cudaProfilerStart/Stop range (after autotuning), for
+    `ncu --profile-from-start off`.  --kernel OP,PREC,NRHS with OP one of
+    wilson_eo, clover_eo, wilson_full; --lattice Lx,Ly,Lz,Lt."""
+    import ctypes
+    import torch
+    import iroiro_b200 as ib
+    opn, prec, nrhs = args.kernel.split(",")
+    nrhs = int(nrhs)
+    Lk = [int(v) for v in args.lattice.split(",")]
+    op = {"wilson_eo": ib.OP_WILSON_SCHUR_EE, "clover_eo": ib.OP_CLOVER_SCHUR_EE,
+          "wilson_full": ib.OP_WILSON_FULL}[opn]
+    sub = 2 if op == ib.OP_WILSON_FULL else 0
+    V = int(np.prod(Lk))
+    ctx = ib.Context(Lk, 0)
+    ctx.upload_gauge(ib.synth_gauge(Lk, EPS, SEED, gauge_transform=True), force=True)
+    a = ib.DeviceField(ctx, sub, prec, nrhs).upload(
+        ib.synth_gaussian((V if sub == 2 else V // 2) * nrhs, SEED + 3))
+    b = ib.DeviceField(ctx, sub, prec, nrhs)
+    lib = ctx._lib
+    for _ in range(3):
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, CSW, 0, a.h, b.h), "apply")
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for _ in range(args.steps):
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, CSW, 0, a.h, b.h), "apply")
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"kernel": args.kernel, "lattice": Lk, "autotune": ctx.autotune_report()}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -489,7 +522,11 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--kernel", default=None, help="profiling driver: OP,PREC,NRHS")
+    ap.add_argument("--lattice", default="24,24,24,48")
     args = ap.parse_args()
+    if args.kernel:
+        return kernel_only(args)
     world, rank, local = (1, 0, 0) if args.impl == "reference" and _env_int("WORLD_SIZE", 1) == 1 \
         else ((_env_int("WORLD_SIZE", 1), _env_int("RANK", 0), _env_int("LOCAL_RANK", 0))
               if args.impl == "reference" else dist_setup())

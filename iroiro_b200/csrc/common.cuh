@@ -222,6 +222,10 @@ struct SpinorIO<PREC_HALF> {
     float m = 0.f;
 #pragma unroll
     for (int k = 0; k < 12; ++k) m = fmaxf(m, fmaxf(fabsf(v[k].re), fabsf(v[k].im)));
+    // sites whose largest component is below the normal FP32 range are stored
+    // as zero: 1/m would overflow (0 * inf = NaN), and such values are far
+    // below FP16 resolution relative to any field they belong to
+    if (!(m >= 1e-37f)) m = 0.f;
     const float inv = (m > 0.f) ? 1.0f / m : 0.f;
     uint4* p = static_cast<uint4*>(s.data);
 #pragma unroll

@@ -78,6 +78,10 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
         s[r].rr = tot[r];
         const int it = s[r].iter;
         s[r].iter = it + 1;
+        if (!isfinite(s[r].rr)) {  // breakdown: stop rather than iterate to max_iter
+          R.done[r] = STOPPED;
+          continue;
+        }
         if (s[r].delta2 > 0.0) {
           // mixed precision: pause for an FP64 residual recomputation when
           // |r| fell by delta since the last one, or looks converged;
