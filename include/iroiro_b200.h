@@ -87,7 +87,9 @@ typedef struct iro_field iro_field;
 /* One context per lattice and device; it owns all device memory.  Replaces
    the geometry singletons CommonPrms::instance(Lattice)
    (lib/Main/commonPrms.cpp:22-65) and SiteIndex_EvenOdd
-   (lib/Geometry/siteIndex_EvenOdd.cpp:21-62).  Every extent must be even. */
+   (lib/Geometry/siteIndex_EvenOdd.cpp:21-62).  Every extent must be even
+   (the reference asserts Nx%2==0, siteIndex_EvenOdd.hpp:45) and the volume
+   a multiple of 64 (device arrays are blocked in groups of 32 sites). */
 int iro_ctx_create(const int L[4], int device, iro_ctx** ctx);
 int iro_ctx_destroy(iro_ctx* ctx);
 const char* iro_last_error(const iro_ctx* ctx);

@@ -485,7 +485,9 @@ int iro_ctx_create(const int L[4], int device, iro_ctx** out) {
   for (int d = 0; d < 4; ++d)
     if (L[d] < 2 || (L[d] & 1)) return IRO_BAD_ARG;
   const int64_t V = int64_t(L[0]) * L[1] * L[2] * L[3];
-  if (V / 2 > int64_t(1) << 30) return IRO_BAD_ARG;
+  // 32-bit element indices for up to 16 right-hand sides, and warp-blocked
+  // arrays whose half-lattice element counts are multiples of 32
+  if (V / 2 * kMaxRhs >= int64_t(1) << 31 || V % 64 != 0) return IRO_BAD_ARG;
   std::unique_ptr<iro_ctx> c(new iro_ctx());
   for (int d = 0; d < 4; ++d) c->L[d] = L[d];
   c->V = V;
@@ -496,6 +498,9 @@ int iro_ctx_create(const int L[4], int device, iro_ctx** out) {
   c->g.sy = c->g.Lxh;
   c->g.sz = c->g.Lxh * L[1];
   c->g.st = c->g.Lxh * L[1] * L[2];
+  c->g.dxh = make_fastdiv(uint32_t(c->g.Lxh));
+  c->g.dy = make_fastdiv(uint32_t(L[1]));
+  c->g.dz = make_fastdiv(uint32_t(L[2]));
   c->device = device;
   iro_ctx* cp = c.get();
   {

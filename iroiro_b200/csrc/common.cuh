@@ -2,29 +2,32 @@
 // lattice geometry of the even/odd-ordered half lattices, and the storage
 // formats of spinors, links and clover blocks in HBM.
 //
-// Device layouts (all structure-of-arrays, 16-byte chunks, so that a warp's
-// 32 lanes read 512 contiguous bytes per chunk):
+// Every field is stored warp-blocked ("array of structures of arrays"): the
+// element index i (a half-lattice site, or site*nrhs + rhs for several
+// right-hand sides) is split into a block of 32 (i >> 5) and a lane (i & 31),
+// and 16-byte chunk k of element i lives at
+//     ((i >> 5) * NCHUNK + k) * 32 + (i & 31)            [in 16-byte units]
+// so that a warp reading chunk k of 32 consecutive elements reads 512
+// contiguous bytes, and the chunks of one element sit at compile-time
+// offsets (k * 512 bytes) from one base address.
 //
-//  spinor, parity p, nrhs right-hand sides, Vh half-lattice sites:
-//    complex k = c + 3*s (the Format_F order, include/format_F.h:36-42)
-//    FP64: 12 chunks of double2 (one complex each)
-//    FP32:  6 chunks of float4  (complexes 2j, 2j+1)
-//    FP16:  3 chunks of 8 halves (complexes 4j..4j+3) + one FP32 norm per
-//           site: values are stored divided by the site's largest |real|
-//    chunk j of (site hs, rhs r) lives at chunk[j*Vh*nrhs + hs*nrhs + r]
-//
-//  links U_mu(x) of the sites x of parity p:
-//    [p][mu][chunk][Vh]; rows 0 and 1 only (reconstruct-12: row 2 =
-//    conj(row0 x row1)) or all three rows (FP64 only, for non-SU(3) input)
-//    FP64: 6 (or 9) double2 chunks, FP32: 3 float4 chunks,
-//    FP16: one 8-half chunk + one 4-half chunk (two arrays)
-//
-//  clover, parity p: two Hermitian 6x6 blocks per site acting on
-//    phi+ = (psi0+psi2, psi1+psi3) and phi- = (psi0-psi2, psi1-psi3)
-//    (the gamma5 eigenbasis of the Dirac-Pauli basis used by the reference,
-//    lib/Dirac_ops/wilsonLikeUtils.cpp:42-49); per block 6 real diagonal
+//  spinor (12 complex, k = c + 3*s, the Format_F order of include/format_F.h:36-42):
+//    FP64: 12 chunks of double2; FP32: 6 chunks of float4 (complexes 2j, 2j+1);
+//    FP16: 3 chunks of 8 halves + one FP32 norm per element (values are
+//          stored divided by the element's largest real component)
+//  links U_mu(x) of the sites x of parity p, element = site:
+//    [p][mu][blocked element]; rows 0 and 1 only (reconstruct-12: row 2 =
+//    conj(row0 x row1)) or all three rows (FP64, for non-SU(3) input)
+//    FP64: 6 (or 9) double2 chunks; FP32: 3 float4 chunks;
+//    FP16: one 8-half chunk + one 4-half chunk (two plain arrays)
+//  clover, parity p, element = site: two Hermitian 6x6 blocks acting on
+//    phi+ = (psi0+psi2, psi1+psi3) and phi- = (psi0-psi2, psi1-psi3), the
+//    gamma5 eigenbasis of the Dirac-Pauli basis used by the reference
+//    (lib/Dirac_ops/wilsonLikeUtils.cpp:42-49); per block 6 real diagonal
 //    entries and 15 complex upper-triangle entries = 36 reals
 //    FP64: 36 double2 chunks, FP32: 18 float4, FP16: 9 chunks of 8 halves
+// The element count of every array is a multiple of 32 (the context
+// requires the lattice volume to be a multiple of 64).
 #pragma once
 
 #include <cuda_fp16.h>
@@ -85,11 +88,34 @@ __device__ __forceinline__ Cx<R> mul_mi(Cx<R> a) {
 }
 
 // ---- geometry ------------------------------------------------------------------
+// n / d for 0 <= n < 2^31 by multiply-high (Granlund & Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994): l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1, q = (mulhi(n, m) + n) >> l.
+struct FastDiv {
+  uint32_t d, m, l;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{d, 0u, 0u};
+  if (d > 1) {
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    f.l = l;
+    f.m = uint32_t((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+  }
+  return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+  return f.d == 1 ? n : (__umulhi(n, f.m) + n) >> f.l;
+}
+
 struct Geom {
   int L[4];  // Lx, Ly, Lz, Lt (all even)
   int Lxh;   // Lx/2
   int Vh;    // half volume
   int sy, sz, st;  // half-site strides of y, z, t: Lxh, Lxh*Ly, Lxh*Ly*Lz
+  FastDiv dxh, dy, dz;  // division by Lxh, Ly, Lz
 };
 
 // Coordinates of half-site hs of parity p; the lexicographic site is
@@ -101,11 +127,11 @@ struct Coord {
 
 __device__ __forceinline__ Coord coord_of(const Geom& g, int hs, int p) {
   Coord c;
-  c.row = hs / g.Lxh;
+  c.row = int(fdiv(uint32_t(hs), g.dxh));
   const int xh = hs - c.row * g.Lxh;
-  const int yz = c.row / g.L[1];
+  const int yz = int(fdiv(uint32_t(c.row), g.dy));
   c.y = c.row - yz * g.L[1];
-  c.t = yz / g.L[2];
+  c.t = int(fdiv(uint32_t(yz), g.dz));
   c.z = yz - c.t * g.L[2];
   c.x = 2 * xh + ((c.y + c.z + c.t + p) & 1);
   return c;
@@ -137,13 +163,19 @@ enum Epilogue {
 
 enum RedBits { RED_OUT2 = 1, RED_X2 = 2, RED_XOUT = 4 };
 
+// ---- warp-blocked addressing -------------------------------------------------------
+// offset (in 16-byte units) of chunk 0 of element i in an array of NCHUNK chunks
+template <int NCHUNK>
+__host__ __device__ __forceinline__ int64_t blk0(int64_t i) {
+  return (i >> 5) * (NCHUNK * 32) + (i & 31);
+}
+
 // ---- spinor storage ------------------------------------------------------------
 enum Prec { PREC_DOUBLE = 0, PREC_SINGLE = 1, PREC_HALF = 2 };
 
 struct SpinorPtr {
-  void* data;   // chunk array
-  float* norm;  // FP16 only
-  int64_t stride;  // elements between chunks: Vh * nrhs
+  void* data;   // blocked chunk array
+  float* norm;  // FP16 only: one norm per element
 };
 
 template <int P>
@@ -155,17 +187,17 @@ struct SpinorIO<PREC_DOUBLE> {
   static constexpr int NCHUNK = 12;
   static constexpr int BYTES = 192;
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<double> v[12]) {
-    const double2* p = static_cast<const double2*>(s.data);
+    const double2* p = static_cast<const double2*>(s.data) + blk0<12>(i);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      double2 d = __ldg(p + k * s.stride + i);
+      double2 d = __ldg(p + 32 * k);
       v[k] = {d.x, d.y};
     }
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i, const Cx<double> v[12]) {
-    double2* p = static_cast<double2*>(s.data);
+    double2* p = static_cast<double2*>(s.data) + blk0<12>(i);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) p[k * s.stride + i] = make_double2(v[k].re, v[k].im);
+    for (int k = 0; k < 12; ++k) p[32 * k] = make_double2(v[k].re, v[k].im);
   }
 };
 
@@ -175,19 +207,19 @@ struct SpinorIO<PREC_SINGLE> {
   static constexpr int NCHUNK = 6;
   static constexpr int BYTES = 96;
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
-    const float4* p = static_cast<const float4*>(s.data);
+    const float4* p = static_cast<const float4*>(s.data) + blk0<6>(i);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      float4 d = __ldg(p + k * s.stride + i);
+      float4 d = __ldg(p + 32 * k);
       v[2 * k] = {d.x, d.y};
       v[2 * k + 1] = {d.z, d.w};
     }
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i, const Cx<float> v[12]) {
-    float4* p = static_cast<float4*>(s.data);
+    float4* p = static_cast<float4*>(s.data) + blk0<6>(i);
 #pragma unroll
     for (int k = 0; k < 6; ++k)
-      p[k * s.stride + i] = make_float4(v[2 * k].re, v[2 * k].im, v[2 * k + 1].re, v[2 * k + 1].im);
+      p[32 * k] = make_float4(v[2 * k].re, v[2 * k].im, v[2 * k + 1].re, v[2 * k + 1].im);
   }
 };
 
@@ -205,29 +237,35 @@ struct SpinorIO<PREC_HALF> {
   using Real = float;
   static constexpr int NCHUNK = 3;
   static constexpr int BYTES = 52;  // 48 bytes of FP16 + 4-byte norm
-  __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
-    const uint4* p = static_cast<const uint4*>(s.data);
-    const float n = __ldg(s.norm + i);
+  // the stored (normalised) values and the element's norm
+  __device__ __forceinline__ static float load_raw(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
+    const uint4* p = static_cast<const uint4*>(s.data) + blk0<3>(i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      uint4 d = __ldg(p + k * s.stride + i);
+      uint4 d = __ldg(p + 32 * k);
       float2 a = unpack_h2(d.x), b = unpack_h2(d.y), c = unpack_h2(d.z), e = unpack_h2(d.w);
-      v[4 * k + 0] = {a.x * n, a.y * n};
-      v[4 * k + 1] = {b.x * n, b.y * n};
-      v[4 * k + 2] = {c.x * n, c.y * n};
-      v[4 * k + 3] = {e.x * n, e.y * n};
+      v[4 * k + 0] = {a.x, a.y};
+      v[4 * k + 1] = {b.x, b.y};
+      v[4 * k + 2] = {c.x, c.y};
+      v[4 * k + 3] = {e.x, e.y};
     }
+    return __ldg(s.norm + i);
+  }
+  __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
+    const float n = load_raw(s, i, v);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) v[k] = n * v[k];
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i, const Cx<float> v[12]) {
     float m = 0.f;
 #pragma unroll
     for (int k = 0; k < 12; ++k) m = fmaxf(m, fmaxf(fabsf(v[k].re), fabsf(v[k].im)));
-    // sites whose largest component is below the normal FP32 range are stored
-    // as zero: 1/m would overflow (0 * inf = NaN), and such values are far
-    // below FP16 resolution relative to any field they belong to
+    // elements whose largest component is below the normal FP32 range are
+    // stored as zero: 1/m would overflow (0 * inf = NaN), and such values are
+    // far below FP16 resolution relative to any field they belong to
     if (!(m >= 1e-37f)) m = 0.f;
     const float inv = (m > 0.f) ? 1.0f / m : 0.f;
-    uint4* p = static_cast<uint4*>(s.data);
+    uint4* p = static_cast<uint4*>(s.data) + blk0<3>(i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       uint4 d;
@@ -235,7 +273,7 @@ struct SpinorIO<PREC_HALF> {
       d.y = pack_h2(v[4 * k + 1].re * inv, v[4 * k + 1].im * inv);
       d.z = pack_h2(v[4 * k + 2].re * inv, v[4 * k + 2].im * inv);
       d.w = pack_h2(v[4 * k + 3].re * inv, v[4 * k + 3].im * inv);
-      p[k * s.stride + i] = d;
+      p[32 * k] = d;
     }
     s.norm[i] = m;
   }
@@ -243,8 +281,8 @@ struct SpinorIO<PREC_HALF> {
 
 // ---- link storage -------------------------------------------------------------------
 struct GaugePtr {
-  const void* a;  // main chunk array  [p][mu][chunk][Vh]
-  const void* b;  // FP16 second array [p][mu][Vh] (4 halves)
+  const void* a;  // main chunk array  [p][mu][blocked site]
+  const void* b;  // FP16 second array [p][mu][site] (4 halves)
   int64_t Vh;
 };
 
@@ -260,6 +298,12 @@ __device__ __forceinline__ void reconstruct_row2(Su3<R>& U) {
   U.e[2][2] = conjx(U.e[0][0] * U.e[1][1] - U.e[0][1] * U.e[1][0]);
 }
 
+// offset (16-byte units) of chunk 0 of the link of site i, direction mu, parity p
+template <int NCHUNK>
+__host__ __device__ __forceinline__ int64_t link0(int64_t Vh, int p, int mu, int64_t i) {
+  return int64_t(p * 4 + mu) * Vh * NCHUNK + blk0<NCHUNK>(i);
+}
+
 template <int P, int RECON>
 struct GaugeIO;
 
@@ -269,10 +313,10 @@ struct GaugeIO<PREC_DOUBLE, RECON> {
   static constexpr int NCHUNK = RECON / 2;
   static constexpr int BYTES = RECON * 8;
   __device__ __forceinline__ static void load(const GaugePtr& g, int p, int mu, int64_t i, Su3<double>& U) {
-    const double2* q = static_cast<const double2*>(g.a) + int64_t(p * 4 + mu) * NCHUNK * g.Vh + i;
+    const double2* q = static_cast<const double2*>(g.a) + link0<NCHUNK>(g.Vh, p, mu, i);
 #pragma unroll
     for (int k = 0; k < NCHUNK; ++k) {
-      double2 d = __ldg(q + k * g.Vh);
+      double2 d = __ldg(q + 32 * k);
       U.e[k / 3][k % 3] = {d.x, d.y};
     }
     if (RECON == 12) reconstruct_row2(U);
@@ -285,8 +329,8 @@ struct GaugeIO<PREC_SINGLE, 12> {
   static constexpr int NCHUNK = 3;
   static constexpr int BYTES = 48;
   __device__ __forceinline__ static void load(const GaugePtr& g, int p, int mu, int64_t i, Su3<float>& U) {
-    const float4* q = static_cast<const float4*>(g.a) + int64_t(p * 4 + mu) * 3 * g.Vh + i;
-    float4 a = __ldg(q), b = __ldg(q + g.Vh), c = __ldg(q + 2 * g.Vh);
+    const float4* q = static_cast<const float4*>(g.a) + link0<3>(g.Vh, p, mu, i);
+    float4 a = __ldg(q), b = __ldg(q + 32), c = __ldg(q + 64);
     U.e[0][0] = {a.x, a.y};
     U.e[0][1] = {a.z, a.w};
     U.e[0][2] = {b.x, b.y};
@@ -326,7 +370,7 @@ struct CloverBlock {
 };
 
 struct CloverPtr {
-  const void* data;  // [chunk][Vh]
+  const void* data;  // blocked chunk array of one parity
   int64_t Vh;
 };
 
@@ -338,18 +382,18 @@ struct CloverIO<PREC_DOUBLE> {
   using Real = double;
   static constexpr int BYTES = 576;
   __device__ __forceinline__ static void load(const CloverPtr& c, int64_t i, CloverBlock<double> B[2]) {
-    const double2* q = static_cast<const double2*>(c.data) + i;
+    const double2* q = static_cast<const double2*>(c.data) + blk0<36>(i);
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        double2 d = __ldg(q + (b * 18 + k) * c.Vh);
+        double2 d = __ldg(q + 32 * (b * 18 + k));
         B[b].d[2 * k] = d.x;
         B[b].d[2 * k + 1] = d.y;
       }
 #pragma unroll
       for (int k = 0; k < 15; ++k) {
-        double2 d = __ldg(q + (b * 18 + 3 + k) * c.Vh);
+        double2 d = __ldg(q + 32 * (b * 18 + 3 + k));
         B[b].o[k] = {d.x, d.y};
       }
     }
@@ -361,11 +405,11 @@ struct CloverIO<PREC_SINGLE> {
   using Real = float;
   static constexpr int BYTES = 288;
   __device__ __forceinline__ static void load(const CloverPtr& c, int64_t i, CloverBlock<float> B[2]) {
-    const float4* q = static_cast<const float4*>(c.data) + i;
+    const float4* q = static_cast<const float4*>(c.data) + blk0<18>(i);
     float v[72];
 #pragma unroll
     for (int k = 0; k < 18; ++k) {
-      float4 d = __ldg(q + k * c.Vh);
+      float4 d = __ldg(q + 32 * k);
       v[4 * k] = d.x;
       v[4 * k + 1] = d.y;
       v[4 * k + 2] = d.z;
@@ -386,11 +430,11 @@ struct CloverIO<PREC_HALF> {
   using Real = float;
   static constexpr int BYTES = 144;
   __device__ __forceinline__ static void load(const CloverPtr& c, int64_t i, CloverBlock<float> B[2]) {
-    const uint4* q = static_cast<const uint4*>(c.data) + i;
+    const uint4* q = static_cast<const uint4*>(c.data) + blk0<9>(i);
     float v[72];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      uint4 d = __ldg(q + k * c.Vh);
+      uint4 d = __ldg(q + 32 * k);
       float2 a = unpack_h2(d.x), b = unpack_h2(d.y), e = unpack_h2(d.z), f = unpack_h2(d.w);
       v[8 * k] = a.x; v[8 * k + 1] = a.y; v[8 * k + 2] = b.x; v[8 * k + 3] = b.y;
       v[8 * k + 4] = e.x; v[8 * k + 5] = e.y; v[8 * k + 6] = f.x; v[8 * k + 7] = f.y;

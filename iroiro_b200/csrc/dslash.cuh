@@ -96,20 +96,38 @@ __device__ __forceinline__ void su3_dag_mul(const Su3<R>& U, const Cx<R> h[6], C
   }
 }
 
+// Neighbour spinor projected to a half spinor.  FP16 elements are projected
+// from their stored (normalised) values and the element norm is applied to
+// the 6 projected complexes instead of the 12 loaded ones.
+template <int MU, int S, int SP>
+__device__ __forceinline__ void load_project(const SpinorPtr& in, int i,
+                                             Cx<typename SpinorIO<SP>::Real> h[6]) {
+  using R = typename SpinorIO<SP>::Real;
+  Cx<R> f[12];
+  if constexpr (SP == PREC_HALF) {
+    const float n = SpinorIO<PREC_HALF>::load_raw(in, i, f);
+    project<MU, S, R>(f, h);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) h[k] = n * h[k];
+  } else {
+    SpinorIO<SP>::load(in, i, f);
+    project<MU, S, R>(f, h);
+  }
+}
+
 // Forward (x+mu) and backward (x-mu) contributions of direction MU.
 template <int MU, bool DAG, int SP, int GP, int RECON>
 __device__ __forceinline__ void hop_dir(const GaugePtr& gauge, const SpinorPtr& in, int p,
-                                        int64_t hs, const int nb[8], int nrhs, int r,
+                                        int hs, const int nb[8], int nrhs, int r,
                                         Cx<typename SpinorIO<SP>::Real> acc[12]) {
   using R = typename SpinorIO<SP>::Real;
-  Cx<R> f[12], h[6], g[6];
+  Cx<R> h[6], g[6];
   // forward: (1 - g_mu) U_mu(x) psi(x+mu)   [dagger: (1 + g_mu)]
   {
     Su3<R> U;
     GaugeIO<GP, RECON>::load(gauge, p, MU, hs, U);
-    SpinorIO<SP>::load(in, int64_t(nb[2 * MU]) * nrhs + r, f);
     constexpr int S = DAG ? -1 : 1;
-    project<MU, S, R>(f, h);
+    load_project<MU, S, SP>(in, nb[2 * MU] * nrhs + r, h);
     su3_mul(U, h, g);
     reconstruct<MU, S, R>(acc, g);
   }
@@ -117,9 +135,8 @@ __device__ __forceinline__ void hop_dir(const GaugePtr& gauge, const SpinorPtr& 
   {
     Su3<R> U;
     GaugeIO<GP, RECON>::load(gauge, 1 - p, MU, nb[2 * MU + 1], U);
-    SpinorIO<SP>::load(in, int64_t(nb[2 * MU + 1]) * nrhs + r, f);
     constexpr int S = DAG ? 1 : -1;
-    project<MU, S, R>(f, h);
+    load_project<MU, S, SP>(in, nb[2 * MU + 1] * nrhs + r, h);
     su3_dag_mul(U, h, g);
     reconstruct<MU, S, R>(acc, g);
   }
@@ -147,12 +164,13 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_kernel(HopParams P
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;
   const int nrhs = P.nrhs;
-  const int64_t nthreads = int64_t(P.g.Vh) * nrhs;
+  const int nthreads = P.g.Vh * nrhs;  // < 2^31, checked at context creation
   double red[3] = {0.0, 0.0, 0.0};
-  for (int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; tid < nthreads;
-       tid += int64_t(gridDim.x) * blockDim.x) {
-    const int hs = int(tid / nrhs);
-    const int r = int(tid - int64_t(hs) * nrhs);
+  // the grid stride is a multiple of nrhs, so each thread keeps one rhs
+  const int r = (nrhs == 1) ? 0 : int((blockIdx.x * blockDim.x + threadIdx.x) % unsigned(nrhs));
+  for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < nthreads;
+       tid += gridDim.x * blockDim.x) {
+    const int hs = (nrhs == 1) ? tid : int(unsigned(tid) / unsigned(nrhs));
     if (P.skip && P.skip[r]) continue;
     const Coord c = coord_of(P.g, hs, p);
     int nb[8];

@@ -16,18 +16,13 @@ int spinor_nchunk(int prec) {
 }
 
 SpinorPtr DevField::half(int p) const {
-  // full fields interleave the parities inside each chunk: [chunk][p][Vh*nrhs]
+  // full fields store the even half, then the odd half (Vh*nrhs elements each,
+  // a multiple of 32, so the two halves are whole warp blocks)
   SpinorPtr s;
   const int64_t per = Vh * nrhs;
-  if (subset == 2) {
-    s.data = static_cast<char*>(data) + p * per * 16;
-    s.norm = norm ? norm + p * per : nullptr;
-    s.stride = 2 * per;
-  } else {
-    s.data = data;
-    s.norm = norm;
-    s.stride = per;
-  }
+  const int64_t off = (subset == 2 && p == 1) ? per : 0;
+  s.data = static_cast<char*>(data) + off * spinor_nchunk(prec) * 16;
+  s.norm = norm ? norm + off : nullptr;
   return s;
 }
 
@@ -35,7 +30,6 @@ SpinorPtr DevField::all() const {
   SpinorPtr s;
   s.data = data;
   s.norm = norm;
-  s.stride = (subset == 2 ? 2 : 1) * Vh * nrhs;
   return s;
 }
 
@@ -483,12 +477,12 @@ __global__ void import_gauge_kernel(Geom g, const double* raw, GaugeArrays ga,
       for (int b = 0; b < 3; ++b) U.e[a][b] = {u[2 * (3 * a + b)], u[2 * (3 * a + b) + 1]};
     const int64_t base = int64_t(p * 4 + mu);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) ga.d12[(base * 6 + k) * Vh + hs] = make_double2(U.e[k / 3][k % 3].re, U.e[k / 3][k % 3].im);
+    for (int k = 0; k < 6; ++k) ga.d12[link0<6>(Vh, p, mu, hs) + 32 * k] = make_double2(U.e[k / 3][k % 3].re, U.e[k / 3][k % 3].im);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) ga.d18[(base * 9 + k) * Vh + hs] = make_double2(U.e[k / 3][k % 3].re, U.e[k / 3][k % 3].im);
-    ga.s12[(base * 3 + 0) * Vh + hs] = make_float4(U.e[0][0].re, U.e[0][0].im, U.e[0][1].re, U.e[0][1].im);
-    ga.s12[(base * 3 + 1) * Vh + hs] = make_float4(U.e[0][2].re, U.e[0][2].im, U.e[1][0].re, U.e[1][0].im);
-    ga.s12[(base * 3 + 2) * Vh + hs] = make_float4(U.e[1][1].re, U.e[1][1].im, U.e[1][2].re, U.e[1][2].im);
+    for (int k = 0; k < 9; ++k) ga.d18[link0<9>(Vh, p, mu, hs) + 32 * k] = make_double2(U.e[k / 3][k % 3].re, U.e[k / 3][k % 3].im);
+    ga.s12[link0<3>(Vh, p, mu, hs)] = make_float4(U.e[0][0].re, U.e[0][0].im, U.e[0][1].re, U.e[0][1].im);
+    ga.s12[link0<3>(Vh, p, mu, hs) + 32] = make_float4(U.e[0][2].re, U.e[0][2].im, U.e[1][0].re, U.e[1][0].im);
+    ga.s12[link0<3>(Vh, p, mu, hs) + 64] = make_float4(U.e[1][1].re, U.e[1][1].im, U.e[1][2].re, U.e[1][2].im);
     uint4 ha;
     ha.x = pack_h2(float(U.e[0][0].re), float(U.e[0][0].im));
     ha.y = pack_h2(float(U.e[0][1].re), float(U.e[0][1].im));
@@ -691,12 +685,12 @@ __device__ void store_block(const CloverArrays& ca, bool inverse, int p, int64_t
     }
   void* const* arr = inverse ? ca.Ainv[0] : ca.A[0];
   double2* d = static_cast<double2*>(arr[p]);
-  for (int k = 0; k < 18; ++k) d[(blk * 18 + k) * Vh + hs] = make_double2(v[2 * k], v[2 * k + 1]);
+  for (int k = 0; k < 18; ++k) d[blk0<36>(hs) + 32 * (blk * 18 + k)] = make_double2(v[2 * k], v[2 * k + 1]);
   float* fptr = reinterpret_cast<float*>(static_cast<float4*>((inverse ? ca.Ainv[1] : ca.A[1])[p]));
   // FP32: 18 float4 chunks over both blocks, values v_all[36*blk + j]
   for (int q = 0; q < 9; ++q) {
     float4 f4 = make_float4(float(v[4 * q]), float(v[4 * q + 1]), float(v[4 * q + 2]), float(v[4 * q + 3]));
-    reinterpret_cast<float4*>(fptr)[(blk * 9 + q) * Vh + hs] = f4;
+    reinterpret_cast<float4*>(fptr)[blk0<18>(hs) + 32 * (blk * 9 + q)] = f4;
   }
   uint4* h = static_cast<uint4*>((inverse ? ca.Ainv[2] : ca.A[2])[p]);
   // FP16: 9 chunks of 8 halves over both blocks: block 0 owns values 0..35,
@@ -707,7 +701,7 @@ __device__ void store_block(const CloverArrays& ca, bool inverse, int p, int64_t
     const int gidx = 36 * blk + j;
     const int q = gidx / 8, w = gidx % 8;
     __half hv = __float2half_rn(float(v[j]));
-    hs16[((int64_t(q) * Vh + hs) * 8) + w] = *reinterpret_cast<unsigned short*>(&hv);
+    hs16[(blk0<9>(hs) + 32 * q) * 8 + w] = *reinterpret_cast<unsigned short*>(&hv);
   }
 }
 
