@@ -219,6 +219,62 @@ int iro_multishift_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const
                             int nshift, const double* shifts, double* x, double precision,
                             int max_iter, iro_solver_out* out, int* nconv);
 
+/* ---- learned preconditioner and flexible GCR --------------------------------
+   No counterpart in the reference (its solvers are CG, BiCGStab and
+   multishift CG, lib/Solver/solver_Factory.cpp:10-45).  A gauge-equivariant
+   network of parallel-transport convolution layers on the full lattice:
+     out_o(x) = sum_{d=0..8} sum_i W_d[o][i] (T_d in_i)(x),
+   T_0 = 1, T_{+mu} f(x) = U_mu(x) f(x+mu), T_{-mu} f(x) = U_mu(x-mu)^dag f(x-mu),
+   channels are colour vectors (a spinor is 4 channels, one per spin), the
+   channel mixing runs on the tensor cores (BF16 weights and operands, FP32
+   accumulation), the transports on the CUDA cores in FP32.  The links are the
+   resident gauge field (which must be SU(3)). */
+typedef struct iro_ptc iro_ptc;
+
+/* widths[0..nlayers]; widths[0] = widths[nlayers] = 4, others 4, 8 or 16. */
+int iro_ptc_create(iro_ctx* ctx, int nlayers, const int* widths, iro_ptc** net);
+int iro_ptc_destroy(iro_ptc* net);
+/* Layer weights W_d[o][i], complex, (re, im) interleaved, [9][cout][cin]. */
+int iro_ptc_set_weights(iro_ptc* net, int layer, const float* w);
+/* out = N(in) for full-lattice spinors: host Format_F arrays (24*V doubles),
+   or device fields (subset full, FP32 or FP64, one rhs).  The links are those
+   resident in `ctx`, which must have the lattice the network was built for;
+   one network serves every gauge field of that lattice. */
+int iro_ptc_apply(iro_ctx* ctx, iro_ptc* net, const double* in, double* out);
+int iro_ptc_apply_field(iro_ctx* ctx, iro_ptc* net, const iro_field* in, iro_field* out);
+/* Training: loss = |N(in) - target|^2 / |target|^2 and, if grad is not
+   NULL, dloss/dW of every layer (complex, layers concatenated in the layout of
+   iro_ptc_set_weights).  Forward and backward run on the device. */
+int iro_ptc_loss_grad(iro_ctx* ctx, iro_ptc* net, const iro_field* in, const iro_field* target,
+                      double* loss, float* grad);
+
+typedef struct {
+  double precision; /* stop when |b - A x|^2 / |b|^2 < precision (FP64 true residual) */
+  int max_iter;
+  int nkrylov;      /* directions kept before a restart (1..16) */
+  double delta;     /* restart when the iterated |r| fell by delta; <= 0: 0.1 */
+} iro_gcr_params;
+
+typedef struct {
+  double diff;         /* final FP64 true residual |b - A x| / |b| */
+  int iterations;      /* GCR iterations (plus fallback CG iterations), -1 if not converged */
+  double timing_ms;
+  int restarts;        /* FP64 residual recomputations */
+  int fallback;        /* 1 if the solve stalled and finished with mixed-precision CG */
+  int precond_applies; /* network applications */
+} iro_gcr_out;
+
+/* Flexible GCR for (D^dagger D) x = b on the full lattice (op
+   IRO_OP_WILSON_FULL or IRO_OP_CLOVER_FULL), right-preconditioned by `net`
+   (NULL: no preconditioner).  Inner iterations in FP32, the solution and the
+   restarted residual in FP64; convergence is declared on the FP64 true
+   residual.  When two restart cycles in a row fail to reduce the residual by
+   4x, the solve finishes with the mixed-precision reliable-update CG.  b and x
+   are FP64 full-lattice device fields, x0 = 0. */
+int iro_gcr_solve_field(iro_ctx* ctx, int op, double mass, double csw, const iro_ptc* net,
+                        const iro_gcr_params* prm, const iro_field* b, iro_field* x,
+                        iro_gcr_out* out);
+
 /* ---- synthetic inputs (host) ---------------------------------------------- */
 /* Seeded SU(3) field U = exp(i eps H), H = sum theta_a lambda_a / 2,
    theta_a ~ N(0,1), projected onto SU(3); optionally followed by a random

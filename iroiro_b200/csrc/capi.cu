@@ -769,6 +769,10 @@ int* done(iro_ctx* c) { return c->done; }
 void* pinned(iro_ctx* c) { return c->h_pinned; }
 int device(iro_ctx* c) { return c->device; }
 DevField* field_dev(iro_field* f) { return f ? &f->f : nullptr; }
+const Geom& geom(iro_ctx* c) { return c->g; }
+GaugePtr gauge_single(iro_ctx* c) { return gauge_ptr(c, PREC_SINGLE); }
+bool gauge_su3(iro_ctx* c) { return c->has_gauge && c->recon == 12; }
+int64_t volume(iro_ctx* c) { return c->V; }
 bool op_is_full(int op) { return is_full(op); }
 int op_subset(int op) { return input_subset(op); }
 bool op_ok(int op) { return op_valid(op); }

@@ -138,4 +138,18 @@ cudaError_t launch_field_strength(const Geom& g, const double* raw, int mu, int 
                                   cudaStream_t st);
 void clover_init_tables();
 
+// ---- learned preconditioner (learned.cu) -------------------------------------------
+struct PtcGeo;
+constexpr int kMaxVec = 16;
+struct CFieldList {
+  SpinorPtr f[kMaxVec];
+};
+struct CCoef {
+  float re[kMaxVec], im[kMaxVec];
+};
+cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
+                        cudaStream_t st);
+cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
+                         cudaStream_t st);
+
 }  // namespace iro

@@ -1,0 +1,1172 @@
+// Gauge-equivariant learned preconditioner: parallel-transport convolution
+// (PTC) layers and their gradients.
+//
+// A layer maps C_in colour-vector channels to C_out channels on every site of
+// the full lattice:
+//     out_o(x) = sum_{d=0..8} sum_i W_d[o][i] (T_d in_i)(x)
+// with T_0 the identity and, for d = 1 + 2*mu + s,
+//     T_{+mu} f(x) = U_mu(x) f(x+mu),   T_{-mu} f(x) = U_mu(x-mu)^dag f(x-mu),
+// so the layer commutes with gauge transformations (the weights act on the
+// channel index only, the links on colour).  A Wilson spinor is 4 channels
+// (its spins).  The reference has no learned part; this follows the
+// parallel-transport convolutions of Lehner & Wettig, "Gauge-equivariant
+// neural networks as preconditioners in lattice QCD", PRD 108 (2023).
+//
+// Forward kernel, one CTA per tile of 42 sites = 126 rows (site, colour):
+//  1. the CUDA cores transport every input channel along the 9 displacements
+//     and write the real GEMM operand A[row][k], k = (2d + re/im)*C_in + i,
+//     in BF16 into shared memory in the canonical K-major no-swizzle UMMA
+//     layout (8x16-byte core matrices);
+//  2. one thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M=128)
+//     against the packed real weight matrix B[n][k] (n = 2*o + re/im), the
+//     accumulator lives in tensor memory;
+//  3. the four warps read their 32 accumulator lanes back (tcgen05.ld) and
+//     store the output channels in FP32.
+// Every wait on the MMA's mbarrier is bounded: on time-out the kernel sets
+// an error flag, skips the read-back, frees its tensor memory and returns.
+//
+// Backward: dA = dY B (tcgen05, same machinery), then the adjoint transport
+// (a gather) gives d in; dB = A^T dY per tile on the CUDA cores with a
+// deterministic reduction over tiles.
+#include <cuda_bf16.h>
+
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+#include "iroiro_b200.h"
+
+namespace iro {
+
+// ---- tcgen05 / mbarrier primitives ------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\n"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// D(tmem) (+)= A(smem) * B(smem)^T, BF16 inputs, FP32 accumulation
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\n"
+      "setp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
+// matrices, LBO = byte step between the two K-halves of an MMA's K=16, SBO =
+// byte step between 8-row groups; version 1 (sm100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+// Instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, M=128, N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+}
+// byte offset of element (r, k) of a K-major R x K BF16 operand in the canonical layout
+__host__ __device__ __forceinline__ uint32_t canon(int r, int k, int K) {
+  return uint32_t((r >> 3) * (K / 8) * 128 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+constexpr int kTileSites = 42;  // 126 of the 128 MMA rows
+constexpr int kThreads = 128;
+constexpr int kWaitLimit = 1 << 24;
+
+template <int CIN, int COUT>
+struct Ptc {
+  static constexpr int KF = 18 * CIN;
+  static constexpr int KP = (KF + 15) / 16 * 16;
+  static constexpr int NF = 2 * COUT;
+  static constexpr int NP = NF < 16 ? 16 : (NF + 15) / 16 * 16;
+  static constexpr int TCOLS = NP <= 32 ? 32 : 64;
+  static constexpr int A_BYTES = 128 * KP * 2;
+  static constexpr int B_BYTES = NP * KP * 2;
+};
+
+struct PtcGeo {
+  Geom g;
+  GaugePtr gauge;  // FP32 two-row links
+  int V;
+  int* err;
+};
+
+// Builds the BF16 A tile: rows (site, colour) of the tile, columns
+// (2d + part)*CIN + i; padding rows/columns are zero.
+template <int CIN, int KP>
+__device__ void build_a_tile(const PtcGeo& G, const float2* __restrict__ in, int site0,
+                             unsigned char* A) {
+  // zero the tile (padding rows and columns must not hold stale values)
+  for (int b = threadIdx.x * 16; b < 128 * KP * 2; b += kThreads * 16)
+    *reinterpret_cast<uint4*>(A + b) = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  const int Vh = G.g.Vh;
+  for (int j = threadIdx.x; j < kTileSites * 9; j += kThreads) {
+    const int sl = j / 9, d = j - sl * 9;
+    const int s = site0 + sl;
+    if (s >= G.V) continue;
+    const int p = s >= Vh ? 1 : 0;
+    const int hs = s - p * Vh;
+    int src = s;
+    Su3<float> U;
+    bool fwd = true;
+    if (d > 0) {
+      const Coord c = coord_of(G.g, hs, p);
+      int nb[8];
+      neighbours(G.g, c, hs, nb);
+      const int mu = (d - 1) >> 1;
+      fwd = ((d - 1) & 1) == 0;
+      const int n = nb[d - 1];
+      src = (1 - p) * Vh + n;
+      if (fwd)
+        GaugeIO<PREC_SINGLE, 12>::load(G.gauge, p, mu, hs, U);
+      else
+        GaugeIO<PREC_SINGLE, 12>::load(G.gauge, 1 - p, mu, n, U);
+    }
+    const float2* f = in + size_t(src) * CIN * 3;
+#pragma unroll 4
+    for (int i = 0; i < CIN; ++i) {
+      Cx<float> v[3], w[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float2 t = f[i * 3 + a];
+        v[a] = {t.x, t.y};
+      }
+      if (d == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) w[a] = v[a];
+      } else if (fwd) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) w[a] = U.e[a][0] * v[0] + U.e[a][1] * v[1] + U.e[a][2] * v[2];
+      } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          w[a] = cj_mul(U.e[0][a], v[0]) + cj_mul(U.e[1][a], v[1]) + cj_mul(U.e[2][a], v[2]);
+      }
+      const int kre = (2 * d) * CIN + i, kim = (2 * d + 1) * CIN + i;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int r = sl * 3 + a;
+        *reinterpret_cast<__nv_bfloat16*>(A + canon(r, kre, KP)) = __float2bfloat16_rn(w[a].re);
+        *reinterpret_cast<__nv_bfloat16*>(A + canon(r, kim, KP)) = __float2bfloat16_rn(w[a].im);
+      }
+    }
+  }
+}
+
+// Loads an N x K row-major BF16 matrix into the canonical K-major layout.
+template <int N, int K>
+__device__ void load_b(const __nv_bfloat16* __restrict__ B, unsigned char* Bs) {
+  for (int idx = threadIdx.x; idx < N * K; idx += kThreads) {
+    const int n = idx / K, k = idx - n * K;
+    *reinterpret_cast<__nv_bfloat16*>(Bs + canon(n, k, K)) = B[idx];
+  }
+}
+
+// Issues the K/16 MMAs of D = A B^T into TMEM, commits to the mbarrier and
+// waits (bounded).  Returns false on time-out.
+template <int K>
+__device__ bool mma_and_wait(const unsigned char* A, const unsigned char* B, uint32_t tmem,
+                             uint32_t idesc, uint64_t* bar, uint32_t phase, int* err) {
+  fence_async_smem();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x == 0) {
+    const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+    constexpr uint32_t sbo = (K / 8) * 128;
+#pragma unroll 1
+    for (int kb = 0; kb < K / 16; ++kb)
+      umma_bf16(tmem, smem_desc(a0 + kb * 256, 128, sbo), smem_desc(b0 + kb * 256, 128, sbo), idesc,
+                kb > 0 ? 1u : 0u);
+    umma_commit(bar);
+  }
+  bool ok = false;
+  for (int it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, phase)) {
+      ok = true;
+      break;
+    }
+  if (!ok && err) atomicExch(err, 1);
+  tc_fence_after();
+  return ok;
+}
+
+// ---- forward ----------------------------------------------------------------------
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads) ptc_fwd_kernel(PtcGeo G, const float2* __restrict__ in,
+                                                           float2* __restrict__ out,
+                                                           const __nv_bfloat16* __restrict__ bop) {
+  using S = Ptc<CIN, COUT>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* A = smem;
+  unsigned char* B = smem + S::A_BYTES;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tslot;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) tmem_alloc(&tslot, S::TCOLS);
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  load_b<S::NP, S::KP>(bop, B);
+  const int site0 = blockIdx.x * kTileSites;
+  build_a_tile<CIN, S::KP>(G, in, site0, A);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tslot;
+  const bool ok = mma_and_wait<S::KP>(A, B, tmem, idesc_bf16(S::NP), &bar, 0, G.err);
+  if (ok) {
+    const int r = warp * 32 + lane;
+    float v[S::NP];
+#pragma unroll
+    for (int c = 0; c < S::NP; c += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c, v + c);
+    const int sl = r / 3, a = r - sl * 3;
+    const int s = site0 + sl;
+    if (sl < kTileSites && s < G.V) {
+#pragma unroll
+      for (int o = 0; o < COUT; ++o) out[(size_t(s) * COUT + o) * 3 + a] = make_float2(v[2 * o], v[2 * o + 1]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, S::TCOLS);
+}
+
+// ---- backward: dA = dY B, stored as FP32 rows (site, colour) x KP ------------------
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads) ptc_da_kernel(PtcGeo G, const float2* __restrict__ dy,
+                                                          float* __restrict__ da,
+                                                          const __nv_bfloat16* __restrict__ bopT) {
+  using S = Ptc<CIN, COUT>;
+  // operand A' = dY tile: 128 rows x NP (K' = NP); operand B' = B^T: KP rows x NP
+  constexpr int NCH = S::KP <= 256 ? S::KP : S::KP / 2;  // output columns per MMA pass
+  static_assert(NCH % 16 == 0 && NCH <= 256, "bad pass width");
+  constexpr int NPASS = S::KP / NCH;
+  constexpr int TC = NCH <= 32 ? 32 : (NCH <= 64 ? 64 : (NCH <= 128 ? 128 : 256));
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* A = smem;                 // 128 x NP
+  unsigned char* B = smem + 128 * S::NP * 2;  // KP x NP
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tslot;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) tmem_alloc(&tslot, TC);
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  load_b<S::KP, S::NP>(bopT, B);
+  const int site0 = blockIdx.x * kTileSites;
+  for (int idx = threadIdx.x; idx < 128 * S::NP; idx += kThreads) {
+    const int r = idx / S::NP, n = idx - r * S::NP;
+    const int sl = r / 3, a = r - sl * 3, s = site0 + sl;
+    float val = 0.f;
+    if (sl < kTileSites && s < G.V && n < S::NF) {
+      const float2 t = dy[(size_t(s) * COUT + (n >> 1)) * 3 + a];
+      val = (n & 1) ? t.y : t.x;
+    }
+    *reinterpret_cast<__nv_bfloat16*>(A + canon(r, n, S::NP)) = __float2bfloat16_rn(val);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tslot;
+  const int r = warp * 32 + lane;
+  const int sl = r / 3, a = r - sl * 3, s = site0 + sl;
+  for (int pass = 0; pass < NPASS; ++pass) {
+    const bool ok = mma_and_wait<S::NP>(A, B + pass * NCH * S::NP * 2 / 1, tmem, idesc_bf16(NCH), &bar,
+                                        uint32_t(pass & 1), G.err);
+    if (!ok) break;
+    float v[16];
+    for (int c = 0; c < NCH; c += 16) {
+      tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c, v);
+      if (sl < kTileSites && s < G.V) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) da[(size_t(s) * 3 + a) * S::KP + pass * NCH + c + k] = v[k];
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, TC);
+}
+
+// d in(y)_i = dA_0(y) + sum_mu U_mu(y-mu)^dag dA_{+mu}(y-mu) + U_mu(y) dA_{-mu}(y+mu)
+template <int CIN, int KP>
+__global__ void ptc_gather_kernel(PtcGeo G, const float* __restrict__ da, float2* __restrict__ din) {
+  const int Vh = G.g.Vh;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < G.V; s += gridDim.x * blockDim.x) {
+    const int p = s >= Vh ? 1 : 0;
+    const int hs = s - p * Vh;
+    const Coord c = coord_of(G.g, hs, p);
+    int nb[8];
+    neighbours(G.g, c, hs, nb);
+    for (int i = 0; i < CIN; ++i) {
+      Cx<float> acc[3];
+      auto grad = [&](int site, int d, Cx<float> g[3]) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          g[a] = {da[(size_t(site) * 3 + a) * KP + (2 * d) * CIN + i],
+                  da[(size_t(site) * 3 + a) * KP + (2 * d + 1) * CIN + i]};
+      };
+      grad(s, 0, acc);
+#pragma unroll 1
+      for (int mu = 0; mu < 4; ++mu) {
+        Cx<float> g[3];
+        Su3<float> U;
+        // from x = y - mu (d = +mu): U_mu(x)^dag g
+        const int xm = nb[2 * mu + 1];
+        grad((1 - p) * Vh + xm, 1 + 2 * mu, g);
+        GaugeIO<PREC_SINGLE, 12>::load(G.gauge, 1 - p, mu, xm, U);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          acc[a] = acc[a] + cj_mul(U.e[0][a], g[0]) + cj_mul(U.e[1][a], g[1]) + cj_mul(U.e[2][a], g[2]);
+        // from x = y + mu (d = -mu): U_mu(y) g
+        const int xp = nb[2 * mu];
+        grad((1 - p) * Vh + xp, 2 + 2 * mu, g);
+        GaugeIO<PREC_SINGLE, 12>::load(G.gauge, p, mu, hs, U);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[a] = acc[a] + U.e[a][0] * g[0] + U.e[a][1] * g[1] + U.e[a][2] * g[2];
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) din[(size_t(s) * CIN + i) * 3 + a] = make_float2(acc[a].re, acc[a].im);
+    }
+  }
+}
+
+// dB[n][k] = sum_rows dY[row][n] A[row][k], one partial per tile (CUDA cores)
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads) ptc_db_kernel(PtcGeo G, const float2* __restrict__ in,
+                                                          const float2* __restrict__ dy,
+                                                          float* __restrict__ partial) {
+  using S = Ptc<CIN, COUT>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* A = smem;
+  float* Y = reinterpret_cast<float*>(smem + S::A_BYTES);  // 128 x NF
+  const int site0 = blockIdx.x * kTileSites;
+  build_a_tile<CIN, S::KP>(G, in, site0, A);
+  for (int idx = threadIdx.x; idx < 128 * S::NF; idx += kThreads) {
+    const int r = idx / S::NF, n = idx - r * S::NF;
+    const int sl = r / 3, a = r - sl * 3, s = site0 + sl;
+    float val = 0.f;
+    if (sl < kTileSites && s < G.V) {
+      const float2 t = dy[(size_t(s) * COUT + (n >> 1)) * 3 + a];
+      val = (n & 1) ? t.y : t.x;
+    }
+    Y[idx] = val;
+  }
+  __syncthreads();
+  float* out = partial + size_t(blockIdx.x) * S::NF * S::KF;
+  for (int q = threadIdx.x; q < S::NF * S::KF; q += kThreads) {
+    const int n = q / S::KF, k = q - n * S::KF;
+    float acc = 0.f;
+    for (int r = 0; r < 126; ++r)
+      acc += Y[r * S::NF + n] * __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(A + canon(r, k, S::KP)));
+    out[q] = acc;
+  }
+}
+
+// deterministic sum over tiles
+__global__ void sum_partials_kernel(const float* __restrict__ partial, int ntiles, int n, float* out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int t = 0; t < ntiles; ++t) acc += partial[size_t(t) * n + q];
+    out[q] = float(acc);
+  }
+}
+
+// spinor field (FP32, full lattice) <-> 4-channel features [site][spin][colour]
+__global__ void spinor_to_feat_kernel(int Vh, SpinorPtr e, SpinorPtr o, float2* feat) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < 2 * Vh; s += gridDim.x * blockDim.x) {
+    const int p = s >= Vh ? 1 : 0;
+    Cx<float> v[12];
+    SpinorIO<PREC_SINGLE>::load(p ? o : e, s - p * Vh, v);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) feat[size_t(s) * 12 + k] = make_float2(v[k].re, v[k].im);
+  }
+}
+__global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < 2 * Vh; s += gridDim.x * blockDim.x) {
+    const int p = s >= Vh ? 1 : 0;
+    Cx<float> v[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      const float2 t = feat[size_t(s) * 12 + k];
+      v[k] = {t.x, t.y};
+    }
+    SpinorIO<PREC_SINGLE>::store(p ? o : e, s - p * Vh, v);
+  }
+}
+
+// ---- host launchers ------------------------------------------------------------------
+template <int CIN, int COUT>
+static cudaError_t fwd_t(const PtcGeo& G, const float2* in, float2* out, const __nv_bfloat16* bop,
+                         cudaStream_t st) {
+  using S = Ptc<CIN, COUT>;
+  const int smem = S::A_BYTES + S::B_BYTES;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(ptc_fwd_kernel<CIN, COUT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int grid = (G.V + kTileSites - 1) / kTileSites;
+  ptc_fwd_kernel<CIN, COUT><<<grid, kThreads, smem, st>>>(G, in, out, bop);
+  return cudaGetLastError();
+}
+
+template <int CIN, int COUT>
+static cudaError_t bwd_t(const PtcGeo& G, const float2* in, const float2* dy, float* da, float2* din,
+                         const __nv_bfloat16* bopT, float* partial, float* db, cudaStream_t st) {
+  using S = Ptc<CIN, COUT>;
+  const int grid = (G.V + kTileSites - 1) / kTileSites;
+  if (din) {
+    const int smem = 128 * S::NP * 2 + S::KP * S::NP * 2;
+    static bool attr = false;
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(ptc_da_kernel<CIN, COUT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    ptc_da_kernel<CIN, COUT><<<grid, kThreads, smem, st>>>(G, dy, da, bopT);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    ptc_gather_kernel<CIN, S::KP><<<(G.V + 255) / 256, 256, 0, st>>>(G, da, din);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (db) {
+    const int smem = S::A_BYTES + 128 * S::NF * 4;
+    static bool attr = false;
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(ptc_db_kernel<CIN, COUT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    ptc_db_kernel<CIN, COUT><<<grid, kThreads, smem, st>>>(G, in, dy, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    sum_partials_kernel<<<(S::NF * S::KF + 255) / 256, 256, 0, st>>>(partial, grid, S::NF * S::KF, db);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int ptc_shape_ok(int cin, int cout) {
+  return (cin == 4 || cin == 8 || cin == 16) && (cout == 4 || cout == 8 || cout == 16);
+}
+
+#define IRO_PTC_DISPATCH(CALL)                              \
+  switch (cin * 100 + cout) {                               \
+    case 404: return CALL(4, 4);                            \
+    case 408: return CALL(4, 8);                            \
+    case 416: return CALL(4, 16);                           \
+    case 804: return CALL(8, 4);                            \
+    case 808: return CALL(8, 8);                            \
+    case 816: return CALL(8, 16);                           \
+    case 1604: return CALL(16, 4);                          \
+    case 1608: return CALL(16, 8);                          \
+    case 1616: return CALL(16, 16);                         \
+  }                                                         \
+  return cudaErrorInvalidValue;
+
+cudaError_t launch_ptc_fwd(int cin, int cout, const PtcGeo& G, const float2* in, float2* out,
+                           const void* bop, cudaStream_t st) {
+#define IRO_F(A, B) fwd_t<A, B>(G, in, out, static_cast<const __nv_bfloat16*>(bop), st)
+  IRO_PTC_DISPATCH(IRO_F)
+#undef IRO_F
+}
+
+cudaError_t launch_ptc_bwd(int cin, int cout, const PtcGeo& G, const float2* in, const float2* dy,
+                           float* da, float2* din, const void* bopT, float* partial, float* db,
+                           cudaStream_t st) {
+#define IRO_B(A, B) bwd_t<A, B>(G, in, dy, da, din, static_cast<const __nv_bfloat16*>(bopT), partial, db, st)
+  IRO_PTC_DISPATCH(IRO_B)
+#undef IRO_B
+}
+
+void ptc_dims(int cin, int cout, int* kf, int* kp, int* nf, int* np) {
+  *kf = 18 * cin;
+  *kp = (*kf + 15) / 16 * 16;
+  *nf = 2 * cout;
+  *np = *nf < 16 ? 16 : (*nf + 15) / 16 * 16;
+}
+
+cudaError_t launch_spinor_to_feat(int Vh, SpinorPtr e, SpinorPtr o, float2* feat, cudaStream_t st) {
+  spinor_to_feat_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, e, o, feat);
+  return cudaGetLastError();
+}
+cudaError_t launch_feat_to_spinor(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o, cudaStream_t st) {
+  feat_to_spinor_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, feat, e, o);
+  return cudaGetLastError();
+}
+
+// ---- loss of a training pair: |y - t|^2 and |t|^2, and dy = 2 (y - t) / |t|^2 ------------
+constexpr int kRedBlocks = 296;
+
+__global__ void loss_partials_kernel(int n, const float2* y, const float2* t, double* part) {
+  __shared__ double sa[256], sb[256];
+  double a = 0.0, b = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float2 yy = y[i], tt = t[i];
+    const double dr = double(yy.x) - tt.x, di = double(yy.y) - tt.y;
+    a += dr * dr + di * di;
+    b += double(tt.x) * tt.x + double(tt.y) * tt.y;
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      sa[threadIdx.x] += sa[threadIdx.x + h];
+      sb[threadIdx.x] += sb[threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = sa[0];
+    part[2 * blockIdx.x + 1] = sb[0];
+  }
+}
+
+__global__ void loss_grad_kernel(int n, const float2* y, const float2* t, float scale, float2* dy) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float2 yy = y[i], tt = t[i];
+    dy[i] = make_float2(scale * (yy.x - tt.x), scale * (yy.y - tt.y));
+  }
+}
+
+cudaError_t launch_loss_partials(int n, const float2* y, const float2* t, double* part, cudaStream_t st) {
+  loss_partials_kernel<<<kRedBlocks, 256, 0, st>>>(n, y, t, part);
+  return cudaGetLastError();
+}
+cudaError_t launch_loss_grad(int n, const float2* y, const float2* t, float scale, float2* dy,
+                             cudaStream_t st) {
+  loss_grad_kernel<<<kRedBlocks, 256, 0, st>>>(n, y, t, scale, dy);
+  return cudaGetLastError();
+}
+int loss_blocks() { return kRedBlocks; }
+
+// ---- complex linear algebra for GCR on FP32 fields ---------------------------------------
+// <w_q, t> = sum conj(w_q) t for q < m, per-block partials [block][2m]
+__global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double* part) {
+  __shared__ double sm[2 * kMaxVec][64];
+  double acc[2 * kMaxVec];
+#pragma unroll
+  for (int q = 0; q < 2 * kMaxVec; ++q) acc[q] = 0.0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<float> tv[12], wv[12];
+    SpinorIO<PREC_SINGLE>::load(t, i, tv);
+#pragma unroll
+    for (int q = 0; q < kMaxVec; ++q) {
+      if (q >= m) break;
+      SpinorIO<PREC_SINGLE>::load(w.f[q], i, wv);
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        re += double(wv[k].re) * tv[k].re + double(wv[k].im) * tv[k].im;
+        im += double(wv[k].re) * tv[k].im - double(wv[k].im) * tv[k].re;
+      }
+      acc[2 * q] += re;
+      acc[2 * q + 1] += im;
+    }
+  }
+  for (int q = 0; q < 2 * m; ++q) {
+    double v = acc[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sm[q][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * m) {
+    double v = 0.0;
+    for (int wv = 0; wv < int(blockDim.x >> 5); ++wv) v += sm[threadIdx.x][wv];
+    part[size_t(blockIdx.x) * 2 * m + threadIdx.x] = v;
+  }
+}
+
+// y += sum_q c_q x_q  (complex coefficients)
+__global__ void caxpy_kernel(int64_t n, int m, CFieldList x, CCoef c, SpinorPtr y) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<float> yv[12], xv[12];
+    SpinorIO<PREC_SINGLE>::load(y, i, yv);
+    for (int q = 0; q < m; ++q) {
+      SpinorIO<PREC_SINGLE>::load(x.f[q], i, xv);
+      const Cx<float> cq = {c.re[q], c.im[q]};
+#pragma unroll
+      for (int k = 0; k < 12; ++k) yv[k] = yv[k] + cq * xv[k];
+    }
+    SpinorIO<PREC_SINGLE>::store(y, i, yv);
+  }
+}
+
+cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
+                        cudaStream_t st) {
+  cdot_kernel<<<blocks, 256, 0, st>>>(n, m, w, t, part);
+  return cudaGetLastError();
+}
+cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
+                         cudaStream_t st) {
+  int grid = int((n + 255) / 256);
+  if (grid > 148 * 16) grid = 148 * 16;
+  caxpy_kernel<<<grid, 256, 0, st>>>(n, m, x, c, y);
+  return cudaGetLastError();
+}
+
+}  // namespace iro
+
+// =====================================================================================
+// Host side: the network object, training gradients and flexible GCR.
+// =====================================================================================
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <memory>
+#include <string>
+
+namespace iro {
+namespace host {
+int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in, DevField& out,
+          const Reduce* red, int red_mask, const int* skip);
+DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
+int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
+int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
+int norms(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
+          std::vector<double>* nw);
+int axpby(iro_ctx* c, double a, const DevField& x, double b, const DevField& y, DevField& v);
+int convert(iro_ctx* c, const DevField& in, DevField& out);
+int set_error(iro_ctx* c, int code, const std::string& msg);
+int cuda_error(iro_ctx* c, cudaError_t e, const char* where);
+cudaStream_t stream(iro_ctx* c);
+int device(iro_ctx* c);
+DevField* field_dev(iro_field* f);
+const Geom& geom(iro_ctx* c);
+GaugePtr gauge_single(iro_ctx* c);
+bool gauge_su3(iro_ctx* c);
+int64_t volume(iro_ctx* c);
+}  // namespace host
+}  // namespace iro
+
+// CG on device fields (solvers.cu), the fallback of the preconditioned solve
+int cg_any_dev(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+               const iro::DevField* B, iro::DevField* X, int nrhs, iro_solver_out* out);
+
+using namespace iro;
+using namespace iro::host;
+
+#define LCK(call)                                            \
+  do {                                                       \
+    cudaError_t e__ = (call);                                \
+    if (e__ != cudaSuccess) return cuda_error(c, e__, #call); \
+  } while (0)
+#define LRC(call)                  \
+  do {                             \
+    int r__ = (call);              \
+    if (r__ != IRO_OK) return r__; \
+  } while (0)
+
+struct iro_ptc {
+  iro_ctx* ctx = nullptr;
+  int nl = 0;
+  std::vector<int> w;                 // widths, nl+1 entries
+  std::vector<std::vector<float>> W;  // host weights, complex [9][cout][cin] (re,im)
+  std::vector<void*> bop, bopT;       // device BF16 packed weights per layer
+  std::vector<float2*> act;           // act[l]: input of layer l (act[nl]: output)
+  float2* g0 = nullptr;               // gradient ping-pong buffers
+  float2* g1 = nullptr;
+  float* da = nullptr;
+  float* partial = nullptr;
+  std::vector<float*> db;
+  int* err = nullptr;
+  double* lpart = nullptr;
+  size_t maxc = 0;
+};
+
+namespace {
+
+void pack_bop(int cin, int cout, const std::vector<float>& W, std::vector<__nv_bfloat16>& bop,
+              std::vector<__nv_bfloat16>& bopT) {
+  int kf, kp, nf, np;
+  ptc_dims(cin, cout, &kf, &kp, &nf, &np);
+  std::vector<float> B(size_t(np) * kp, 0.f);
+  for (int d = 0; d < 9; ++d)
+    for (int o = 0; o < cout; ++o)
+      for (int i = 0; i < cin; ++i) {
+        const size_t w = ((size_t(d) * cout + o) * cin + i) * 2;
+        const float wr = W[w], wi = W[w + 1];
+        const int kre = (2 * d) * cin + i, kim = (2 * d + 1) * cin + i;
+        B[size_t(2 * o) * kp + kre] = wr;
+        B[size_t(2 * o) * kp + kim] = -wi;
+        B[size_t(2 * o + 1) * kp + kre] = wi;
+        B[size_t(2 * o + 1) * kp + kim] = wr;
+      }
+  bop.resize(B.size());
+  bopT.resize(B.size());
+  for (int n = 0; n < np; ++n)
+    for (int k = 0; k < kp; ++k) {
+      bop[size_t(n) * kp + k] = __float2bfloat16_rn(B[size_t(n) * kp + k]);
+      bopT[size_t(k) * np + n] = __float2bfloat16_rn(B[size_t(n) * kp + k]);
+    }
+}
+
+// dL/dB (NF x KF, real) -> dL/dW (complex [9][cout][cin])
+void unpack_grad(int cin, int cout, const std::vector<float>& dB, float* g) {
+  int kf, kp, nf, np;
+  ptc_dims(cin, cout, &kf, &kp, &nf, &np);
+  for (int d = 0; d < 9; ++d)
+    for (int o = 0; o < cout; ++o)
+      for (int i = 0; i < cin; ++i) {
+        const int kre = (2 * d) * cin + i, kim = (2 * d + 1) * cin + i;
+        const float rr = dB[size_t(2 * o) * kf + kre], ri = dB[size_t(2 * o) * kf + kim];
+        const float ir = dB[size_t(2 * o + 1) * kf + kre], ii = dB[size_t(2 * o + 1) * kf + kim];
+        const size_t w = ((size_t(d) * cout + o) * cin + i) * 2;
+        g[w] = rr + ii;
+        g[w + 1] = -ri + ir;
+      }
+}
+
+PtcGeo make_geo(iro_ctx* c, int* err) {
+  PtcGeo G;
+  G.g = geom(c);
+  G.gauge = gauge_single(c);
+  G.V = int(volume(c));
+  G.err = err;
+  return G;
+}
+
+// features of a full-lattice spinor field (FP32 or FP64; converted to FP32)
+int field_to_feat(iro_ctx* c, const DevField& f, float2* feat) {
+  const DevField* src = &f;
+  int rc = IRO_OK;
+  if (f.prec != PREC_SINGLE) {
+    DevField* t = workspace(c, 2, PREC_SINGLE, 1, 70, &rc);
+    if (!t) return rc;
+    LRC(convert(c, f, *t));
+    src = t;
+  }
+  LCK(launch_spinor_to_feat(int(src->Vh), src->half(0), src->half(1), feat, stream(c)));
+  return IRO_OK;
+}
+
+int feat_to_field(iro_ctx* c, const float2* feat, DevField& f) {
+  if (f.prec == PREC_SINGLE) {
+    LCK(launch_feat_to_spinor(int(f.Vh), feat, f.half(0), f.half(1), stream(c)));
+    return IRO_OK;
+  }
+  int rc = IRO_OK;
+  DevField* t = workspace(c, 2, PREC_SINGLE, 1, 71, &rc);
+  if (!t) return rc;
+  LCK(launch_feat_to_spinor(int(t->Vh), feat, t->half(0), t->half(1), stream(c)));
+  return convert(c, *t, f);
+}
+
+int check_err(iro_ctx* c, iro_ptc* n) {
+  int e = 0;
+  LCK(cudaMemcpyAsync(&e, n->err, sizeof(int), cudaMemcpyDeviceToHost, stream(c)));
+  LCK(cudaStreamSynchronize(stream(c)));
+  if (e) return set_error(c, IRO_TIMEOUT, "tensor-core wait timed out in the network kernels");
+  return IRO_OK;
+}
+
+// act[0] must hold the input features; runs every layer
+int forward(iro_ctx* c, iro_ptc* n) {
+  PtcGeo G = make_geo(c, n->err);
+  for (int l = 0; l < n->nl; ++l)
+    LCK(launch_ptc_fwd(n->w[l], n->w[l + 1], G, n->act[l], n->act[l + 1], n->bop[l], stream(c)));
+  return IRO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int iro_ptc_create(iro_ctx* c, int nlayers, const int* widths, iro_ptc** out) {
+  if (!c || !widths || !out || nlayers < 1 || nlayers > 8)
+    return set_error(c, IRO_BAD_ARG, "bad network arguments");
+  if (widths[0] != 4 || widths[nlayers] != 4)
+    return set_error(c, IRO_BAD_ARG, "network input and output must be 4 channels (a spinor)");
+  for (int l = 0; l < nlayers; ++l)
+    if (!ptc_shape_ok(widths[l], widths[l + 1]))
+      return set_error(c, IRO_BAD_ARG, "layer widths must be 4, 8 or 16 channels");
+  LCK(cudaSetDevice(device(c)));
+  std::unique_ptr<iro_ptc> n(new iro_ptc());
+  n->ctx = c;
+  n->nl = nlayers;
+  n->w.assign(widths, widths + nlayers + 1);
+  const size_t V = size_t(volume(c));
+  size_t maxc = 0;
+  for (int w : n->w) maxc = std::max(maxc, size_t(w));
+  n->maxc = maxc;
+  n->W.resize(nlayers);
+  n->bop.resize(nlayers);
+  n->bopT.resize(nlayers);
+  n->db.resize(nlayers);
+  n->act.resize(nlayers + 1);
+  int maxkp = 0, maxtiles = int((V + kTileSites - 1) / kTileSites), maxnk = 0;
+  for (int l = 0; l < nlayers; ++l) {
+    int kf, kp, nf, np;
+    ptc_dims(n->w[l], n->w[l + 1], &kf, &kp, &nf, &np);
+    maxkp = std::max(maxkp, kp);
+    maxnk = std::max(maxnk, nf * kf);
+    n->W[l].assign(size_t(9) * n->w[l + 1] * n->w[l] * 2, 0.f);
+    LCK(cudaMalloc(&n->bop[l], size_t(np) * kp * 2));
+    LCK(cudaMalloc(&n->bopT[l], size_t(np) * kp * 2));
+    LCK(cudaMemset(n->bop[l], 0, size_t(np) * kp * 2));
+    LCK(cudaMemset(n->bopT[l], 0, size_t(np) * kp * 2));
+    LCK(cudaMalloc(&n->db[l], size_t(nf) * kf * sizeof(float)));
+  }
+  for (int l = 0; l <= nlayers; ++l) LCK(cudaMalloc(&n->act[l], V * n->w[l] * 3 * sizeof(float2)));
+  LCK(cudaMalloc(&n->g0, V * maxc * 3 * sizeof(float2)));
+  LCK(cudaMalloc(&n->g1, V * maxc * 3 * sizeof(float2)));
+  LCK(cudaMalloc(&n->da, V * 3 * maxkp * sizeof(float)));
+  LCK(cudaMalloc(&n->partial, size_t(maxtiles) * maxnk * sizeof(float)));
+  LCK(cudaMalloc(&n->err, sizeof(int)));
+  LCK(cudaMemset(n->err, 0, sizeof(int)));
+  LCK(cudaMalloc(&n->lpart, sizeof(double) * 2 * loss_blocks()));
+  *out = n.release();
+  return IRO_OK;
+}
+
+int iro_ptc_destroy(iro_ptc* n) {
+  if (!n) return IRO_BAD_ARG;
+  cudaSetDevice(device(n->ctx));
+  cudaStreamSynchronize(stream(n->ctx));
+  for (void* p : n->bop) cudaFree(p);
+  for (void* p : n->bopT) cudaFree(p);
+  for (float* p : n->db) cudaFree(p);
+  for (float2* p : n->act) cudaFree(p);
+  void* ps[] = {n->g0, n->g1, n->da, n->partial, n->err, n->lpart};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  delete n;
+  return IRO_OK;
+}
+
+int iro_ptc_set_weights(iro_ptc* n, int layer, const float* w) {
+  if (!n || !w || layer < 0 || layer >= n->nl) return IRO_BAD_ARG;
+  iro_ctx* c = n->ctx;
+  LCK(cudaSetDevice(device(c)));
+  const int cin = n->w[layer], cout = n->w[layer + 1];
+  n->W[layer].assign(w, w + size_t(9) * cout * cin * 2);
+  std::vector<__nv_bfloat16> b, bt;
+  pack_bop(cin, cout, n->W[layer], b, bt);
+  LCK(cudaMemcpyAsync(n->bop[layer], b.data(), b.size() * 2, cudaMemcpyHostToDevice, stream(c)));
+  LCK(cudaMemcpyAsync(n->bopT[layer], bt.data(), bt.size() * 2, cudaMemcpyHostToDevice, stream(c)));
+  LCK(cudaStreamSynchronize(stream(c)));
+  return IRO_OK;
+}
+
+static bool same_lattice(iro_ctx* c, const iro_ptc* n) {
+  return volume(c) == volume(n->ctx) && geom(c).L[0] == geom(n->ctx).L[0] &&
+         geom(c).L[1] == geom(n->ctx).L[1] && geom(c).L[2] == geom(n->ctx).L[2];
+}
+
+int iro_ptc_apply_field(iro_ctx* c, iro_ptc* n, const iro_field* in, iro_field* out) {
+  if (!c || !n || !in || !out) return IRO_BAD_ARG;
+  if (!same_lattice(c, n)) return set_error(c, IRO_BAD_ARG, "network built for another lattice");
+  const DevField* fi = field_dev(const_cast<iro_field*>(in));
+  DevField* fo = field_dev(out);
+  if (fi->subset != 2 || fo->subset != 2 || fi->nrhs != 1 || fo->nrhs != 1 || fi->prec == PREC_HALF ||
+      fo->prec == PREC_HALF)
+    return set_error(c, IRO_BAD_ARG, "network fields must be full-lattice FP32/FP64, one rhs");
+  if (!gauge_su3(c)) return set_error(c, IRO_NO_GAUGE, "network needs an SU(3) gauge field");
+  LCK(cudaSetDevice(device(c)));
+  LRC(field_to_feat(c, *fi, n->act[0]));
+  LRC(forward(c, n));
+  LRC(feat_to_field(c, n->act[n->nl], *fo));
+  return check_err(c, n);
+}
+
+int iro_ptc_apply(iro_ctx* c, iro_ptc* n, const double* in, double* out) {
+  if (!c || !n || !in || !out) return IRO_BAD_ARG;
+  if (!same_lattice(c, n)) return set_error(c, IRO_BAD_ARG, "network built for another lattice");
+  if (!gauge_su3(c)) return set_error(c, IRO_NO_GAUGE, "network needs an SU(3) gauge field");
+  LCK(cudaSetDevice(device(c)));
+  int rc = IRO_OK;
+  DevField* a = workspace(c, 2, PREC_DOUBLE, 1, 72, &rc);
+  if (!a) return rc;
+  DevField* b = workspace(c, 2, PREC_DOUBLE, 1, 73, &rc);
+  if (!b) return rc;
+  LRC(import_field(c, in, true, *a));
+  LRC(field_to_feat(c, *a, n->act[0]));
+  LRC(forward(c, n));
+  LRC(check_err(c, n));
+  LRC(feat_to_field(c, n->act[n->nl], *b));
+  return export_field(c, *b, true, out);
+}
+
+int iro_ptc_loss_grad(iro_ctx* c, iro_ptc* n, const iro_field* in, const iro_field* target,
+                      double* loss, float* grad) {
+  if (!c || !n || !in || !target || !loss) return IRO_BAD_ARG;
+  if (!same_lattice(c, n)) return set_error(c, IRO_BAD_ARG, "network built for another lattice");
+  const DevField* fi = field_dev(const_cast<iro_field*>(in));
+  const DevField* ft = field_dev(const_cast<iro_field*>(target));
+  if (fi->subset != 2 || ft->subset != 2 || fi->nrhs != 1 || ft->nrhs != 1)
+    return set_error(c, IRO_BAD_ARG, "training fields must be full-lattice, one rhs");
+  if (!gauge_su3(c)) return set_error(c, IRO_NO_GAUGE, "network needs an SU(3) gauge field");
+  LCK(cudaSetDevice(device(c)));
+  cudaStream_t st = stream(c);
+  const int V = int(volume(c));
+  LRC(field_to_feat(c, *fi, n->act[0]));
+  LRC(forward(c, n));
+  // target features into g1, loss and dL/dy into g0
+  LRC(field_to_feat(c, *ft, n->g1));
+  const int nel = V * 12;
+  LCK(launch_loss_partials(nel, n->act[n->nl], n->g1, n->lpart, st));
+  std::vector<double> part(2 * loss_blocks());
+  LCK(cudaMemcpyAsync(part.data(), n->lpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st));
+  LCK(cudaStreamSynchronize(st));
+  double dd = 0.0, tt = 0.0;
+  for (int b = 0; b < loss_blocks(); ++b) {
+    dd += part[2 * b];
+    tt += part[2 * b + 1];
+  }
+  *loss = dd / tt;
+  if (!grad) return check_err(c, n);
+  LCK(launch_loss_grad(nel, n->act[n->nl], n->g1, float(2.0 / tt), n->g0, st));
+  PtcGeo G = make_geo(c, n->err);
+  float2* dy = n->g0;
+  float2* dx = n->g1;
+  std::vector<size_t> goff(n->nl + 1, 0);
+  for (int l = 0; l < n->nl; ++l) goff[l + 1] = goff[l] + size_t(9) * n->w[l + 1] * n->w[l] * 2;
+  for (int l = n->nl - 1; l >= 0; --l) {
+    const int cin = n->w[l], cout = n->w[l + 1];
+    LCK(launch_ptc_bwd(cin, cout, G, n->act[l], dy, n->da, l > 0 ? dx : nullptr, n->bopT[l],
+                       n->partial, n->db[l], st));
+    int kf, kp, nf, np;
+    ptc_dims(cin, cout, &kf, &kp, &nf, &np);
+    std::vector<float> dB(size_t(nf) * kf);
+    LCK(cudaMemcpyAsync(dB.data(), n->db[l], dB.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+    unpack_grad(cin, cout, dB, grad + goff[l]);
+    std::swap(dy, dx);
+  }
+  return check_err(c, n);
+}
+
+// ---- flexible GCR on A = D^dag D with the network as right preconditioner ---------------
+int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_ptc* net,
+                        const iro_gcr_params* prm, const iro_field* b, iro_field* x, iro_gcr_out* out) {
+  const DevField* B = field_dev(const_cast<iro_field*>(b));
+  DevField* X = field_dev(x);
+  if (!c || !prm || !B || !X || !out || (op != IRO_OP_WILSON_FULL && op != IRO_OP_CLOVER_FULL) ||
+      B->subset != 2 || X->subset != 2 || B->prec != PREC_DOUBLE || X->prec != PREC_DOUBLE ||
+      B->nrhs != 1 || X->nrhs != 1 || prm->nkrylov < 1 || prm->nkrylov > kMaxVec ||
+      !(prm->precision > 0.0))
+    return set_error(c, IRO_BAD_ARG, "bad GCR arguments");
+  if (net && !same_lattice(c, net)) return set_error(c, IRO_BAD_ARG, "network built for another lattice");
+  LCK(cudaSetDevice(device(c)));
+  auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t st = stream(c);
+  const int m = prm->nkrylov;
+  int rc = IRO_OK;
+  DevField* R = workspace(c, 2, PREC_DOUBLE, 1, 80, &rc); if (!R) return rc;
+  DevField* Q = workspace(c, 2, PREC_DOUBLE, 1, 81, &rc); if (!Q) return rc;
+  DevField* S = workspace(c, 2, PREC_DOUBLE, 1, 82, &rc); if (!S) return rc;
+  DevField* r32 = workspace(c, 2, PREC_SINGLE, 1, 83, &rc); if (!r32) return rc;
+  DevField* e32 = workspace(c, 2, PREC_SINGLE, 1, 84, &rc); if (!e32) return rc;
+  DevField* t32 = workspace(c, 2, PREC_SINGLE, 1, 85, &rc); if (!t32) return rc;
+  std::vector<DevField*> Z(m), W(m);
+  for (int j = 0; j < m; ++j) {
+    Z[j] = workspace(c, 2, PREC_SINGLE, 1, 90 + j, &rc); if (!Z[j]) return rc;
+    W[j] = workspace(c, 2, PREC_SINGLE, 1, 90 + kMaxVec + j, &rc); if (!W[j]) return rc;
+  }
+  const int64_t nel = R->sites();
+  const int blocks = 296;
+  double* part = nullptr;
+  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * blocks * 2 * kMaxVec, st));
+  struct Free {
+    double* p;
+    cudaStream_t s;
+    ~Free() { if (p) cudaFreeAsync(p, s); }
+  } free_part{part, st};
+  std::vector<double> hp(size_t(blocks) * 2 * kMaxVec);
+  // <w_q, t> for the listed fields, summed on the host in block order
+  auto cdots = [&](const std::vector<const DevField*>& ws, const DevField& t,
+                   std::vector<std::complex<double>>& res) -> int {
+    CFieldList L{};
+    const int k = int(ws.size());
+    for (int q = 0; q < k; ++q) L.f[q] = ws[q]->all();
+    LCK(launch_cdot(nel, k, L, t.all(), part, blocks, st));
+    LCK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * blocks * 2 * k, cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+    res.assign(k, {0.0, 0.0});
+    for (int bb = 0; bb < blocks; ++bb)
+      for (int q = 0; q < k; ++q)
+        res[q] += std::complex<double>(hp[size_t(bb) * 2 * k + 2 * q], hp[size_t(bb) * 2 * k + 2 * q + 1]);
+    return IRO_OK;
+  };
+  auto caxpy = [&](const std::vector<const DevField*>& xs, const std::vector<std::complex<double>>& cs,
+                   DevField& y) -> int {
+    CFieldList L{};
+    CCoef C{};
+    for (size_t q = 0; q < xs.size(); ++q) {
+      L.f[q] = xs[q]->all();
+      C.re[q] = float(cs[q].real());
+      C.im[q] = float(cs[q].imag());
+    }
+    LCK(launch_caxpy(nel, int(xs.size()), L, C, y.all(), st));
+    return IRO_OK;
+  };
+  // x = 0, r = b
+  LRC(axpby(c, 0.0, *B, 0.0, *B, *X));
+  LRC(axpby(c, 1.0, *B, 0.0, *B, *R));
+  std::vector<double> bn;
+  LRC(norms(c, *B, nullptr, bn, nullptr));
+  const double target = prm->precision * bn[0];
+  double rr = bn[0];
+  const double delta = prm->delta > 0.0 ? prm->delta : 0.1;
+  int iters = 0, restarts = 0, fallback = 0, pcapplies = 0, stalls = 0;
+  bool converged = rr < target;
+  std::vector<int> ones(1, 1);
+  int* dmask = nullptr;
+  LCK(cudaMallocAsync(reinterpret_cast<void**>(&dmask), sizeof(int), st));
+  struct FreeI {
+    int* p;
+    cudaStream_t s;
+    ~FreeI() { if (p) cudaFreeAsync(p, s); }
+  } free_mask{dmask, st};
+  LCK(cudaMemcpyAsync(dmask, ones.data(), sizeof(int), cudaMemcpyHostToDevice, st));
+  while (!converged && iters < prm->max_iter) {
+    LRC(convert(c, *R, *r32));
+    LRC(axpby(c, 0.0, *r32, 0.0, *r32, *e32));
+    const double rr_start = rr;
+    std::vector<double> nw(m, 0.0);
+    for (int j = 0; j < m && iters < prm->max_iter; ++j) {
+      // z_j = N(r) (or r without a network), w_j = A z_j
+      if (net) {
+        LRC(field_to_feat(c, *r32, net->act[0]));
+        LRC(forward(c, const_cast<iro_ptc*>(net)));
+        LRC(feat_to_field(c, net->act[net->nl], *Z[j]));
+        ++pcapplies;
+      } else {
+        LRC(axpby(c, 1.0, *r32, 0.0, *r32, *Z[j]));
+      }
+      LRC(apply(c, op, mass, csw, false, *Z[j], *t32, nullptr, 0, nullptr));
+      LRC(apply(c, op, mass, csw, true, *t32, *W[j], nullptr, 0, nullptr));
+      if (j > 0) {
+        std::vector<const DevField*> ws(W.begin(), W.begin() + j), zs(Z.begin(), Z.begin() + j);
+        std::vector<std::complex<double>> cw;
+        LRC(cdots(ws, *W[j], cw));
+        std::vector<std::complex<double>> beta(j);
+        for (int q = 0; q < j; ++q) beta[q] = -cw[q] / nw[q];
+        LRC(caxpy(ws, beta, *W[j]));
+        LRC(caxpy(zs, beta, *Z[j]));
+      }
+      std::vector<std::complex<double>> g1, g2;
+      LRC(cdots({W[j]}, *W[j], g1));
+      LRC(cdots({W[j]}, *r32, g2));
+      nw[j] = g1[0].real();
+      const std::complex<double> alpha = g2[0] / nw[j];
+      LRC(caxpy({Z[j]}, {alpha}, *e32));
+      LRC(caxpy({W[j]}, {-alpha}, *r32));
+      std::vector<std::complex<double>> rn;
+      LRC(cdots({r32}, *r32, rn));
+      ++iters;
+      if (rn[0].real() < target || rn[0].real() < delta * delta * rr_start) break;
+    }
+    // x += e, r = b - A x in FP64
+    LCK(launch_mx_merge(PREC_SINGLE, X->sites(), 1, X->all(), e32->all(), dmask, st));
+    LRC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+    LRC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+    LRC(axpby(c, 1.0, *B, -1.0, *S, *R));
+    std::vector<double> rnorm;
+    LRC(norms(c, *R, nullptr, rnorm, nullptr));
+    ++restarts;
+    stalls = (rnorm[0] > 0.25 * rr) ? stalls + 1 : 0;
+    rr = rnorm[0];
+    converged = rr < target;
+    if (!std::isfinite(rr)) break;
+    if (!converged && stalls >= 2) {
+      // the preconditioned iteration stalls: finish with mixed-precision CG on
+      // the correction A e = r, then x += e
+      iro_cg_params cp{prm->precision * bn[0] / rr, prm->max_iter, IRO_PREC_SINGLE, 0.1, 1};
+      DevField* E = workspace(c, 2, PREC_DOUBLE, 1, 86, &rc); if (!E) return rc;
+      iro_solver_out co;
+      const int crc = cg_any_dev(c, op, mass, csw, &cp, R, E, 1, &co);
+      if (crc != IRO_OK && crc != IRO_NOT_CONVERGED) return crc;
+      LRC(axpby(c, 1.0, *X, 1.0, *E, *X));
+      LRC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
+      LRC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+      LRC(axpby(c, 1.0, *B, -1.0, *S, *R));
+      LRC(norms(c, *R, nullptr, rnorm, nullptr));
+      rr = rnorm[0];
+      converged = rr < target;
+      iters += co.iterations > 0 ? co.iterations : 0;
+      fallback = 1;
+      break;
+    }
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  out->diff = std::sqrt(rr / bn[0]);
+  out->iterations = converged ? iters : -1;
+  out->timing_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  out->restarts = restarts;
+  out->fallback = fallback;
+  out->precond_applies = pcapplies;
+  if (net) {
+    int e = check_err(c, const_cast<iro_ptc*>(net));
+    if (e) return e;
+  }
+  if (!converged) return set_error(c, IRO_NOT_CONVERGED, "GCR not converged");
+  return IRO_OK;
+}
+
+}  // extern "C"

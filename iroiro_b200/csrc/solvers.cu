@@ -190,6 +190,13 @@ static int cg_any(iro_ctx* c, int op, double mass, double csw, const iro_cg_para
   return rc;
 }
 
+// CG on device fields for other solvers in this library (the fallback of the
+// preconditioned GCR)
+int cg_any_dev(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+               const DevField* B, DevField* X, int nrhs, iro_solver_out* out) {
+  return cg_any(c, op, mass, csw, prm, B, X, nrhs, out);
+}
+
 static bool cg_args_ok(const iro_cg_params* prm, int op) {
   return prm && solver_op_ok(op) && prm->inner_prec >= 0 && prm->inner_prec <= 2 &&
          prm->precision > 0.0;

@@ -1,0 +1,97 @@
+"""Learned preconditioner on the GPU: the tensor-core network forward and its
+gradients against the FP64 CPU oracle, GCR with and without the network, and
+training that lowers the loss and the GCR iteration count."""
+import numpy as np
+import pytest
+
+import iroiro_b200 as ib
+from iroiro_b200 import learned
+from oracle import ptc
+
+pytestmark = pytest.mark.gpu
+
+# BF16 operands and weights with FP32 accumulation: a few parts in 1e3 per layer
+TOL_NET = 3e-2
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b)))
+
+
+@pytest.fixture(scope="module")
+def small():
+    L = [4, 4, 4, 8]
+    u = ib.synth_gauge(L, 0.25, 21, gauge_transform=True)
+    ctx = ib.Context(L, 0)
+    ctx.upload_gauge(u, force=True)
+    return L, u, ctx
+
+
+@pytest.mark.parametrize("widths", [(4, 4), (4, 16, 4), (4, 16, 16, 16, 4), (4, 8, 4)])
+def test_forward_vs_oracle(small, widths):
+    L, u, ctx = small
+    V = int(np.prod(L))
+    Ws = learned.init_weights(widths, seed=3, scale=0.5)
+    net = learned.PTCNet(ctx, widths, Ws)
+    f = ib.synth_gaussian(V, 31)
+    got = net.apply(f)
+    lat = ptc.Lattice(L, u)
+    want = ptc.feat_to_spinor(lat, ptc.forward(lat, Ws, ptc.spinor_to_feat(lat, f))[-1])
+    assert rel(got, want) < TOL_NET
+
+
+def test_loss_and_gradients_vs_oracle(small):
+    L, u, ctx = small
+    V = int(np.prod(L))
+    widths = (4, 16, 16, 16, 4)
+    Ws = learned.init_weights(widths, seed=5, scale=0.5)
+    net = learned.PTCNet(ctx, widths, Ws)
+    b, t = ib.synth_gaussian(V, 41), ib.synth_gaussian(V, 42)
+    db = ib.DeviceField(ctx, 2, "double").upload(b)
+    dt = ib.DeviceField(ctx, 2, "double").upload(t)
+    loss, grads = net.loss_grad(ctx, db, dt)
+    lat = ptc.Lattice(L, u)
+    loss_o, grads_o, _ = ptc.loss_grad(lat, Ws, ptc.spinor_to_feat(lat, b), ptc.spinor_to_feat(lat, t))
+    assert abs(loss - loss_o) < TOL_NET * loss_o
+    for g, go in zip(grads, grads_o):
+        assert rel(g, go) < 5e-2
+
+
+def _pair(L, seed):
+    u = ib.synth_gauge(L, 0.2, seed)
+    ctx = ib.Context(L, 0)
+    ctx.upload_gauge(u, force=True)
+    D = ib.Dirac_Wilson(0.5 / 0.12 - 4, u, ctx=ctx)
+    V = int(np.prod(L))
+    b = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(V, seed + 1))
+    return ctx, D, b
+
+
+def test_gcr_converges_with_and_without_network():
+    L = [8, 8, 8, 8]
+    ctx, D, b = _pair(L, 61)
+    x_cg = ib.DeviceField(ctx, 2, "double")
+    outs, rc = ib.Solver_CG(1e-20, 5000, ib.Fopr_DdagD(D)).solve_field(b, x_cg)
+    ref = x_cg.download()
+    for net in (None, learned.PTCNet(ctx, learned.DEFAULT_WIDTHS)):
+        x = ib.DeviceField(ctx, 2, "double")
+        o, st = learned.Solver_GCR(D, net).solve_field(b, x)
+        assert st == ib.OK and o.diff < 1e-10
+        assert rel(x.download(), ref) < 1e-8
+
+
+def test_training_lowers_loss_and_gcr_iterations():
+    L = [8, 8, 8, 8]
+    pairs = learned.make_pairs(L, 4, seed0=7100)
+    net = learned.PTCNet(pairs[0].ctx, learned.DEFAULT_WIDTHS)
+    hist = learned.train(net, pairs, epochs=12, lr=3e-3)
+    assert hist[-1] < 0.7 * hist[0]
+    # an unseen field: fewer GCR iterations with the trained network than with none
+    ctx, D, b = _pair(L, 7900)
+    its = {}
+    for name, n in (("none", None), ("trained", net)):
+        x = ib.DeviceField(ctx, 2, "double")
+        o, st = learned.Solver_GCR(D, n).solve_field(b, x)
+        assert st == ib.OK and o.diff < 1e-10
+        its[name] = o.iterations
+    assert its["trained"] < its["none"], its
