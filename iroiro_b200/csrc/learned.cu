@@ -472,7 +472,14 @@ static cudaError_t bwd_t(const PtcGeo& G, const float2* in, const float2* dy, fl
   using S = Ptc<CIN, COUT>;
   const int grid = (G.V + kTileSites - 1) / kTileSites;
   if (din) {
-    const int smem = 128 * S::NP * 2 + S::KP * S::NP * 2;
+    // the pass accumulator takes up to 256 TMEM columns: ask for enough shared
+    // memory that at most two CTAs share an SM (2 x 256 = its 512 columns),
+    // so tensor-memory allocation never has to wait
+    constexpr int NCH = S::KP <= 256 ? S::KP : S::KP / 2;
+    constexpr int TC = NCH <= 32 ? 32 : (NCH <= 64 ? 64 : (NCH <= 128 ? 128 : 256));
+    const int need = 128 * S::NP * 2 + S::KP * S::NP * 2;
+    const int cap = TC >= 256 ? 100 * 1024 : (TC >= 128 ? 52 * 1024 : 0);
+    const int smem = need > cap ? need : cap;
     static bool attr = false;
     if (!attr) {
       cudaError_t e = cudaFuncSetAttribute(ptc_da_kernel<CIN, COUT>,
