@@ -167,16 +167,24 @@ class Adam:
 @dataclass
 class TrainingPair:
     ctx: Context          # holds the pair's gauge field
-    b: DeviceField
-    x: DeviceField
-    cg_iterations: int
+    b: DeviceField        # network input
+    x: DeviceField        # target, the exact (D^dag D)^-1 b
+    cg_iterations: int    # 0 for kind="random" (no solve is needed)
 
 
 def make_pairs(L, nfields: int, kappa: float = 0.12, eps: float = 0.2, seed0: int = 5000,
-               op=OP_WILSON_FULL, csw: float = 0.0, device: int = 0):
-    """(source, solution) pairs: a seeded gauge field per pair, a Gaussian
-    source b and x = (D^dag D)^-1 b from the plain FP64 CG to 1e-10."""
+               op=OP_WILSON_FULL, csw: float = 0.0, device: int = 0, kind: str = "random"):
+    """Training pairs (b, x) with x = (D^dag D)^-1 b, one seeded gauge field each.
+
+    kind="random" (the default): x = v is a Gaussian field and b = D^dag D v,
+    the cost |N(D^dag D v) - v|^2 of Lehner & Wettig, which weights every
+    eigenmode of the operator alike and needs no solve.  kind="solve": b is
+    Gaussian and x comes from the plain FP64 CG to 1e-10; that target is
+    dominated by the lowest modes, which a local network cannot represent,
+    and trains a much weaker preconditioner."""
     from . import Dirac_Clover, Dirac_Wilson, synth_gauge, synth_gaussian
+    if kind not in ("random", "solve"):
+        raise ValueError(f"unknown pair kind {kind!r}")
     mass = 0.5 / kappa - 4.0
     V = int(np.prod(L))
     pairs = []
@@ -187,7 +195,12 @@ def make_pairs(L, nfields: int, kappa: float = 0.12, eps: float = 0.2, seed0: in
         D = Dirac_Wilson(mass, u, ctx=ctx)
         if op == OP_CLOVER_FULL:
             D = Dirac_Clover(D, csw, u, ctx=ctx)
-        b = DeviceField(ctx, 2, "double").upload(synth_gaussian(V, seed0 + 100000 + k))
+        g = synth_gaussian(V, seed0 + 100000 + k)
+        if kind == "random":
+            b = DeviceField(ctx, 2, "double").upload(Fopr_DdagD(D).mult(g))
+            pairs.append(TrainingPair(ctx, b, DeviceField(ctx, 2, "double").upload(g), 0))
+            continue
+        b = DeviceField(ctx, 2, "double").upload(g)
         x = DeviceField(ctx, 2, "double")
         outs, rc = Solver_CG(1e-20, 20000, Fopr_DdagD(D)).solve_field(b, x)
         if rc != OK:

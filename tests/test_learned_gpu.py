@@ -85,7 +85,7 @@ def test_training_lowers_loss_and_gcr_iterations():
     pairs = learned.make_pairs(L, 4, seed0=7100)
     net = learned.PTCNet(pairs[0].ctx, learned.DEFAULT_WIDTHS)
     hist = learned.train(net, pairs, epochs=12, lr=3e-3)
-    assert hist[-1] < 0.7 * hist[0]
+    assert hist[-1] < 0.3 * hist[0]
     # an unseen field: fewer GCR iterations with the trained network than with none
     ctx, D, b = _pair(L, 7900)
     its = {}
@@ -93,5 +93,6 @@ def test_training_lowers_loss_and_gcr_iterations():
         x = ib.DeviceField(ctx, 2, "double")
         o, st = learned.Solver_GCR(D, n).solve_field(b, x)
         assert st == ib.OK and o.diff < 1e-10
-        its[name] = o.iterations
-    assert its["trained"] < its["none"], its
+        its[name] = (o.iterations, o.fallback)
+    # the trained network removes the stall (no CG fallback) and most iterations
+    assert its["trained"][1] == 0 and its["trained"][0] < 0.6 * its["none"][0], its
