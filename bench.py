@@ -27,6 +27,7 @@ into oracle/_ref) on the host cores for the same metric, config and step.
 from __future__ import annotations
 
 import argparse
+import re
 import json
 import os
 import statistics
@@ -167,16 +168,14 @@ def barrier(world: int):
 
 
 def traffic_per_launch(vh: int):
-    """DRAM bytes per hopping launch from the committed ncu summary, scaled
-    from the captured lattice to this one by the sites processed."""
-    p = ROOT / "profiles" / "hop_fp64_traffic.json"
+    """DRAM bytes (read + write) of one Schur application (both hop launches)
+    from the committed ncu summary, scaled from the captured lattice to this
+    one by the sites processed."""
+    p = ROOT / "profiles" / "hop_fp64_24x24x24x48.txt"
     if not p.exists():
         return None
-    try:
-        d = json.loads(p.read_text())
-        return float(d["dram_bytes_per_site"]) * vh
-    except (KeyError, ValueError):
-        return None
+    m = re.search(r"^dram_bytes_per_site_schur:\s*([0-9.]+)", p.read_text(), re.M)
+    return float(m.group(1)) * vh if m else None
 
 
 def measured_peak():
@@ -464,6 +463,10 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic,
                      "peak_kind": peak_kind,
+                     "dram_GBps": None if traffic is None else
+                     round(traffic / ((t_ms / args.steps) * 1e-3) / 1e9, 1),
+                     "dram_frac": None if traffic is None else
+                     round(traffic / ((t_ms / args.steps) * 1e-3) / 1e9 / peak, 3),
                      "bytes_model": "per even site: hop 2496 + hop 2496 + f_e 192 (FP64, recon-12)",
                      "gflops": round(FLOPS_SCHUR * Vh / ((t_ms / args.steps) * 1e-3) / 1e9, 1)},
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": 24 * 8 * Vh,
