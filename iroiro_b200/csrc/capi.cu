@@ -238,10 +238,14 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
   cudaStream_t st = c->stream;
   static const char* forced = std::getenv("IRO_HOP_VARIANT");
   auto it = c->tuned.find(key);
+  // two right-hand sides per thread (variant bit 2) needs FP32/FP16 storage,
+  // reconstruct-12 links and an even number of right-hand sides
+  const bool pair_ok = L.prec != PREC_DOUBLE && L.recon == 12 && L.nrhs % 2 == 0;
+  const int nvar = pair_ok ? 8 : 4;
   if (forced) {
     int v = 0, b = 256;
     std::sscanf(forced, "%d,%d", &v, &b);
-    c->tuned[key] = {v & 3, b};
+    c->tuned[key] = {v & (nvar - 1), b};
     it = c->tuned.find(key);
   }
   if (it == c->tuned.end()) {
@@ -260,7 +264,7 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
     std::pair<int, int> pick{0, 256};
-    for (int v = 0; v < 4; ++v)
+    for (int v = 0; v < nvar; ++v)
       for (int b : {256, 128}) {
         T.variant = v;
         T.block_cap = b;

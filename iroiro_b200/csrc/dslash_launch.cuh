@@ -3,6 +3,8 @@
 #pragma once
 
 #include "dslash.cuh"
+#include "dslash_pair.cuh"
+#include "dslash_stage.cuh"
 #include "internal.h"
 
 namespace iro {
@@ -30,13 +32,86 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// two right-hand sides per thread (FP32/FP16, reconstruct-12, even nrhs)
+template <int SP, int RECON, bool DAG, int EPI, int VAR>
+static cudaError_t hop_go_pair(const HopLaunch& L, cudaStream_t st) {
+  if constexpr (SP == PREC_DOUBLE || RECON != 12) {
+    return cudaErrorInvalidValue;
+  } else {
+    if (L.nrhs % 2 != 0) return cudaErrorInvalidValue;
+    HopParams P;
+    P.g = L.g;
+    P.p0 = L.p0;
+    P.nrhs = L.nrhs;
+    for (int i = 0; i < 2; ++i) {
+      P.in[i] = L.in[i];
+      P.out[i] = L.out[i];
+      P.xin[i] = L.xin[i];
+      P.clov[i] = L.clov[i];
+    }
+    P.gauge = L.gauge;
+    P.scale = L.scale;
+    P.red_mask = L.red_mask;
+    P.red = L.red;
+    P.skip = L.skip;
+    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
+    dim3 grid(c.grid, L.nparity);
+    hop_pair_kernel<SP, DAG, EPI, VAR><<<grid, c.block, 0, st>>>(P);
+    return cudaGetLastError();
+  }
+}
+
+// two right-hand sides per thread with shared-memory staging of the neighbours
+template <int SP, int RECON, bool DAG, int EPI, int VAR>
+static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
+  if constexpr (SP == PREC_DOUBLE || RECON != 12) {
+    return cudaErrorInvalidValue;
+  } else {
+    if (L.nrhs % 2 != 0) return cudaErrorInvalidValue;
+    HopParams P;
+    P.g = L.g;
+    P.p0 = L.p0;
+    P.nrhs = L.nrhs;
+    for (int i = 0; i < 2; ++i) {
+      P.in[i] = L.in[i];
+      P.out[i] = L.out[i];
+      P.xin[i] = L.xin[i];
+      P.clov[i] = L.clov[i];
+    }
+    P.gauge = L.gauge;
+    P.scale = L.scale;
+    P.red_mask = L.red_mask;
+    P.red = L.red;
+    P.skip = L.skip;
+    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
+    const int smem = kStages * StageSlots<SP>::N * 16 * c.block;
+    static int opted = 0;  // largest dynamic shared memory already allowed
+    if (smem > opted) {
+      cudaError_t e = cudaFuncSetAttribute(hop_stage_kernel<SP, DAG, EPI, VAR>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      opted = smem;
+    }
+    dim3 grid(c.grid, L.nparity);
+    hop_stage_kernel<SP, DAG, EPI, VAR><<<grid, c.block, smem, st>>>(P);
+    return cudaGetLastError();
+  }
+}
+
+// variant bits 0-1: see hop_kernel; variants 4/5: two right-hand sides per
+// thread (5 with the two-blocks-per-SM register cap); 6/7: the same with the
+// neighbours staged through shared memory
 template <int SP, int GP, int RECON, bool DAG, int EPI>
 static cudaError_t hop_var(const HopLaunch& L, cudaStream_t st) {
-  switch (L.variant & 3) {
+  switch (L.variant & 7) {
     case 0: return hop_go<SP, GP, RECON, DAG, EPI, 0>(L, st);
     case 1: return hop_go<SP, GP, RECON, DAG, EPI, 1>(L, st);
     case 2: return hop_go<SP, GP, RECON, DAG, EPI, 2>(L, st);
-    default: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
+    case 3: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
+    case 4: return hop_go_pair<SP, RECON, DAG, EPI, 0>(L, st);
+    case 5: return hop_go_pair<SP, RECON, DAG, EPI, 1>(L, st);
+    case 6: return hop_go_stage<SP, RECON, DAG, EPI, 0>(L, st);
+    default: return hop_go_stage<SP, RECON, DAG, EPI, 1>(L, st);
   }
 }
 

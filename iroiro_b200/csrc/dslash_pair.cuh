@@ -1,0 +1,420 @@
+// The FP32/FP16 hopping stencil with two right-hand sides per thread, in the
+// packed FP32x2 arithmetic of sm_100 (__ffma2_rn, __fadd2_rn, __fmul2_rn).
+//
+// For an even number of right-hand sides, lane q of a site computes
+// right-hand sides 2q and 2q+1.  Both run through one instruction stream with
+// their values in the two halves of a float2 ("pair"), so
+//   * every link (load, FP16 conversion, reconstruction of row 2) and every
+//     neighbour index serves two right-hand sides, and
+//   * each FP32 add or multiply-add of projection, SU(3) product and
+//     reconstruction is one instruction for both.
+// The spin algebra is that of hop_kernel (Dirac_Wilson::mult_offdiag,
+// lib/Dirac_ops/dirac_wilson.cpp:107-113, per-direction projection as in
+// lib/Dirac_ops/dirac_wilson_improved.code:5-648).  Arithmetic stays FP32;
+// only the association of the sums differs from hop_kernel, so results agree
+// with it to FP32 rounding, not bit for bit.  The two elements of a pair are
+// adjacent in the warp-blocked layout (elements hs*nrhs + 2q and +1, never
+// split across a 32-element block since 2q is even), so a pair is two
+// neighbouring 16-byte chunks per chunk index.
+#pragma once
+
+#include "dslash.cuh"
+
+namespace iro {
+
+// one complex number of each of two right-hand sides
+struct Cp {
+  float2 re, im;
+};
+
+__device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, bc(-1.f), a); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+__device__ __forceinline__ Cp cadd(Cp a, Cp b) { return {padd(a.re, b.re), padd(a.im, b.im)}; }
+__device__ __forceinline__ Cp csub(Cp a, Cp b) { return {psub(a.re, b.re), psub(a.im, b.im)}; }
+// a + i b, a - i b
+__device__ __forceinline__ Cp cadd_i(Cp a, Cp b) { return {psub(a.re, b.im), padd(a.im, b.re)}; }
+__device__ __forceinline__ Cp csub_i(Cp a, Cp b) { return {padd(a.re, b.im), psub(a.im, b.re)}; }
+
+// ---- pair storage access -------------------------------------------------------------
+template <int SP>
+struct PairIO;
+
+template <>
+struct PairIO<PREC_SINGLE> {
+  // elements i0, i0+1 (i0 even); w = (1, 1)
+  __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i0, Cp f[12], float2& w) {
+    const float4* p = static_cast<const float4*>(s.data) + blk0<6>(i0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float4 a = __ldg(p + 32 * k), b = __ldg(p + 32 * k + 1);
+      f[2 * k] = {make_float2(a.x, b.x), make_float2(a.y, b.y)};
+      f[2 * k + 1] = {make_float2(a.z, b.z), make_float2(a.w, b.w)};
+    }
+    w = bc(1.f);
+  }
+  __device__ __forceinline__ static void load_scaled(const SpinorPtr& s, int64_t i0, Cp f[12]) {
+    float2 w;
+    load(s, i0, f, w);
+  }
+  __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i0, const Cp v[12]) {
+    float4* p = static_cast<float4*>(s.data) + blk0<6>(i0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const Cp a = v[2 * k], b = v[2 * k + 1];
+      p[32 * k] = make_float4(a.re.x, a.im.x, b.re.x, b.im.x);
+      p[32 * k + 1] = make_float4(a.re.y, a.im.y, b.re.y, b.im.y);
+    }
+  }
+};
+
+template <>
+struct PairIO<PREC_HALF> {
+  // the stored (normalised) values of elements i0, i0+1 and their norms w
+  __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i0, Cp f[12], float2& w) {
+    const uint4* p = static_cast<const uint4*>(s.data) + blk0<3>(i0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const uint4 a = __ldg(p + 32 * k), b = __ldg(p + 32 * k + 1);
+      const uint32_t av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const float2 x = unpack_h2(av[m]), y = unpack_h2(bv[m]);
+        f[4 * k + m] = {make_float2(x.x, y.x), make_float2(x.y, y.y)};
+      }
+    }
+    w = __ldg(reinterpret_cast<const float2*>(s.norm + i0));
+  }
+  __device__ __forceinline__ static void load_scaled(const SpinorPtr& s, int64_t i0, Cp f[12]) {
+    float2 w;
+    load(s, i0, f, w);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f[k] = {pmul(f[k].re, w), pmul(f[k].im, w)};
+  }
+  __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i0, const Cp v[12]) {
+    float m0 = 0.f, m1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      m0 = fmaxf(m0, fmaxf(fabsf(v[k].re.x), fabsf(v[k].im.x)));
+      m1 = fmaxf(m1, fmaxf(fabsf(v[k].re.y), fabsf(v[k].im.y)));
+    }
+    // the same subnormal flush as SpinorIO<PREC_HALF>::store
+    if (!(m0 >= 1e-37f)) m0 = 0.f;
+    if (!(m1 >= 1e-37f)) m1 = 0.f;
+    const float2 inv = make_float2(m0 > 0.f ? 1.0f / m0 : 0.f, m1 > 0.f ? 1.0f / m1 : 0.f);
+    uint4* p = static_cast<uint4*>(s.data) + blk0<3>(i0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      uint32_t a[4], b[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const float2 re = pmul(v[4 * k + m].re, inv), im = pmul(v[4 * k + m].im, inv);
+        a[m] = pack_h2(re.x, im.x);
+        b[m] = pack_h2(re.y, im.y);
+      }
+      p[32 * k] = make_uint4(a[0], a[1], a[2], a[3]);
+      p[32 * k + 1] = make_uint4(b[0], b[1], b[2], b[3]);
+    }
+    *reinterpret_cast<float2*>(s.norm + i0) = make_float2(m0, m1);
+  }
+};
+
+// one right-hand side of a pair <-> a plain complex array (for the clover epilogue)
+__device__ __forceinline__ void pair_get(const Cp v[12], int j, Cx<float> o[12]) {
+#pragma unroll
+  for (int k = 0; k < 12; ++k) o[k] = j ? Cx<float>{v[k].re.y, v[k].im.y} : Cx<float>{v[k].re.x, v[k].im.x};
+}
+__device__ __forceinline__ void pair_set(Cp v[12], int j, const Cx<float> o[12]) {
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    if (j) {
+      v[k].re.y = o[k].re;
+      v[k].im.y = o[k].im;
+    } else {
+      v[k].re.x = o[k].re;
+      v[k].im.x = o[k].im;
+    }
+  }
+}
+
+// ---- spin projection / reconstruction (same gammas as project/reconstruct) -------------
+// For the t direction the projector's factor 2 is left to the reconstruction
+// weight, so the projection is a plain selection.
+template <int MU, int S>
+__device__ __forceinline__ void project_pair(const Cp f[12], Cp h[6]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const Cp f0 = f[c], f1 = f[3 + c], f2 = f[6 + c], f3 = f[9 + c];
+    if (MU == 0) {  // h0 = f0 + S i f3, h1 = f1 + S i f2
+      h[c] = (S > 0) ? cadd_i(f0, f3) : csub_i(f0, f3);
+      h[3 + c] = (S > 0) ? cadd_i(f1, f2) : csub_i(f1, f2);
+    } else if (MU == 1) {  // h0 = f0 + S f3, h1 = f1 - S f2
+      h[c] = (S > 0) ? cadd(f0, f3) : csub(f0, f3);
+      h[3 + c] = (S > 0) ? csub(f1, f2) : cadd(f1, f2);
+    } else if (MU == 2) {  // h0 = f0 + S i f2, h1 = f1 - S i f3
+      h[c] = (S > 0) ? cadd_i(f0, f2) : csub_i(f0, f2);
+      h[3 + c] = (S > 0) ? csub_i(f1, f3) : cadd_i(f1, f3);
+    } else {  // t: (2 f2, 2 f3) for S=+1, (2 f0, 2 f1) for S=-1; the 2 goes to the weight
+      h[c] = (S > 0) ? f2 : f0;
+      h[3 + c] = (S > 0) ? f3 : f1;
+    }
+  }
+}
+
+// a += w b, a += w (i b), a += w (-i b), with nw = -w
+__device__ __forceinline__ void acc_w(Cp& a, float2 w, const Cp& b) {
+  a.re = pfma(w, b.re, a.re);
+  a.im = pfma(w, b.im, a.im);
+}
+__device__ __forceinline__ void acc_wi(Cp& a, float2 w, float2 nw, const Cp& b) {
+  a.re = pfma(nw, b.im, a.re);
+  a.im = pfma(w, b.re, a.im);
+}
+__device__ __forceinline__ void acc_wmi(Cp& a, float2 w, float2 nw, const Cp& b) {
+  a.re = pfma(w, b.im, a.re);
+  a.im = pfma(nw, b.re, a.im);
+}
+
+// acc += w * (1 - S gamma_mu) reconstructed from g
+template <int MU, int S>
+__device__ __forceinline__ void reconstruct_pair(Cp acc[12], const Cp g[6], float2 w) {
+  const float2 nw = pmul(w, bc(-1.f));
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const Cp g0 = g[c], g1 = g[3 + c];
+    if (MU == 3) {
+      if (S > 0) {
+        acc_w(acc[6 + c], w, g0);
+        acc_w(acc[9 + c], w, g1);
+      } else {
+        acc_w(acc[c], w, g0);
+        acc_w(acc[3 + c], w, g1);
+      }
+      continue;
+    }
+    acc_w(acc[c], w, g0);
+    acc_w(acc[3 + c], w, g1);
+    if (MU == 0) {  // [h0, h1, -S i h1, -S i h0]
+      if (S > 0) {
+        acc_wmi(acc[6 + c], w, nw, g1);
+        acc_wmi(acc[9 + c], w, nw, g0);
+      } else {
+        acc_wi(acc[6 + c], w, nw, g1);
+        acc_wi(acc[9 + c], w, nw, g0);
+      }
+    } else if (MU == 1) {  // [h0, h1, -S h1, S h0]
+      if (S > 0) {
+        acc_w(acc[6 + c], nw, g1);
+        acc_w(acc[9 + c], w, g0);
+      } else {
+        acc_w(acc[6 + c], w, g1);
+        acc_w(acc[9 + c], nw, g0);
+      }
+    } else {  // MU==2: [h0, h1, -S i h0, S i h1]
+      if (S > 0) {
+        acc_wmi(acc[6 + c], w, nw, g0);
+        acc_wi(acc[9 + c], w, nw, g1);
+      } else {
+        acc_wi(acc[6 + c], w, nw, g0);
+        acc_wmi(acc[9 + c], w, nw, g1);
+      }
+    }
+  }
+}
+
+// g = U h (ADJ false) or U^dag h (ADJ true) for the two colour vectors of h;
+// the link elements are broadcast to both lanes
+template <bool ADJ>
+__device__ __forceinline__ void su3_pair(const Su3<float>& U, const Cp h[6], Cp g[6]) {
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float2 s1, s2, s3;  // re = s1 -/+ s2, im = s3 (one chain) -- see below
+      const Cx<float> u0 = ADJ ? U.e[0][a] : U.e[a][0];
+      const Cx<float> u1 = ADJ ? U.e[1][a] : U.e[a][1];
+      const Cx<float> u2 = ADJ ? U.e[2][a] : U.e[a][2];
+      const Cp h0 = h[3 * v], h1 = h[3 * v + 1], h2 = h[3 * v + 2];
+      if (!ADJ) {
+        // re = sum ur h.re - sum ui h.im,  im = sum ur h.im + ui h.re
+        s1 = pmul(bc(u0.re), h0.re);
+        s1 = pfma(bc(u1.re), h1.re, s1);
+        s1 = pfma(bc(u2.re), h2.re, s1);
+        s2 = pmul(bc(u0.im), h0.im);
+        s2 = pfma(bc(u1.im), h1.im, s2);
+        s2 = pfma(bc(u2.im), h2.im, s2);
+        s3 = pmul(bc(u0.re), h0.im);
+        s3 = pfma(bc(u0.im), h0.re, s3);
+        s3 = pfma(bc(u1.re), h1.im, s3);
+        s3 = pfma(bc(u1.im), h1.re, s3);
+        s3 = pfma(bc(u2.re), h2.im, s3);
+        s3 = pfma(bc(u2.im), h2.re, s3);
+        g[3 * v + a] = {psub(s1, s2), s3};
+      } else {
+        // conj(u): re = sum ur h.re + ui h.im,  im = sum ur h.im - sum ui h.re
+        s3 = pmul(bc(u0.re), h0.re);
+        s3 = pfma(bc(u0.im), h0.im, s3);
+        s3 = pfma(bc(u1.re), h1.re, s3);
+        s3 = pfma(bc(u1.im), h1.im, s3);
+        s3 = pfma(bc(u2.re), h2.re, s3);
+        s3 = pfma(bc(u2.im), h2.im, s3);
+        s1 = pmul(bc(u0.re), h0.im);
+        s1 = pfma(bc(u1.re), h1.im, s1);
+        s1 = pfma(bc(u2.re), h2.im, s1);
+        s2 = pmul(bc(u0.im), h0.re);
+        s2 = pfma(bc(u1.im), h1.re, s2);
+        s2 = pfma(bc(u2.im), h2.re, s2);
+        g[3 * v + a] = {s3, psub(s1, s2)};
+      }
+    }
+  }
+}
+
+// Forward and backward contributions of direction MU for the pair at
+// element e0 (= site * nrhs + 2q) of every neighbour.
+template <int MU, bool DAG, int SP>
+__device__ __forceinline__ void hop_dir_pair(const GaugePtr& gauge, const SpinorPtr& in, int p,
+                                             int hs, const int nb[8], int nrhs, int r0,
+                                             Cp acc[12]) {
+  constexpr float kT = (MU == 3) ? 2.f : 1.f;  // the t projector's factor 2
+  {
+    Su3<float> U;
+    GaugeIO<SP, 12>::load(gauge, p, MU, hs, U);
+    constexpr int S = DAG ? -1 : 1;
+    Cp f[12], h[6], g[6];
+    float2 w;
+    PairIO<SP>::load(in, int64_t(nb[2 * MU]) * nrhs + r0, f, w);
+    project_pair<MU, S>(f, h);
+    su3_pair<false>(U, h, g);
+    reconstruct_pair<MU, S>(acc, g, kT == 1.f ? w : pmul(w, bc(kT)));
+  }
+  {
+    Su3<float> U;
+    GaugeIO<SP, 12>::load(gauge, 1 - p, MU, nb[2 * MU + 1], U);
+    constexpr int S = DAG ? 1 : -1;
+    Cp f[12], h[6], g[6];
+    float2 w;
+    PairIO<SP>::load(in, int64_t(nb[2 * MU + 1]) * nrhs + r0, f, w);
+    project_pair<MU, S>(f, h);
+    su3_pair<true>(U, h, g);
+    reconstruct_pair<MU, S>(acc, g, kT == 1.f ? w : pmul(w, bc(kT)));
+  }
+}
+
+// Epilogue of one site for a pair: scale / clover / x + a*y, store, and the
+// per-site FP32 sums of the reductions added to red[] in FP64.
+template <int SP, int EPI>
+__device__ __forceinline__ void pair_epilogue(const HopParams& P, int yi, int hs, int64_t e0,
+                                              Cp acc[12], double red[6]) {
+  const float2 sc = bc(float(P.scale));
+  Cp xv[12];
+  if (EPI == EPI_SCALE || EPI == EPI_SCALE_CLOV) {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = {pmul(sc, acc[k].re), pmul(sc, acc[k].im)};
+    if (EPI == EPI_SCALE_CLOV) {
+      CloverBlock<float> B[2];
+      CloverIO<SP>::load(P.clov[yi], hs, B);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        Cx<float> v[12];
+        pair_get(acc, j, v);
+        clover_apply(B, v);
+        pair_set(acc, j, v);
+      }
+    }
+  } else {
+    PairIO<SP>::load_scaled(P.xin[yi], e0, xv);
+    Cp ax[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) ax[k] = xv[k];
+    if (EPI == EPI_XPAY_CLOV) {
+      CloverBlock<float> B[2];
+      CloverIO<SP>::load(P.clov[yi], hs, B);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        Cx<float> v[12];
+        pair_get(ax, j, v);
+        clover_apply(B, v);
+        pair_set(ax, j, v);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 12; ++k)
+      acc[k] = {pfma(sc, acc[k].re, ax[k].re), pfma(sc, acc[k].im, ax[k].im)};
+  }
+  PairIO<SP>::store(P.out[yi], e0, acc);
+  if (P.red_mask) {
+    float2 o2 = bc(0.f), x2 = bc(0.f), xo = bc(0.f);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      o2 = pfma(acc[k].re, acc[k].re, o2);
+      o2 = pfma(acc[k].im, acc[k].im, o2);
+      if (EPI == EPI_XPAY || EPI == EPI_XPAY_CLOV) {
+        x2 = pfma(xv[k].re, xv[k].re, x2);
+        x2 = pfma(xv[k].im, xv[k].im, x2);
+        xo = pfma(xv[k].re, acc[k].re, xo);
+        xo = pfma(xv[k].im, acc[k].im, xo);
+      }
+    }
+    red[0] += o2.x;
+    red[1] += x2.x;
+    red[2] += xo.x;
+    red[3] += o2.y;
+    red[4] += x2.y;
+    red[5] += xo.y;
+  }
+}
+
+// The stencil over pairs; same parameters, epilogues and reductions as
+// hop_kernel.  A pair is skipped only when both its right-hand sides are
+// flagged converged; a pair with one converged member still writes it (its
+// outputs are scratch, and the solvers' stage updates ignore its sums).
+// Per-site sums of the reductions are formed in FP32 and accumulated in FP64.
+template <int SP, bool DAG, int EPI, int VAR>
+__global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_pair_kernel(HopParams P) {
+  const int yi = blockIdx.y;
+  const int p = P.p0 ^ yi;
+  const int nrhs = P.nrhs;
+  const int lanes = nrhs >> 1;
+  const int nthreads = P.g.Vh * lanes;  // < 2^31, checked at context creation
+  double red[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // the grid stride is a multiple of lanes, so each thread keeps one pair
+  const int q = (lanes == 1) ? 0 : int((blockIdx.x * blockDim.x + threadIdx.x) % unsigned(lanes));
+  const int r0 = 2 * q;
+  const bool idle = P.skip && P.skip[r0] && P.skip[r0 + 1];
+  for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < nthreads && !idle;
+       tid += gridDim.x * blockDim.x) {
+    const int hs = (lanes == 1) ? tid : int(unsigned(tid) / unsigned(lanes));
+    const Coord c = coord_of(P.g, hs, p);
+    int nb[8];
+    neighbours(P.g, c, hs, nb);
+    Cp acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = {bc(0.f), bc(0.f)};
+    if (VAR & 2) {
+#pragma unroll 1
+      for (int mu = 0; mu < 4; ++mu) {
+        switch (mu) {
+          case 0: hop_dir_pair<0, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
+          case 1: hop_dir_pair<1, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
+          case 2: hop_dir_pair<2, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
+          default: hop_dir_pair<3, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
+        }
+      }
+    } else {
+      hop_dir_pair<0, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+      hop_dir_pair<1, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+      hop_dir_pair<2, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+      hop_dir_pair<3, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+    }
+    pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, acc, red);
+  }
+  if (P.red_mask)
+    block_reduce_finish<3, 2>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,
+                              gridDim.x * gridDim.y);
+}
+
+}  // namespace iro

@@ -99,6 +99,15 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
         s[r].beta = s[r].rr / s[r].rr_prev;
         if (s[r].iter >= R.max_iter) R.done[r] = STOPPED;
       }
+      // mixed precision: when one right-hand side pauses, the others pause
+      // with it, so all share one FP64 residual recomputation (which treats
+      // every right-hand side in one launch anyway) instead of idling in
+      // lockstep until each reaches its own trigger
+      bool any_pause = false;
+      for (int r = 0; r < nrhs; ++r) any_pause = any_pause || R.done[r] == PAUSED;
+      if (any_pause)
+        for (int r = 0; r < nrhs; ++r)
+          if (R.done[r] == RUNNING && s[r].delta2 > 0.0) R.done[r] = PAUSED;
     } break;
     case ST_MS_ALPHA: {
       MSState* m = static_cast<MSState*>(R.state);
@@ -166,28 +175,32 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
   }
 }
 
-// Block size must be nrhs * 2^k (so each thread keeps one right-hand side
-// across a grid-stride loop whose stride is a multiple of nrhs).
-template <int NRED>
+// Each thread holds RPT consecutive right-hand sides: v[j*NRED + k] is value k
+// of right-hand side (RPT*t + j) mod nrhs.  Block size must be (nrhs/RPT)*2^k
+// (so each thread keeps its right-hand sides across a grid-stride loop whose
+// stride is a multiple of nrhs/RPT).
+template <int NRED, int RPT = 1>
 __device__ void block_reduce_finish(const Reduce& R, const double* v, int nrhs, int bid, int nblk) {
-  __shared__ double sm[NRED][256];
+  __shared__ double sm[NRED][256 * RPT];
   __shared__ bool last;
   const int t = threadIdx.x;
   const int n = blockDim.x;
 #pragma unroll
-  for (int k = 0; k < NRED; ++k) sm[k][t] = v[k];
-  __syncthreads();
-  for (int s = (n / nrhs) / 2; s > 0; s >>= 1) {
-    if (t < s * nrhs) {
+  for (int j = 0; j < RPT; ++j)
 #pragma unroll
-      for (int k = 0; k < NRED; ++k) sm[k][t] += sm[k][t + s * nrhs];
+    for (int k = 0; k < NRED; ++k) sm[k][RPT * t + j] = v[j * NRED + k];
+  __syncthreads();
+  for (int s = (RPT * n / nrhs) / 2; s > 0; s >>= 1) {
+    for (int u = t; u < s * nrhs; u += n) {
+#pragma unroll
+      for (int k = 0; k < NRED; ++k) sm[k][u] += sm[k][u + s * nrhs];
     }
     __syncthreads();
   }
   const int nv = NRED * nrhs;
-  if (t < nrhs) {
+  for (int u = t; u < nrhs; u += n) {
 #pragma unroll
-    for (int k = 0; k < NRED; ++k) R.partials[int64_t(bid) * nv + k * nrhs + t] = sm[k][t];
+    for (int k = 0; k < NRED; ++k) R.partials[int64_t(bid) * nv + k * nrhs + u] = sm[k][u];
   }
   __threadfence();
   __syncthreads();

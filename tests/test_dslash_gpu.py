@@ -149,4 +149,10 @@ def test_multi_rhs_equals_single(prec):
     blk = c.apply(ib.OP_CLOVER_SCHUR_EE, m, 1.0, 0, fs.ravel(), prec, nrhs=12).reshape(12, -1)
     for r in range(12):
         one = c.apply(ib.OP_CLOVER_SCHUR_EE, m, 1.0, 0, fs[r], prec)
-        assert np.array_equal(blk[r], one)
+        if prec == "double":
+            assert np.array_equal(blk[r], one)
+        else:
+            # FP32/FP16 blocks may run two right-hand sides per thread in
+            # packed FP32x2 arithmetic: equal to FP32 rounding, not bitwise
+            tol = TOL_FP32 if prec == "single" else TOL_FP16
+            assert np.linalg.norm(blk[r] - one) < tol * np.linalg.norm(one)
