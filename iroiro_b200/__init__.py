@@ -24,6 +24,7 @@ device is missing.
 from __future__ import annotations
 
 import ctypes
+import weakref
 import os
 import threading
 from dataclasses import dataclass
@@ -194,6 +195,8 @@ class Context:
             raise IroError(rc, f"iro_ctx_create({self.L}, device={device})")
         self.h = h
         self._gauge_key = None
+        # fields and networks of this context, closed before it
+        self._owned = weakref.WeakSet()
 
     def check(self, rc: int, what: str):
         if rc == OK:
@@ -205,6 +208,8 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            for obj in list(getattr(self, "_owned", ())):
+                obj.close()
             self._lib.iro_ctx_destroy(self.h)
             self.h = None
 
@@ -271,6 +276,7 @@ class DeviceField:
         ctx.check(ctx._lib.iro_field_create(ctx.h, subset, self.prec, nrhs, ctypes.byref(h)),
                   "iro_field_create")
         self.h = h
+        ctx._owned.add(self)
 
     @property
     def size(self) -> int:

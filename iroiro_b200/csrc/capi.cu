@@ -20,6 +20,7 @@ using namespace iro;
 
 struct iro_field {
   iro_ctx* ctx;
+  int dev;  // device of the buffers (iro_field_destroy does not touch the context)
   DevField f;
 };
 
@@ -670,6 +671,7 @@ int iro_field_create(iro_ctx* c, int subset, int prec, int nrhs, iro_field** f) 
   CK(cudaSetDevice(c->device));
   std::unique_ptr<iro_field> h(new iro_field());
   h->ctx = c;
+  h->dev = c->device;
   int rc = alloc_field(c, subset, prec, nrhs, h->f);
   if (rc) return rc;
   CK(cudaMemset(h->f.data, 0, h->f.bytes_data));
@@ -680,7 +682,7 @@ int iro_field_create(iro_ctx* c, int subset, int prec, int nrhs, iro_field** f) 
 
 int iro_field_destroy(iro_field* f) {
   if (!f) return IRO_BAD_ARG;
-  cudaSetDevice(f->ctx->device);
+  cudaSetDevice(f->dev);  // the context may already be destroyed
   free_field(f->f);
   delete f;
   return IRO_OK;

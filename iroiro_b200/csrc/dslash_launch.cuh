@@ -84,7 +84,7 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
     P.red = L.red;
     P.skip = L.skip;
     LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
-    const int smem = kStages * StageSlots<SP>::N * 16 * c.block;
+    const int smem = stage_bytes<SP>() * c.block;
     static int opted = 0;  // largest dynamic shared memory already allowed
     if (smem > opted) {
       cudaError_t e = cudaFuncSetAttribute(hop_stage_kernel<SP, DAG, EPI, VAR>,

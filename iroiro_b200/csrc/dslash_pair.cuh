@@ -144,24 +144,27 @@ __device__ __forceinline__ void pair_set(Cp v[12], int j, const Cx<float> o[12])
 // For the t direction the projector's factor 2 is left to the reconstruction
 // weight, so the projection is a plain selection.
 template <int MU, int S>
+__device__ __forceinline__ void project_col(const Cp f0, const Cp f1, const Cp f2, const Cp f3, Cp& h0,
+                                            Cp& h1) {
+  if (MU == 0) {  // h0 = f0 + S i f3, h1 = f1 + S i f2
+    h0 = (S > 0) ? cadd_i(f0, f3) : csub_i(f0, f3);
+    h1 = (S > 0) ? cadd_i(f1, f2) : csub_i(f1, f2);
+  } else if (MU == 1) {  // h0 = f0 + S f3, h1 = f1 - S f2
+    h0 = (S > 0) ? cadd(f0, f3) : csub(f0, f3);
+    h1 = (S > 0) ? csub(f1, f2) : cadd(f1, f2);
+  } else if (MU == 2) {  // h0 = f0 + S i f2, h1 = f1 - S i f3
+    h0 = (S > 0) ? cadd_i(f0, f2) : csub_i(f0, f2);
+    h1 = (S > 0) ? csub_i(f1, f3) : cadd_i(f1, f3);
+  } else {  // t: (2 f2, 2 f3) for S=+1, (2 f0, 2 f1) for S=-1; the 2 goes to the weight
+    h0 = (S > 0) ? f2 : f0;
+    h1 = (S > 0) ? f3 : f1;
+  }
+}
+
+template <int MU, int S>
 __device__ __forceinline__ void project_pair(const Cp f[12], Cp h[6]) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const Cp f0 = f[c], f1 = f[3 + c], f2 = f[6 + c], f3 = f[9 + c];
-    if (MU == 0) {  // h0 = f0 + S i f3, h1 = f1 + S i f2
-      h[c] = (S > 0) ? cadd_i(f0, f3) : csub_i(f0, f3);
-      h[3 + c] = (S > 0) ? cadd_i(f1, f2) : csub_i(f1, f2);
-    } else if (MU == 1) {  // h0 = f0 + S f3, h1 = f1 - S f2
-      h[c] = (S > 0) ? cadd(f0, f3) : csub(f0, f3);
-      h[3 + c] = (S > 0) ? csub(f1, f2) : cadd(f1, f2);
-    } else if (MU == 2) {  // h0 = f0 + S i f2, h1 = f1 - S i f3
-      h[c] = (S > 0) ? cadd_i(f0, f2) : csub_i(f0, f2);
-      h[3 + c] = (S > 0) ? csub_i(f1, f3) : cadd_i(f1, f3);
-    } else {  // t: (2 f2, 2 f3) for S=+1, (2 f0, 2 f1) for S=-1; the 2 goes to the weight
-      h[c] = (S > 0) ? f2 : f0;
-      h[3 + c] = (S > 0) ? f3 : f1;
-    }
-  }
+  for (int c = 0; c < 3; ++c) project_col<MU, S>(f[c], f[3 + c], f[6 + c], f[9 + c], h[c], h[3 + c]);
 }
 
 // a += w b, a += w (i b), a += w (-i b), with nw = -w
@@ -178,99 +181,165 @@ __device__ __forceinline__ void acc_wmi(Cp& a, float2 w, float2 nw, const Cp& b)
   a.im = pfma(nw, b.re, a.im);
 }
 
-// acc += w * (1 - S gamma_mu) reconstructed from g
+// acc (colour c) += w * (1 - S gamma_mu) reconstructed from g0 = g[c], g1 = g[3+c]
 template <int MU, int S>
-__device__ __forceinline__ void reconstruct_pair(Cp acc[12], const Cp g[6], float2 w) {
-  const float2 nw = pmul(w, bc(-1.f));
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const Cp g0 = g[c], g1 = g[3 + c];
-    if (MU == 3) {
-      if (S > 0) {
-        acc_w(acc[6 + c], w, g0);
-        acc_w(acc[9 + c], w, g1);
-      } else {
-        acc_w(acc[c], w, g0);
-        acc_w(acc[3 + c], w, g1);
-      }
-      continue;
+__device__ __forceinline__ void reconstruct_col(Cp acc[12], int c, const Cp g0, const Cp g1, float2 w,
+                                                float2 nw) {
+  if (MU == 3) {
+    if (S > 0) {
+      acc_w(acc[6 + c], w, g0);
+      acc_w(acc[9 + c], w, g1);
+    } else {
+      acc_w(acc[c], w, g0);
+      acc_w(acc[3 + c], w, g1);
     }
-    acc_w(acc[c], w, g0);
-    acc_w(acc[3 + c], w, g1);
-    if (MU == 0) {  // [h0, h1, -S i h1, -S i h0]
-      if (S > 0) {
-        acc_wmi(acc[6 + c], w, nw, g1);
-        acc_wmi(acc[9 + c], w, nw, g0);
-      } else {
-        acc_wi(acc[6 + c], w, nw, g1);
-        acc_wi(acc[9 + c], w, nw, g0);
-      }
-    } else if (MU == 1) {  // [h0, h1, -S h1, S h0]
-      if (S > 0) {
-        acc_w(acc[6 + c], nw, g1);
-        acc_w(acc[9 + c], w, g0);
-      } else {
-        acc_w(acc[6 + c], w, g1);
-        acc_w(acc[9 + c], nw, g0);
-      }
-    } else {  // MU==2: [h0, h1, -S i h0, S i h1]
-      if (S > 0) {
-        acc_wmi(acc[6 + c], w, nw, g0);
-        acc_wi(acc[9 + c], w, nw, g1);
-      } else {
-        acc_wi(acc[6 + c], w, nw, g0);
-        acc_wmi(acc[9 + c], w, nw, g1);
-      }
+    return;
+  }
+  acc_w(acc[c], w, g0);
+  acc_w(acc[3 + c], w, g1);
+  if (MU == 0) {  // [h0, h1, -S i h1, -S i h0]
+    if (S > 0) {
+      acc_wmi(acc[6 + c], w, nw, g1);
+      acc_wmi(acc[9 + c], w, nw, g0);
+    } else {
+      acc_wi(acc[6 + c], w, nw, g1);
+      acc_wi(acc[9 + c], w, nw, g0);
+    }
+  } else if (MU == 1) {  // [h0, h1, -S h1, S h0]
+    if (S > 0) {
+      acc_w(acc[6 + c], nw, g1);
+      acc_w(acc[9 + c], w, g0);
+    } else {
+      acc_w(acc[6 + c], w, g1);
+      acc_w(acc[9 + c], nw, g0);
+    }
+  } else {  // MU==2: [h0, h1, -S i h0, S i h1]
+    if (S > 0) {
+      acc_wmi(acc[6 + c], w, nw, g0);
+      acc_wi(acc[9 + c], w, nw, g1);
+    } else {
+      acc_wi(acc[6 + c], w, nw, g0);
+      acc_wmi(acc[9 + c], w, nw, g1);
     }
   }
 }
 
-// g = U h (ADJ false) or U^dag h (ADJ true) for the two colour vectors of h;
-// the link elements are broadcast to both lanes
+template <int MU, int S>
+__device__ __forceinline__ void reconstruct_pair(Cp acc[12], const Cp g[6], float2 w) {
+  const float2 nw = pmul(w, bc(-1.f));
+#pragma unroll
+  for (int c = 0; c < 3; ++c) reconstruct_col<MU, S>(acc, c, g[c], g[3 + c], w, nw);
+}
+
+// row a of g = U h (ADJ false) or U^dag h (ADJ true), for the colour vector
+// h[0..2] of the pair; the link elements are broadcast to both lanes
+template <bool ADJ>
+__device__ __forceinline__ Cp su3_row(const Su3<float>& U, int a, const Cp h0, const Cp h1, const Cp h2) {
+  const Cx<float> u0 = ADJ ? U.e[0][a] : U.e[a][0];
+  const Cx<float> u1 = ADJ ? U.e[1][a] : U.e[a][1];
+  const Cx<float> u2 = ADJ ? U.e[2][a] : U.e[a][2];
+  float2 s1, s2, s3;
+  if (!ADJ) {
+    // re = sum ur h.re - sum ui h.im,  im = sum ur h.im + ui h.re
+    s1 = pmul(bc(u0.re), h0.re);
+    s1 = pfma(bc(u1.re), h1.re, s1);
+    s1 = pfma(bc(u2.re), h2.re, s1);
+    s2 = pmul(bc(u0.im), h0.im);
+    s2 = pfma(bc(u1.im), h1.im, s2);
+    s2 = pfma(bc(u2.im), h2.im, s2);
+    s3 = pmul(bc(u0.re), h0.im);
+    s3 = pfma(bc(u0.im), h0.re, s3);
+    s3 = pfma(bc(u1.re), h1.im, s3);
+    s3 = pfma(bc(u1.im), h1.re, s3);
+    s3 = pfma(bc(u2.re), h2.im, s3);
+    s3 = pfma(bc(u2.im), h2.re, s3);
+    return {psub(s1, s2), s3};
+  }
+  // conj(u): re = sum ur h.re + ui h.im,  im = sum ur h.im - sum ui h.re
+  s3 = pmul(bc(u0.re), h0.re);
+  s3 = pfma(bc(u0.im), h0.im, s3);
+  s3 = pfma(bc(u1.re), h1.re, s3);
+  s3 = pfma(bc(u1.im), h1.im, s3);
+  s3 = pfma(bc(u2.re), h2.re, s3);
+  s3 = pfma(bc(u2.im), h2.im, s3);
+  s1 = pmul(bc(u0.re), h0.im);
+  s1 = pfma(bc(u1.re), h1.im, s1);
+  s1 = pfma(bc(u2.re), h2.im, s1);
+  s2 = pmul(bc(u0.im), h0.re);
+  s2 = pfma(bc(u1.im), h1.re, s2);
+  s2 = pfma(bc(u2.im), h2.re, s2);
+  return {s3, psub(s1, s2)};
+}
+
 template <bool ADJ>
 __device__ __forceinline__ void su3_pair(const Su3<float>& U, const Cp h[6], Cp g[6]) {
 #pragma unroll
-  for (int v = 0; v < 2; ++v) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      float2 s1, s2, s3;  // re = s1 -/+ s2, im = s3 (one chain) -- see below
-      const Cx<float> u0 = ADJ ? U.e[0][a] : U.e[a][0];
-      const Cx<float> u1 = ADJ ? U.e[1][a] : U.e[a][1];
-      const Cx<float> u2 = ADJ ? U.e[2][a] : U.e[a][2];
-      const Cp h0 = h[3 * v], h1 = h[3 * v + 1], h2 = h[3 * v + 2];
-      if (!ADJ) {
-        // re = sum ur h.re - sum ui h.im,  im = sum ur h.im + ui h.re
-        s1 = pmul(bc(u0.re), h0.re);
-        s1 = pfma(bc(u1.re), h1.re, s1);
-        s1 = pfma(bc(u2.re), h2.re, s1);
-        s2 = pmul(bc(u0.im), h0.im);
-        s2 = pfma(bc(u1.im), h1.im, s2);
-        s2 = pfma(bc(u2.im), h2.im, s2);
-        s3 = pmul(bc(u0.re), h0.im);
-        s3 = pfma(bc(u0.im), h0.re, s3);
-        s3 = pfma(bc(u1.re), h1.im, s3);
-        s3 = pfma(bc(u1.im), h1.re, s3);
-        s3 = pfma(bc(u2.re), h2.im, s3);
-        s3 = pfma(bc(u2.im), h2.re, s3);
-        g[3 * v + a] = {psub(s1, s2), s3};
-      } else {
-        // conj(u): re = sum ur h.re + ui h.im,  im = sum ur h.im - sum ui h.re
-        s3 = pmul(bc(u0.re), h0.re);
-        s3 = pfma(bc(u0.im), h0.im, s3);
-        s3 = pfma(bc(u1.re), h1.re, s3);
-        s3 = pfma(bc(u1.im), h1.im, s3);
-        s3 = pfma(bc(u2.re), h2.re, s3);
-        s3 = pfma(bc(u2.im), h2.im, s3);
-        s1 = pmul(bc(u0.re), h0.im);
-        s1 = pfma(bc(u1.re), h1.im, s1);
-        s1 = pfma(bc(u2.re), h2.im, s1);
-        s2 = pmul(bc(u0.im), h0.re);
-        s2 = pfma(bc(u1.im), h1.re, s2);
-        s2 = pfma(bc(u2.im), h2.re, s2);
-        g[3 * v + a] = {s3, psub(s1, s2)};
-      }
-    }
+  for (int a = 0; a < 3; ++a) {
+    g[a] = su3_row<ADJ>(U, a, h[0], h[1], h[2]);
+    g[3 + a] = su3_row<ADJ>(U, a, h[3], h[4], h[5]);
   }
+}
+
+// ---- one half-direction from raw (undecoded) pair data -------------------------------
+// raw[2k + j] is 16-byte chunk k of right-hand side j: FP16 holds complexes
+// 4k..4k+3 of the element, FP32 complexes 2k, 2k+1 (complex i = 3*spin + colour).
+template <int SP>
+struct RawPair {
+  uint4 v[SP == PREC_HALF ? 6 : 12];
+};
+
+template <int SP>
+__device__ __forceinline__ Cp raw_get(const RawPair<SP>& r, int i) {
+  if constexpr (SP == PREC_HALF) {
+    const int k = i >> 2, m = i & 3;
+    const uint4 a = r.v[2 * k], b = r.v[2 * k + 1];
+    const uint32_t wa = m == 0 ? a.x : m == 1 ? a.y : m == 2 ? a.z : a.w;
+    const uint32_t wb = m == 0 ? b.x : m == 1 ? b.y : m == 2 ? b.z : b.w;
+    const float2 x = unpack_h2(wa), y = unpack_h2(wb);
+    return {make_float2(x.x, y.x), make_float2(x.y, y.y)};
+  } else {
+    const int k = i >> 1;
+    const uint4 a = r.v[2 * k], b = r.v[2 * k + 1];
+    if (i & 1)
+      return {make_float2(__uint_as_float(a.z), __uint_as_float(b.z)),
+              make_float2(__uint_as_float(a.w), __uint_as_float(b.w))};
+    return {make_float2(__uint_as_float(a.x), __uint_as_float(b.x)),
+            make_float2(__uint_as_float(a.y), __uint_as_float(b.y))};
+  }
+}
+
+// acc += w (1 - S gamma_mu) [U or U^dag] (1 - S gamma_mu)-projection of the
+// neighbour pair, decoding one colour at a time (short live ranges)
+template <int SP, int MU, int S, bool ADJ>
+__device__ __forceinline__ void half_dir_raw(const RawPair<SP>& raw, float2 w, const Su3<float>& U,
+                                             Cp acc[12]) {
+  Cp h[6];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    project_col<MU, S>(raw_get<SP>(raw, c), raw_get<SP>(raw, 3 + c), raw_get<SP>(raw, 6 + c),
+                       raw_get<SP>(raw, 9 + c), h[c], h[3 + c]);
+  if (MU == 3) w = pmul(w, bc(2.f));
+  const float2 nw = pmul(w, bc(-1.f));
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    reconstruct_col<MU, S>(acc, a, su3_row<ADJ>(U, a, h[0], h[1], h[2]),
+                           su3_row<ADJ>(U, a, h[3], h[4], h[5]), w, nw);
+}
+
+template <int SP>
+__device__ __forceinline__ void load_raw_pair(const SpinorPtr& s, int64_t i0, RawPair<SP>& r,
+                                              float2& w) {
+  constexpr int NC = SP == PREC_HALF ? 3 : 6;
+  const uint4* p = static_cast<const uint4*>(s.data) + blk0<NC>(i0);
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    r.v[2 * k] = __ldg(p + 32 * k);
+    r.v[2 * k + 1] = __ldg(p + 32 * k + 1);
+  }
+  if constexpr (SP == PREC_HALF)
+    w = __ldg(reinterpret_cast<const float2*>(s.norm + i0));
+  else
+    w = bc(1.f);
 }
 
 // Forward and backward contributions of direction MU for the pair at
@@ -279,28 +348,21 @@ template <int MU, bool DAG, int SP>
 __device__ __forceinline__ void hop_dir_pair(const GaugePtr& gauge, const SpinorPtr& in, int p,
                                              int hs, const int nb[8], int nrhs, int r0,
                                              Cp acc[12]) {
-  constexpr float kT = (MU == 3) ? 2.f : 1.f;  // the t projector's factor 2
   {
     Su3<float> U;
     GaugeIO<SP, 12>::load(gauge, p, MU, hs, U);
-    constexpr int S = DAG ? -1 : 1;
-    Cp f[12], h[6], g[6];
+    RawPair<SP> raw;
     float2 w;
-    PairIO<SP>::load(in, int64_t(nb[2 * MU]) * nrhs + r0, f, w);
-    project_pair<MU, S>(f, h);
-    su3_pair<false>(U, h, g);
-    reconstruct_pair<MU, S>(acc, g, kT == 1.f ? w : pmul(w, bc(kT)));
+    load_raw_pair<SP>(in, int64_t(nb[2 * MU]) * nrhs + r0, raw, w);
+    half_dir_raw<SP, MU, DAG ? -1 : 1, false>(raw, w, U, acc);
   }
   {
     Su3<float> U;
     GaugeIO<SP, 12>::load(gauge, 1 - p, MU, nb[2 * MU + 1], U);
-    constexpr int S = DAG ? 1 : -1;
-    Cp f[12], h[6], g[6];
+    RawPair<SP> raw;
     float2 w;
-    PairIO<SP>::load(in, int64_t(nb[2 * MU + 1]) * nrhs + r0, f, w);
-    project_pair<MU, S>(f, h);
-    su3_pair<true>(U, h, g);
-    reconstruct_pair<MU, S>(acc, g, kT == 1.f ? w : pmul(w, bc(kT)));
+    load_raw_pair<SP>(in, int64_t(nb[2 * MU + 1]) * nrhs + r0, raw, w);
+    half_dir_raw<SP, MU, DAG ? 1 : -1, true>(raw, w, U, acc);
   }
 }
 

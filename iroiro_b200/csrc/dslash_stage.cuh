@@ -13,7 +13,10 @@
 // stage index and neighbour lookup is known at compile time.
 //
 // Shared memory per thread and stage, in 16-byte slots laid out
-// [stage][slot][thread] (a warp's 32 slots are contiguous: no bank conflicts):
+// [thread][stage][slot], each thread's block padded by 16 bytes so that the
+// 8 threads of a quarter warp start on different bank groups (no conflicts
+// for 16-byte accesses); slot offsets within a thread are compile-time
+// constants:
 //   FP16: 6 spinor slots (3 chunks x 2 elements), the link's first 16 bytes,
 //         and (norm pair, link's last 8 bytes);
 //   FP32: 12 spinor slots (6 chunks x 2 elements) and 3 link slots.
@@ -54,9 +57,15 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// byte address of slot k of stage s of this thread
-__device__ __forceinline__ uint32_t slot_addr(uint32_t base, int s, int k, int nslots) {
-  return base + uint32_t(((s * nslots + k) * int(blockDim.x) + int(threadIdx.x)) * 16);
+// bytes of one thread's stages (padded by one slot)
+template <int SP>
+__host__ __device__ constexpr int stage_bytes() {
+  return (kStages * StageSlots<SP>::N + 1) * 16;
+}
+
+// byte address of slot k of stage s, from this thread's first slot
+__device__ __forceinline__ uint32_t slot_addr(uint32_t tbase, int s, int k, int nslots) {
+  return tbase + uint32_t((s * nslots + k) * 16);
 }
 
 // Issues the copies of half-direction HD (mu = HD/2, backward if HD odd) of
@@ -96,25 +105,24 @@ __device__ __forceinline__ void stage_issue(const GaugePtr& gauge, const SpinorP
   }
 }
 
-// Decodes stage S into the neighbour pair f (raw FP16 values and their norms
-// w, or FP32 values and w = 1) and the link U.
-template <int SP, int S>
-__device__ __forceinline__ void stage_read(const uint4* sm, Cp f[12], float2& w, Su3<float>& U) {
+// Computes half-direction HD from stage S into acc: raw pair chunks, the
+// FP16 norms, and the link read back from the thread's slots, then decoded
+// one colour at a time.
+template <int SP, int HD, int S, bool DAG>
+__device__ __forceinline__ void stage_compute(const uint4* sm, Cp acc[12]) {
+  constexpr int MU = HD >> 1;
+  constexpr bool BWD = HD & 1;
+  // forward hop: projector (1 - g_mu) [dagger (1 + g_mu)], U; backward: the opposite, U^dag
+  constexpr int SG = (BWD ? -1 : 1) * (DAG ? -1 : 1);
   constexpr int NS = StageSlots<SP>::N;
-  // plain shared-memory loads (ordered after the copies by cp_wait's clobber),
-  // so the compiler can place each one next to its use
-  auto lds = [&](int k) { return sm[(S * NS + k) * int(blockDim.x) + int(threadIdx.x)]; };
+  // plain shared-memory loads (ordered after the copies by cp_wait's clobber)
+  auto lds = [&](int k) { return sm[S * NS + k]; };
+  RawPair<SP> raw;
+  float2 w;
+  Su3<float> U;
   if constexpr (SP == PREC_HALF) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const uint4 a = lds(2 * k), b = lds(2 * k + 1);
-      const uint32_t av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const float2 x = unpack_h2(av[m]), y = unpack_h2(bv[m]);
-        f[4 * k + m] = {make_float2(x.x, y.x), make_float2(x.y, y.y)};
-      }
-    }
+    for (int k = 0; k < 6; ++k) raw.v[k] = lds(k);
     const uint4 la = lds(6), nl = lds(7);
     w = make_float2(__uint_as_float(nl.x), __uint_as_float(nl.y));
     float2 t;
@@ -126,13 +134,7 @@ __device__ __forceinline__ void stage_read(const uint4* sm, Cp f[12], float2& w,
     t = unpack_h2(nl.w); U.e[1][2] = {t.x, t.y};
   } else {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const uint4 a = lds(2 * k), b = lds(2 * k + 1);
-      f[2 * k] = {make_float2(__uint_as_float(a.x), __uint_as_float(b.x)),
-                  make_float2(__uint_as_float(a.y), __uint_as_float(b.y))};
-      f[2 * k + 1] = {make_float2(__uint_as_float(a.z), __uint_as_float(b.z)),
-                      make_float2(__uint_as_float(a.w), __uint_as_float(b.w))};
-    }
+    for (int k = 0; k < 12; ++k) raw.v[k] = lds(k);
     const uint4 a = lds(12), b = lds(13), c = lds(14);
     U.e[0][0] = {__uint_as_float(a.x), __uint_as_float(a.y)};
     U.e[0][1] = {__uint_as_float(a.z), __uint_as_float(a.w)};
@@ -143,22 +145,7 @@ __device__ __forceinline__ void stage_read(const uint4* sm, Cp f[12], float2& w,
     w = bc(1.f);
   }
   reconstruct_row2(U);
-}
-
-// Computes half-direction HD from stage S into acc.
-template <int SP, int HD, int S, bool DAG>
-__device__ __forceinline__ void stage_compute(const uint4* sm, Cp acc[12]) {
-  constexpr int MU = HD >> 1;
-  constexpr bool BWD = HD & 1;
-  // forward hop: projector (1 - g_mu) [dagger (1 + g_mu)], U; backward: the opposite, U^dag
-  constexpr int SG = (BWD ? -1 : 1) * (DAG ? -1 : 1);
-  Cp f[12], h[6], g[6];
-  float2 w;
-  Su3<float> U;
-  stage_read<SP, S>(sm, f, w, U);
-  project_pair<MU, SG>(f, h);
-  su3_pair<BWD>(U, h, g);
-  reconstruct_pair<MU, SG>(acc, g, MU == 3 ? pmul(w, bc(2.f)) : w);
+  half_dir_raw<SP, MU, SG, BWD>(raw, w, U, acc);
 }
 
 // One pipeline step: issue item HD+3 (of this site, or of the next site for
@@ -187,8 +174,9 @@ __device__ __forceinline__ void stage_step(const HopParams& P, int yi, int p, in
 template <int SP, bool DAG, int EPI, int VAR>
 __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_stage_kernel(HopParams P) {
   extern __shared__ __align__(16) unsigned char stage_smem[];
-  const uint32_t base = smem_u32_generic(stage_smem);
-  const uint4* sm = reinterpret_cast<const uint4*>(stage_smem);
+  // this thread's slots
+  const uint32_t base = smem_u32_generic(stage_smem) + threadIdx.x * stage_bytes<SP>();
+  const uint4* sm = reinterpret_cast<const uint4*>(stage_smem + threadIdx.x * stage_bytes<SP>());
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;
   const int nrhs = P.nrhs;

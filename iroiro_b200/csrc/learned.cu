@@ -33,6 +33,7 @@
 #include <cstring>
 #include <vector>
 
+#include "dslash_pair.cuh"
 #include "internal.h"
 #include "iroiro_b200.h"
 
@@ -136,7 +137,31 @@ struct Ptc {
   static constexpr int TCOLS = NP <= 32 ? 32 : 64;
   static constexpr int A_BYTES = 128 * KP * 2;
   static constexpr int B_BYTES = NP * KP * 2;
+  // forward kernel: A holds the 96 rows of 32 sites; the MMA's rows 96..127
+  // read the bytes that follow (the weights, padded to at least 32 rows),
+  // which only feed accumulator rows that are never read back
+  static constexpr int A96_BYTES = 96 * KP * 2;
+  static constexpr int BF_BYTES = NP >= 32 ? B_BYTES : 32 * KP * 2;
 };
+
+// Feature element (site s, channel o, colour a) of a V-site field.  Channels
+// are stored in pairs, structure-of-arrays over sites in 16-byte units: pair
+// q = o/2 and colour a occupy the float4 row (3q + a)*V + s holding
+// (re o=2q, re o=2q+1, im o=2q, im o=2q+1).  A warp reading one row for 32
+// consecutive (or uniformly shifted) sites is coalesced, and a row is
+// directly the packed FP32x2 operand pair of the two channels.
+__host__ __device__ __forceinline__ size_t fidx(int s, int o, int a, int V) {
+  return (size_t((o >> 1) * 3 + a) * V + s) * 4 + (o & 1);
+}
+__device__ __forceinline__ float2 feat_get(const float2* f, int s, int o, int a, int V) {
+  const float* p = reinterpret_cast<const float*>(f) + fidx(s, o, a, V);
+  return make_float2(p[0], p[2]);
+}
+__device__ __forceinline__ void feat_set(float2* f, int s, int o, int a, int V, float2 v) {
+  float* p = reinterpret_cast<float*>(f) + fidx(s, o, a, V);
+  p[0] = v.x;
+  p[2] = v.y;
+}
 
 struct PtcGeo {
   Geom g;
@@ -177,13 +202,12 @@ __device__ void build_a_tile(const PtcGeo& G, const float2* __restrict__ in, int
       else
         GaugeIO<PREC_SINGLE, 12>::load(G.gauge, 1 - p, mu, n, U);
     }
-    const float2* f = in + size_t(src) * CIN * 3;
 #pragma unroll 4
     for (int i = 0; i < CIN; ++i) {
       Cx<float> v[3], w[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        const float2 t = f[i * 3 + a];
+        const float2 t = feat_get(in, src, i, a, G.V);
         v[a] = {t.x, t.y};
       }
       if (d == 0) {
@@ -218,66 +242,194 @@ __device__ void load_b(const __nv_bfloat16* __restrict__ B, unsigned char* Bs) {
 }
 
 // Issues the K/16 MMAs of D = A B^T into TMEM, commits to the mbarrier and
-// waits (bounded).  Returns false on time-out.
+// waits (bounded).  Only warp 0 polls the barrier (the other warps wait at
+// the block barrier without taking issue slots); the block barrier then
+// orders everyone's tcgen05 accesses after the completed MMAs.  Returns false
+// on time-out, in every thread.
 template <int K>
 __device__ bool mma_and_wait(const unsigned char* A, const unsigned char* B, uint32_t tmem,
                              uint32_t idesc, uint64_t* bar, uint32_t phase, int* err) {
+  __shared__ int mma_ok;
   fence_async_smem();
   __syncthreads();
   tc_fence_after();
-  if (threadIdx.x == 0) {
-    const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
-    constexpr uint32_t sbo = (K / 8) * 128;
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) {
+      const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+      constexpr uint32_t sbo = (K / 8) * 128;
 #pragma unroll 1
-    for (int kb = 0; kb < K / 16; ++kb)
-      umma_bf16(tmem, smem_desc(a0 + kb * 256, 128, sbo), smem_desc(b0 + kb * 256, 128, sbo), idesc,
-                kb > 0 ? 1u : 0u);
-    umma_commit(bar);
-  }
-  bool ok = false;
-  for (int it = 0; it < kWaitLimit; ++it)
-    if (mbar_try_wait(bar, phase)) {
-      ok = true;
-      break;
+      for (int kb = 0; kb < K / 16; ++kb)
+        umma_bf16(tmem, smem_desc(a0 + kb * 256, 128, sbo), smem_desc(b0 + kb * 256, 128, sbo),
+                  idesc, kb > 0 ? 1u : 0u);
+      umma_commit(bar);
     }
-  if (!ok && err) atomicExch(err, 1);
+    __syncwarp();
+    bool ok = false;
+    for (int it = 0; it < kWaitLimit; ++it)
+      if (mbar_try_wait(bar, phase)) {
+        ok = true;
+        break;
+      }
+    if (threadIdx.x == 0) {
+      mma_ok = ok ? 1 : 0;
+      if (!ok && err) atomicExch(err, 1);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
   tc_fence_after();
-  return ok;
+  return mma_ok != 0;
 }
 
 // ---- forward ----------------------------------------------------------------------
+// Writes the A-tile entries of one (site, displacement) job: the CIN
+// transported channel vectors of the tile's site sl, as BF16 in columns
+// (2d + re/im)*CIN + i of rows 3*sl + colour.  Channels are handled in pairs
+// in the packed FP32x2 arithmetic (su3_row); each colour row receives CIN/8
+// 16-byte stores (8-byte stores for CIN = 4).
+template <int CIN, int KP>
+__device__ __forceinline__ void a_tile_job(const PtcGeo& G, const float2* __restrict__ in, int s,
+                                           int sl, int d, unsigned char* A) {
+  constexpr int NW = CIN / 2;  // BF16x2 words per colour and part
+  uint32_t wre[3][NW], wim[3][NW];
+  if (s < G.V) {
+    const int Vh = G.g.Vh;
+    const int p = s >= Vh ? 1 : 0;
+    const int hs = s - p * Vh;
+    int src = s;
+    Su3<float> U;
+    bool fwd = true;
+    if (d > 0) {
+      const Coord c = coord_of(G.g, hs, p);
+      int nb[8];
+      neighbours(G.g, c, hs, nb);
+      const int mu = (d - 1) >> 1;
+      fwd = ((d - 1) & 1) == 0;
+      const int n = nb[d - 1];
+      src = (1 - p) * Vh + n;
+      if (fwd)
+        GaugeIO<PREC_SINGLE, 12>::load(G.gauge, p, mu, hs, U);
+      else
+        GaugeIO<PREC_SINGLE, 12>::load(G.gauge, 1 - p, mu, n, U);
+    }
+    // channels 2q, 2q+1 of the source site, one float4 row per colour (see fidx)
+    const float4* f4 = reinterpret_cast<const float4*>(in) + src;
+    const size_t V = size_t(G.V);
+#pragma unroll
+    for (int q = 0; q < NW; ++q) {
+      const float4 a = __ldg(f4 + (3 * q) * V), b = __ldg(f4 + (3 * q + 1) * V),
+                   e = __ldg(f4 + (3 * q + 2) * V);
+      const Cp h0 = {make_float2(a.x, a.y), make_float2(a.z, a.w)};
+      const Cp h1 = {make_float2(b.x, b.y), make_float2(b.z, b.w)};
+      const Cp h2 = {make_float2(e.x, e.y), make_float2(e.z, e.w)};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        Cp w;
+        if (d == 0)
+          w = r == 0 ? h0 : (r == 1 ? h1 : h2);
+        else if (fwd)
+          w = su3_row<false>(U, r, h0, h1, h2);
+        else
+          w = su3_row<true>(U, r, h0, h1, h2);
+        const __nv_bfloat162 br = __floats2bfloat162_rn(w.re.x, w.re.y);
+        const __nv_bfloat162 bi = __floats2bfloat162_rn(w.im.x, w.im.y);
+        wre[r][q] = *reinterpret_cast<const uint32_t*>(&br);
+        wim[r][q] = *reinterpret_cast<const uint32_t*>(&bi);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int q = 0; q < NW; ++q) wre[r][q] = wim[r][q] = 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int row = 3 * sl + r;
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      const uint32_t* w = part ? wim[r] : wre[r];
+      const int k0 = (2 * d + part) * CIN;
+      if constexpr (CIN == 4) {
+        *reinterpret_cast<uint2*>(A + canon(row, k0, KP)) = make_uint2(w[0], w[1]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < NW; q += 4)
+          *reinterpret_cast<uint4*>(A + canon(row, k0 + 2 * q, KP)) =
+              make_uint4(w[q], w[q + 1], w[q + 2], w[q + 3]);
+      }
+    }
+  }
+}
+
+// Persistent forward kernel: each CTA allocates its tensor memory, loads the
+// weights and zeroes its A tile once, then loops over tiles of 32 sites
+// (96 of the 128 MMA rows).  The 9 warps build the A tile, warp d handling
+// displacement d for the 32 sites (lane = site): branches on the displacement
+// are warp-uniform, a warp's gathers are the neighbours of 32 consecutive
+// sites, and its 16-byte stores into the canonical layout hit 8 different
+// bank groups per 128 bytes.  One thread issues the MMAs; warps 0-2 read the
+// accumulator back.  The mbarrier phase alternates per tile; every wait is
+// bounded and a time-out stops the CTA with the error flag set.
+constexpr int kFwdSites = 32;
+constexpr int kFwdThreads = 288;
+
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kThreads) ptc_fwd_kernel(PtcGeo G, const float2* __restrict__ in,
-                                                           float2* __restrict__ out,
-                                                           const __nv_bfloat16* __restrict__ bop) {
+__global__ void __launch_bounds__(kFwdThreads) ptc_fwd_kernel(PtcGeo G, const float2* __restrict__ in,
+                                                              float2* __restrict__ out,
+                                                              const __nv_bfloat16* __restrict__ bop,
+                                                              int ntiles) {
   using S = Ptc<CIN, COUT>;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* A = smem;
-  unsigned char* B = smem + S::A_BYTES;
+  unsigned char* B = smem + S::A96_BYTES;
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tslot;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == 0) tmem_alloc(&tslot, S::TCOLS);
   if (threadIdx.x == 0) mbar_init(&bar, 1);
-  load_b<S::NP, S::KP>(bop, B);
-  const int site0 = blockIdx.x * kTileSites;
-  build_a_tile<CIN, S::KP>(G, in, site0, A);
+  // zero the weights' padding rows (read only as A rows 96..127), then the
+  // weights: NP x KP row-major BF16, copied in 16-byte pieces into the canonical layout
+  for (int b = S::B_BYTES + threadIdx.x * 16; b < S::BF_BYTES; b += kFwdThreads * 16)
+    *reinterpret_cast<uint4*>(B + b) = make_uint4(0, 0, 0, 0);
+  for (int idx = threadIdx.x; idx < S::NP * (S::KP / 8); idx += kFwdThreads) {
+    const int n = idx / (S::KP / 8), k0 = (idx - n * (S::KP / 8)) * 8;
+    *reinterpret_cast<uint4*>(B + canon(n, k0, S::KP)) =
+        __ldg(reinterpret_cast<const uint4*>(bop + size_t(n) * S::KP + k0));
+  }
+  // columns KF..KP are never written by a job
+  for (int b = threadIdx.x * 16; b < S::A96_BYTES; b += kFwdThreads * 16)
+    *reinterpret_cast<uint4*>(A + b) = make_uint4(0, 0, 0, 0);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tslot;
-  const bool ok = mma_and_wait<S::KP>(A, B, tmem, idesc_bf16(S::NP), &bar, 0, G.err);
-  if (ok) {
-    const int r = warp * 32 + lane;
-    float v[S::NP];
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int site0 = tile * kFwdSites;
+    a_tile_job<CIN, S::KP>(G, in, site0 + lane, lane, warp, A);
+    const bool ok = mma_and_wait<S::KP>(A, B, tmem, idesc_bf16(S::NP), &bar, phase, G.err);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) break;  // all threads leave together on a time-out
+    if (warp < 3) {
+      const int r = warp * 32 + lane;
+      float v[S::NP];
 #pragma unroll
-    for (int c = 0; c < S::NP; c += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c, v + c);
-    const int sl = r / 3, a = r - sl * 3;
-    const int s = site0 + sl;
-    if (sl < kTileSites && s < G.V) {
+      for (int c = 0; c < S::NP; c += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c, v + c);
+      const int sl = r / 3, a = r - sl * 3;
+      const int s = site0 + sl;
+      if (s < G.V) {
+        // channel pair (2q, 2q+1) of colour a: one 16-byte store
+        float4* o4 = reinterpret_cast<float4*>(out) + size_t(a) * G.V + s;
 #pragma unroll
-      for (int o = 0; o < COUT; ++o) out[(size_t(s) * COUT + o) * 3 + a] = make_float2(v[2 * o], v[2 * o + 1]);
+        for (int q = 0; q < COUT / 2; ++q)
+          o4[size_t(3 * q) * G.V] = make_float4(v[4 * q], v[4 * q + 2], v[4 * q + 1], v[4 * q + 3]);
+      }
     }
+    // the accumulator is read and the MMA has consumed A before the next tile
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
   }
   tc_fence_before();
   __syncthreads();
@@ -310,7 +462,7 @@ __global__ void __launch_bounds__(kThreads) ptc_da_kernel(PtcGeo G, const float2
     const int sl = r / 3, a = r - sl * 3, s = site0 + sl;
     float val = 0.f;
     if (sl < kTileSites && s < G.V && n < S::NF) {
-      const float2 t = dy[(size_t(s) * COUT + (n >> 1)) * 3 + a];
+      const float2 t = feat_get(dy, s, n >> 1, a, G.V);
       val = (n & 1) ? t.y : t.x;
     }
     *reinterpret_cast<__nv_bfloat16*>(A + canon(r, n, S::NP)) = __float2bfloat16_rn(val);
@@ -379,7 +531,7 @@ __global__ void ptc_gather_kernel(PtcGeo G, const float* __restrict__ da, float2
         for (int a = 0; a < 3; ++a) acc[a] = acc[a] + U.e[a][0] * g[0] + U.e[a][1] * g[1] + U.e[a][2] * g[2];
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) din[(size_t(s) * CIN + i) * 3 + a] = make_float2(acc[a].re, acc[a].im);
+      for (int a = 0; a < 3; ++a) feat_set(din, s, i, a, G.V, make_float2(acc[a].re, acc[a].im));
     }
   }
 }
@@ -400,7 +552,7 @@ __global__ void __launch_bounds__(kThreads) ptc_db_kernel(PtcGeo G, const float2
     const int sl = r / 3, a = r - sl * 3, s = site0 + sl;
     float val = 0.f;
     if (sl < kTileSites && s < G.V) {
-      const float2 t = dy[(size_t(s) * COUT + (n >> 1)) * 3 + a];
+      const float2 t = feat_get(dy, s, n >> 1, a, G.V);
       val = (n & 1) ? t.y : t.x;
     }
     Y[idx] = val;
@@ -432,7 +584,7 @@ __global__ void spinor_to_feat_kernel(int Vh, SpinorPtr e, SpinorPtr o, float2* 
     Cx<float> v[12];
     SpinorIO<PREC_SINGLE>::load(p ? o : e, s - p * Vh, v);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) feat[size_t(s) * 12 + k] = make_float2(v[k].re, v[k].im);
+    for (int k = 0; k < 12; ++k) feat_set(feat, s, k / 3, k % 3, 2 * Vh, make_float2(v[k].re, v[k].im));
   }
 }
 __global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o) {
@@ -441,7 +593,7 @@ __global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, S
     Cx<float> v[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      const float2 t = feat[size_t(s) * 12 + k];
+      const float2 t = feat_get(feat, s, k / 3, k % 3, 2 * Vh);
       v[k] = {t.x, t.y};
     }
     SpinorIO<PREC_SINGLE>::store(p ? o : e, s - p * Vh, v);
@@ -449,11 +601,22 @@ __global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, S
 }
 
 // ---- host launchers ------------------------------------------------------------------
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n < 1) n = 1;
+  }
+  return n;
+}
+
 template <int CIN, int COUT>
 static cudaError_t fwd_t(const PtcGeo& G, const float2* in, float2* out, const __nv_bfloat16* bop,
                          cudaStream_t st) {
   using S = Ptc<CIN, COUT>;
-  const int smem = S::A_BYTES + S::B_BYTES;
+  const int smem = S::A96_BYTES + S::BF_BYTES;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(ptc_fwd_kernel<CIN, COUT>,
@@ -461,8 +624,16 @@ static cudaError_t fwd_t(const PtcGeo& G, const float2* in, float2* out, const _
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int grid = (G.V + kTileSites - 1) / kTileSites;
-  ptc_fwd_kernel<CIN, COUT><<<grid, kThreads, smem, st>>>(G, in, out, bop);
+  const int ntiles = (G.V + kFwdSites - 1) / kFwdSites;
+  // persistent: as many CTAs as fit on the device (threads, and shared memory
+  // up to ~150 KB per SM so that the rest of the SM's 256 KB stays L1 cache
+  // for the neighbour gathers), at most one per tile
+  int per_sm = (150 * 1024) / (smem + 1024);
+  if (per_sm > 2048 / kFwdThreads) per_sm = 2048 / kFwdThreads;
+  if (per_sm < 1) per_sm = 1;
+  int grid = sm_count() * per_sm;
+  if (grid > ntiles) grid = ntiles;
+  ptc_fwd_kernel<CIN, COUT><<<grid, kFwdThreads, smem, st>>>(G, in, out, bop, ntiles);
   return cudaGetLastError();
 }
 
@@ -731,6 +902,7 @@ using namespace iro::host;
 
 struct iro_ptc {
   iro_ctx* ctx = nullptr;
+  int dev = 0;  // device of the buffers (iro_ptc_destroy does not touch the context)
   int nl = 0;
   std::vector<int> w;                 // widths, nl+1 entries
   std::vector<std::vector<float>> W;  // host weights, complex [9][cout][cin] (re,im)
@@ -855,6 +1027,7 @@ int iro_ptc_create(iro_ctx* c, int nlayers, const int* widths, iro_ptc** out) {
   LCK(cudaSetDevice(device(c)));
   std::unique_ptr<iro_ptc> n(new iro_ptc());
   n->ctx = c;
+  n->dev = device(c);
   n->nl = nlayers;
   n->w.assign(widths, widths + nlayers + 1);
   const size_t V = size_t(volume(c));
@@ -893,8 +1066,8 @@ int iro_ptc_create(iro_ctx* c, int nlayers, const int* widths, iro_ptc** out) {
 
 int iro_ptc_destroy(iro_ptc* n) {
   if (!n) return IRO_BAD_ARG;
-  cudaSetDevice(device(n->ctx));
-  cudaStreamSynchronize(stream(n->ctx));
+  // cudaFree waits for the device's work on these buffers; the context may be gone
+  cudaSetDevice(n->dev);
   for (void* p : n->bop) cudaFree(p);
   for (void* p : n->bopT) cudaFree(p);
   for (float* p : n->db) cudaFree(p);

@@ -95,6 +95,7 @@ class PTCNet:
         ctx.check(self.L.iro_ptc_create(ctx.h, len(self.widths) - 1, arr, ctypes.byref(h)),
                   "iro_ptc_create")
         self.h = h
+        ctx._owned.add(self)
         self.set_weights(weights if weights is not None else init_weights(self.widths, seed))
 
     def set_weights(self, Ws):
