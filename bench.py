@@ -303,6 +303,123 @@ def batched_solves(torch, device):
     return out
 
 
+def learned_solves(torch, device, nfields=24, epochs=15, widths=(4, 8, 8, 4), nkrylov=16):
+    """Learned preconditioner: a PTC network trained by the library's own
+    forward/backward kernels on pairs (b = D^dag D v, v) from `nfields` seeded
+    16^3x32 gauge fields (eps=0.2, kappa=0.12), then applied inside flexible
+    GCR at 32^3x64 (unseen field, one Gaussian source) against GCR without it
+    and against CG on the same full-lattice D^dag D: FP64 and mixed precision.
+    Every solve stops on the FP64 true residual 1e-10."""
+    import iroiro_b200 as ib
+    from iroiro_b200 import learned
+    t0 = time.perf_counter()
+    pairs = learned.make_pairs([16, 16, 16, 32], nfields, seed0=SEED + 300, device=device)
+    net0 = learned.PTCNet(pairs[0].ctx, widths)
+    hist = learned.train(net0, pairs, epochs=epochs, lr=3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    W = net0.W
+    for pr in pairs:
+        pr.ctx.close()
+    Lb = [32, 32, 32, 64]
+    Vb = int(np.prod(Lb))
+    ctx = ib.Context(Lb, device)
+    s = torch.cuda.current_stream()
+    ctx.set_stream(s.cuda_stream)
+    u = ib.synth_gauge(Lb, EPS, SEED + 301)
+    ctx.upload_gauge(u, force=True)
+    D = ib.Dirac_Wilson(MASS, u, ctx=ctx)
+    b = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(Vb, SEED + 302))
+    net = learned.PTCNet(ctx, widths, W)
+    out = {"op": "full-lattice Wilson D^dag D 32^3x64, kappa=0.12, one Gaussian source",
+           "network": {"widths": list(widths), "train_fields": nfields, "train_lattice": "16^3x32",
+                       "epochs": epochs, "train_s": round(train_s, 1),
+                       "loss_first": round(hist[0], 4), "loss_last": round(hist[-1], 4)}}
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) * 1e3, r
+
+    for name, n in (("gcr_network", net), ("gcr_plain", None)):
+        x = ib.DeviceField(ctx, 2, "double")
+        slv = learned.Solver_GCR(D, n, nkrylov=nkrylov)
+        ms, (o, rc) = timed(lambda: slv.solve_field(b, x))
+        out[name] = {"ms": round(ms, 1), "iterations": o.iterations, "true_residual": o.diff,
+                     "cg_fallback": bool(o.fallback), "converged": rc == ib.OK}
+        x.close()
+    for inner in ("double", "single", "half"):
+        x = ib.DeviceField(ctx, 2, "double")
+        slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner)
+        ms, (outs, rc) = timed(lambda: slv.solve_field(b, x))
+        out["cg_" + inner] = {"ms": round(ms, 1), "iterations": outs[0].Iterations,
+                              "true_residual": outs[0].diff, "converged": rc == ib.OK}
+        x.close()
+    a = ib.DeviceField(ctx, 2, "single").upload(ib.synth_gaussian(Vb, SEED + 303))
+    c2 = ib.DeviceField(ctx, 2, "single")
+    apply_ms, _ = timed(lambda: ctx.check(net.L.iro_ptc_apply_field(ctx.h, net.h, a.h, c2.h), "apply"))
+    out["network_apply_ms"] = round(apply_ms, 3)
+    best_cg = min(out["cg_single"]["ms"], out["cg_half"]["ms"])
+    out["gcr_network_vs_best_mixed_cg"] = round(best_cg / out["gcr_network"]["ms"], 2)
+    out["iteration_ratio_vs_gcr_plain"] = round(out["gcr_plain"]["iterations"] /
+                                                max(1, out["gcr_network"]["iterations"]), 2)
+    ctx.close()
+    return out
+
+
+def mixed48(torch, device):
+    """Mixed-precision configuration: 48^3x96 even-odd Wilson-clover
+    (csw=1.0, kappa=0.124, eps=0.25 field), 12 Gaussian right-hand sides
+    solved together with FP16 storage (per-site norms, reconstruct-12 links),
+    FP32 arithmetic and FP64 reliable updates, against the FP64 block CG on
+    the same sources; every result's error against the FP64 solution."""
+    import iroiro_b200 as ib
+    Lb = [48, 48, 48, 96]
+    Vb = int(np.prod(Lb))
+    kappa = 0.124
+    mass = 0.5 / kappa - 4.0
+    ctx = ib.Context(Lb, device)
+    s = torch.cuda.current_stream()
+    ctx.set_stream(s.cuda_stream)
+    u = ib.synth_gauge(Lb, 0.25, SEED + 400)
+    ctx.upload_gauge(u, force=True)
+    D = ib.Dirac_Clover_EvenOdd(mass, CSW, u, ctx=ctx)
+    src = np.concatenate([ib.synth_gaussian(Vb // 2, SEED + 401 + r) for r in range(12)])
+    B = ib.DeviceField(ctx, 0, "double", 12).upload(src)
+    del src
+    out = {"op": "e/o Wilson-clover Schur 48^3x96, kappa=0.124, csw=1.0, eps=0.25, 12 Gaussian sources"}
+    X64 = ib.DeviceField(ctx, 0, "double", 12)
+    res = {}
+    # (FP32 storage is left out here: its 12-RHS workspaces would not fit
+    # beside the FP64 and FP16 ones and the clover terms in 180 GB)
+    for inner, X in (("double", X64), ("half", None)):
+        X = X or ib.DeviceField(ctx, 0, "double", 12)
+        slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner, delta=0.1)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        outs, rc = slv.solve_field(B, X)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t) * 1e3
+        res[inner] = {"ms": round(ms, 1), "iterations": max(o.Iterations for o in outs),
+                      "true_residual_max": max(o.diff for o in outs),
+                      "reliable_updates": max(o.reliable_updates for o in outs),
+                      "converged": rc == ib.OK}
+        if inner != "double":
+            x = X.download().reshape(12, -1)
+            x64 = X64.download().reshape(12, -1)
+            res[inner]["error_vs_fp64_per_rhs"] = [
+                float(np.linalg.norm(x[r] - x64[r]) / np.linalg.norm(x64[r])) for r in range(12)]
+            res[inner]["speedup_vs_fp64_block_cg"] = round(res["double"]["ms"] / ms, 2)
+            X.close()
+    out.update(res)
+    out["note"] = "single timed solve each (first call includes autotuning and workspace allocation)"
+    ctx.close()
+    return out
+
+
 def cpu_baseline_leg():
     """The reference's own e/o mult on the host cores, a bounded sample."""
     import oracle
@@ -445,6 +562,12 @@ def run_ours(args, world, rank, local):
     batched = {}
     if not args.no_solve and not args.no_batched:
         batched = batched_solves(torch, local)
+    learned_res = {}
+    if not args.no_solve and not args.no_learned:
+        learned_res = learned_solves(torch, local)
+    mixed = {}
+    if args.mixed48:
+        mixed = mixed48(torch, local)
 
     lib.iro_field_destroy(fin)
     lib.iro_field_destroy(fout)
@@ -477,6 +600,8 @@ def run_ours(args, world, rank, local):
         "variants": variants,
         "solve": solve,
         "batched": batched,
+        "learned": learned_res,
+        "mixed48": mixed,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
@@ -525,6 +650,9 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--mixed48", action="store_true",
+                    help="also run the 48^3x96 mixed-precision 12-RHS configuration (~1 min)")
     ap.add_argument("--kernel", default=None, help="profiling driver: OP,PREC,NRHS")
     ap.add_argument("--lattice", default="24,24,24,48")
     args = ap.parse_args()
