@@ -137,7 +137,9 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend: str = None):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo when asked (the
+    CPU tests of the replica path)."""
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local = _env_int("LOCAL_RANK", 0)
@@ -145,20 +147,33 @@ def dist_setup():
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        backend = backend or "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return world, rank, local
 
 
 def reduce_max(v: float, world: int) -> float:
+    """Max over ranks (device times are reported as the slowest replica)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(step_bytes: float, steps: int, t_ms: float, world: int) -> float:
+    """Whole-job GB/s of N independent replicas: every rank moves step_bytes
+    per step, the job takes as long as its slowest rank."""
+    t_max = reduce_max(t_ms, world)
+    return world * step_bytes * steps / (t_max * 1e-3) / 1e9
 
 
 def barrier(world: int):
@@ -494,9 +509,9 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ck = clocks.stop()
     t_ms = sum(s.elapsed_time(e) for s, e in ev)
-    t_max = reduce_max(t_ms, world)
     step_bytes = (2 * BYTES_HOP + BYTES_XPAY) * Vh
-    value = world * step_bytes * args.steps / (t_max * 1e-3) / 1e9
+    t_max = reduce_max(t_ms, world)
+    value = replica_value(step_bytes, args.steps, t_ms, world)
     achieved = step_bytes / ((t_ms / args.steps) * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
 
