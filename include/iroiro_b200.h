@@ -219,6 +219,29 @@ int iro_multishift_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const
                             int nshift, const double* shifts, double* x, double precision,
                             int max_iter, iro_solver_out* out, int* nconv);
 
+/* RationalSolver_CG::solve (lib/Solver/rationalSolver_CG.cpp:12-39):
+   sol = c0 b + sum_i residues[i] (D^dagger D + poles[i])^-1 b, the shifted
+   systems solved by iro_multishift_cg_solve's algorithm (poles ascending, at
+   most 16) and the sum formed on the device.  The reference obtains poles,
+   residues and c0 from a GMP Remez approximation (RationalApprox); here they
+   are inputs.  out / nconv as for the multishift solve. */
+int iro_rational_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const double* b,
+                          int npole, const double* poles, const double* residues, double c0,
+                          double* sol, double precision, int max_iter, iro_solver_out* out,
+                          int* nconv);
+
+/* Inverter_WilsonLike::invert (lib/Dirac_ops/eoUtils.cpp:43-81): solves the
+   FULL-lattice system D sol = src through the even/odd Schur operator `op`
+   (IRO_OP_WILSON_SCHUR_EE: D the full Wilson operator; IRO_OP_CLOVER_SCHUR_EE:
+   the full clover operator): be = b_e - D_eo A_oo^-1 b_o, CG on
+   M^dagger M y_e = M^dagger be with prm, x_o = A_oo^-1 (b_o - D_oe y_e).
+   src and sol are nrhs consecutive full-lattice Format_F arrays (24*V
+   doubles each).  out[r] is the CG's output for right-hand side r.
+   Qprop_EvenOdd::calc (lib/Measurements/FermionicM/qprop_EvenOdd.cpp:10-21)
+   is this call with the 12 spin-colour point sources as one block. */
+int iro_eo_invert(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
+                  const double* src, double* sol, int nrhs, iro_solver_out* out);
+
 /* ---- learned preconditioner and flexible GCR --------------------------------
    No counterpart in the reference (its solvers are CG, BiCGStab and
    multishift CG, lib/Solver/solver_Factory.cpp:10-45).  A gauge-equivariant

@@ -113,6 +113,10 @@ def _declare(L):
                                    ctypes.POINTER(SolverOut)]),
         "iro_multishift_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, I,
                                         ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
+        "iro_rational_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, _D, D, I,
+                                      ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
+        "iro_eo_invert": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
+                              ctypes.POINTER(SolverOut)]),
         "iro_synth_gauge": (I, [L4, D, ctypes.c_uint64, I, _D]),
         "iro_synth_gaussian": (I, [ctypes.c_int64, ctypes.c_uint64, _D]),
         "iro_synth_point_sources": (I, [ctypes.c_int64, ctypes.c_int64, _D]),
@@ -609,3 +613,182 @@ class MultiShiftSolver_CG:
                            o.operator_applies)
         out.Nconv = nconv.value
         return out
+
+
+# ---- rational functions of D^dag D ---------------------------------------------------
+
+class RationalApprox:
+    """The numbers RationalSolver_CG takes from RationalApprox
+    (lib/Tools/RationalApprox/rationalapprox.hpp:85-91):
+    f(x) = Const + sum_i Residuals[i] / (x + Poles[i]) and its inverse.  The
+    reference computes them with a GMP Remez algorithm; here they are given."""
+
+    def __init__(self, const, residues, poles, inv_const=0.0, inv_residues=(), inv_poles=()):
+        self._c, self._r, self._p = float(const), [float(v) for v in residues], [float(v) for v in poles]
+        self._ic, self._ir = float(inv_const), [float(v) for v in inv_residues]
+        self._ip = [float(v) for v in inv_poles]
+        if len(self._r) != len(self._p) or len(self._ir) != len(self._ip):
+            raise IroError(BAD_ARG, "residues and poles differ in number")
+
+    def Residuals(self): return list(self._r)
+    def Poles(self): return list(self._p)
+    def Const(self): return self._c
+    def InvResiduals(self): return list(self._ir)
+    def InvPoles(self): return list(self._ip)
+    def InvConst(self): return self._ic
+
+
+class RationalSolver_CG:
+    """RationalSolver_CG(MultiShiftSolver_CG, RationalApprox)
+    (lib/Solver/rationalSolver_CG.hpp:35-44).  solve(sol, b):
+    sol = Const b + sum_i Residuals[i] (D^dag D + Poles[i])^-1 b, reconstructed
+    on the device; solve_inv uses the inverse approximation;
+    solve_noReconstruct(_inv) return the shifted solutions."""
+
+    def __init__(self, ms: "MultiShiftSolver_CG", ra: RationalApprox = None):
+        self.ms = ms
+        self.ra = ra
+
+    def set_Approx(self, ra: RationalApprox):
+        self.ra = ra
+
+    def _solve(self, sol, b, c0, res, poles, what):
+        if self.ra is None or not res:
+            raise IroError(BAD_ARG, f"[RationalSolver] {what} rational approximation not initialized yet")
+        D = self.ms.fopr.D
+        D.ctx.upload_gauge(D.u)
+        n = D.fsize()
+        b = _f64(b, n, "source")
+        p, r = _f64(poles), _f64(res)
+        out = np.empty(n)
+        o = SolverOut()
+        nconv = ctypes.c_int(-1)
+        rc = D.ctx._lib.iro_rational_cg_solve(D.ctx.h, D.op, D.mass, D.csw, _ptr(b), p.size, _ptr(p),
+                                              _ptr(r), c0, _ptr(out), self.ms.prec, self.ms.niter,
+                                              ctypes.byref(o), ctypes.byref(nconv))
+        D.ctx.check(rc, "iro_rational_cg_solve")
+        sol[...] = out
+        res_out = SolverOutput(o.diff, o.iterations, o.timing_ms, "Multishift CG solver", 0,
+                               o.operator_applies)
+        res_out.Nconv = nconv.value
+        return res_out
+
+    def solve(self, sol: np.ndarray, b: np.ndarray) -> SolverOutput:
+        ra = self.ra
+        return self._solve(sol, b, ra.Const() if ra else 0.0, ra.Residuals() if ra else [],
+                           ra.Poles() if ra else [], "")
+
+    def solve_inv(self, sol: np.ndarray, b: np.ndarray) -> SolverOutput:
+        ra = self.ra
+        return self._solve(sol, b, ra.InvConst() if ra else 0.0, ra.InvResiduals() if ra else [],
+                           ra.InvPoles() if ra else [], "Inverse")
+
+    def solve_noReconstruct(self, shifted_sol: list, b: np.ndarray) -> SolverOutput:
+        if self.ra is None or not self.ra.InvPoles():
+            raise IroError(BAD_ARG, "[RationalSolver] Inverse rational approximation not initialized yet")
+        return self.ms.solve(shifted_sol, b, self.ra.InvPoles())
+
+    def solve_noReconstruct_inv(self, shifted_sol: list, b: np.ndarray) -> SolverOutput:
+        if self.ra is None or not self.ra.Poles():
+            raise IroError(BAD_ARG, "[RationalSolver] Rational approximation not initialized yet")
+        return self.ms.solve(shifted_sol, b, self.ra.Poles())
+
+
+# ---- propagators: e/o inversion and the 12 spin-colour sources --------------------------
+
+class Source_local:
+    """Source_local (lib/Measurements/FermionicM/source_types.hpp:22-66): a
+    point source at lattice coordinates sp = [x, y, z, t]; mksrc(s, c) is the
+    full-lattice Format_F field with 1 at index_r(c, s, site)."""
+
+    def __init__(self, sp, L):
+        self.sp, self.L = [int(v) for v in sp], [int(v) for v in L]
+        x, y, z, t = (self.sp[i] % self.L[i] for i in range(4))
+        self.site = x + self.L[0] * (y + self.L[1] * (z + self.L[2] * t))
+        self.V = int(np.prod(self.L))
+
+    def mksrc(self, s: int, c: int) -> np.ndarray:
+        f = np.zeros(24 * self.V)
+        f[2 * (c + 3 * s) + 24 * self.site] = 1.0
+        return f
+
+
+class Inverter_WilsonLike:
+    """EvenOddUtils::Inverter_WilsonLike(D, solver) (lib/Dirac_ops/eoUtils.hpp:23-48)
+    for D a Dirac_Wilson_EvenOdd or Dirac_Clover_EvenOdd and solver a
+    Solver_CG on Fopr_DdagD(D): invert(sol, src) solves the full-lattice
+    system through the Schur complement (eoUtils.cpp:43-81)."""
+
+    def __init__(self, D, solver: "Solver_CG"):
+        if D.op not in (OP_WILSON_SCHUR_EE, OP_CLOVER_SCHUR_EE):
+            raise IroError(BAD_ARG, "Inverter_WilsonLike needs an even/odd operator")
+        self.D, self.slv = D, solver
+
+    def invert_many(self, src: np.ndarray, nrhs: int):
+        """nrhs full-lattice sources at once; returns (sol, [SolverOutput], status)."""
+        D = self.D
+        D.ctx.upload_gauge(D.u)
+        n = 24 * D.ctx.V
+        src = _f64(src, n * nrhs, "source")
+        sol = np.empty_like(src)
+        outs = (SolverOut * nrhs)()
+        rc = D.ctx._lib.iro_eo_invert(D.ctx.h, D.op, D.mass, D.csw, ctypes.byref(self.slv.params),
+                                      _ptr(src), _ptr(sol), nrhs, outs)
+        if rc not in (OK, NOT_CONVERGED):
+            D.ctx.check(rc, "iro_eo_invert")
+        res = [SolverOutput(o.diff, o.iterations, o.timing_ms, "CG solver", o.reliable_updates,
+                            o.operator_applies) for o in outs]
+        return sol, res, rc
+
+    def invert(self, sol: np.ndarray, src: np.ndarray) -> SolverOutput:
+        x, res, rc = self.invert_many(src, 1)
+        if rc != OK:
+            raise ConvergenceError(rc, "Inverter_WilsonLike: CG not converged")
+        sol[...] = x
+        return res[0]
+
+
+class Qprop_EvenOdd:
+    """Qprop_EvenOdd(D, solver) (lib/Measurements/FermionicM/qprop_EvenOdd.hpp:17-36):
+    calc(src) returns the 12 solutions D^-1 src.mksrc(s, c), s-major, computed
+    as ONE block of 12 right-hand sides (the reference runs 12 inversions,
+    qprop_EvenOdd.cpp:10-21)."""
+
+    def __init__(self, D, solver: "Solver_CG"):
+        self.inv = Inverter_WilsonLike(D, solver)
+        self.last_outputs = []
+
+    def calc(self, src) -> list:
+        if isinstance(src, (list, tuple)):
+            srcs = np.stack([_f64(f) for f in src])
+        else:
+            srcs = np.stack([src.mksrc(s, c) for s in range(4) for c in range(3)])
+        x, res, rc = self.inv.invert_many(srcs.ravel(), srcs.shape[0])
+        self.last_outputs = res
+        if rc != OK:
+            raise ConvergenceError(rc, "Qprop_EvenOdd: CG not converged")
+        return list(x.reshape(srcs.shape[0], -1))
+
+
+class Qprop:
+    """Qprop(D, solver) (lib/Measurements/FermionicM/qprop.cpp:8-25) on the
+    full-lattice operator: sol = (D^dag D)^-1 D^dag src for the 12 point
+    sources, solved as one block."""
+
+    def __init__(self, D, solver: "Solver_CG"):
+        if D.op not in (OP_WILSON_FULL, OP_CLOVER_FULL):
+            raise IroError(BAD_ARG, "Qprop needs a full-lattice operator")
+        self.D, self.slv = D, solver
+        self.last_outputs = []
+
+    def calc(self, src) -> list:
+        if isinstance(src, (list, tuple)):
+            srcs = [_f64(f) for f in src]
+        else:
+            srcs = [src.mksrc(s, c) for s in range(4) for c in range(3)]
+        b = np.concatenate([self.D.mult_dag(f) for f in srcs])
+        x, res, rc = self.slv.solve_many(b, len(srcs))
+        self.last_outputs = res
+        if rc != OK:
+            raise ConvergenceError(rc, "Qprop: CG not converged")
+        return list(x.reshape(len(srcs), -1))

@@ -782,5 +782,7 @@ int64_t volume(iro_ctx* c) { return c->V; }
 bool op_is_full(int op) { return is_full(op); }
 int op_subset(int op) { return input_subset(op); }
 bool op_ok(int op) { return op_valid(op); }
+int clover_ready(iro_ctx* c, double mass, double csw) { return ensure_clover(c, mass, csw); }
+CloverPtr clover(iro_ctx* c, int prec, int p, bool inverse) { return clover_ptr(c, prec, p, inverse); }
 }  // namespace host
 }  // namespace iro

@@ -138,6 +138,19 @@ cudaError_t launch_field_strength(const Geom& g, const double* raw, int mu, int 
                                   cudaStream_t st);
 void clover_init_tables();
 
+// ---- rational-function reconstruction and clover fields (kernels.cu) --------------
+constexpr int kMaxCombine = 16;
+struct SField {
+  SpinorPtr f[kMaxCombine];
+  double a[kMaxCombine];
+};
+// y = c0 b + sum_{k<n} a_k x_k over `sites` FP64 elements
+cudaError_t launch_combine(int64_t sites, double c0, SpinorPtr b, int n, const SField& x,
+                           SpinorPtr y, cudaStream_t st);
+// out = C in for an FP64 half field of nrhs right-hand sides (C: a clover block or its inverse)
+cudaError_t launch_clover_mult(int64_t Vh, int nrhs, CloverPtr cl, SpinorPtr in, SpinorPtr out,
+                               cudaStream_t st);
+
 // ---- learned preconditioner (learned.cu) -------------------------------------------
 struct PtcGeo;
 constexpr int kMaxVec = 16;

@@ -84,6 +84,56 @@ __global__ void axpby_kernel(int64_t n, double a, SpinorPtr x, double b, SpinorP
   }
 }
 
+// RationalSolver_CG reconstruction (lib/Solver/rationalSolver_CG.cpp:29-36)
+__global__ void combine_kernel(int64_t n, double c0, SpinorPtr b, int m, SField x, SpinorPtr y) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<double> acc[12], v[12];
+    SpinorIO<PREC_DOUBLE>::load(b, i, acc);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = c0 * acc[k];
+    for (int q = 0; q < m; ++q) {
+      SpinorIO<PREC_DOUBLE>::load(x.f[q], i, v);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[k] = acc[k] + x.a[q] * v[k];
+    }
+    SpinorIO<PREC_DOUBLE>::store(y, i, acc);
+  }
+}
+
+cudaError_t launch_combine(int64_t sites, double c0, SpinorPtr b, int n, const SField& x,
+                           SpinorPtr y, cudaStream_t st) {
+  const int blk = 256;
+  int grid = int((sites + blk - 1) / blk);
+  if (grid > 148 * 16) grid = 148 * 16;
+  combine_kernel<<<grid, blk, 0, st>>>(sites, c0, b, n, x, y);
+  return cudaGetLastError();
+}
+
+// out = C in, C the FP64 clover block (or its inverse) of one parity
+__global__ void clover_mult_kernel(int64_t vh, int nrhs, CloverPtr cl, SpinorPtr in, SpinorPtr out) {
+  const int64_t n = vh * nrhs;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<double> v[12];
+    SpinorIO<PREC_DOUBLE>::load(in, i, v);
+    CloverBlock<double> B[2];
+    CloverIO<PREC_DOUBLE>::load(cl, i / nrhs, B);
+    clover_apply(B, v);
+    SpinorIO<PREC_DOUBLE>::store(out, i, v);
+  }
+}
+
+cudaError_t launch_clover_mult(int64_t Vh, int nrhs, CloverPtr cl, SpinorPtr in, SpinorPtr out,
+                               cudaStream_t st) {
+  const int64_t n = Vh * nrhs;
+  const int blk = 128;
+  int grid = int((n + blk - 1) / blk);
+  if (grid > 148 * 16) grid = 148 * 16;
+  clover_mult_kernel<<<grid, blk, 0, st>>>(Vh, nrhs, cl, in, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_axpby(int prec, int64_t Vh, int nrhs, double a, SpinorPtr x, double b,
                          SpinorPtr y, SpinorPtr v, cudaStream_t st) {
   const int64_t n = Vh * nrhs;

@@ -37,6 +37,8 @@ bool op_is_full(int op);
 int op_subset(int op);
 bool op_ok(int op);
 DevField* field_dev(iro_field* f);
+int clover_ready(iro_ctx* c, double mass, double csw);
+CloverPtr clover(iro_ctx* c, int prec, int p, bool inverse);
 }  // namespace host
 }  // namespace iro
 
@@ -235,13 +237,12 @@ extern "C" int iro_cg_solve_field(iro_ctx* c, int op, double mass, double csw,
 
 // ---- multishift CG ---------------------------------------------------------------------
 // MultiShiftSolver_CG::solve (lib/Solver/multiShiftSolver_CG.cpp:95-185) in FP64.
-extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double csw,
-                                       const double* b, int nshift, const double* shifts,
-                                       double* x, double precision, int max_iter,
-                                       iro_solver_out* out, int* nconv) {
-  if (!c || !b || !shifts || !x || !out || !nconv || nshift < 1 || nshift > MAXSHIFT ||
-      !solver_op_ok(op) || !(precision > 0.0))
-    return set_error(c, IRO_BAD_ARG, "bad multishift arguments");
+// The solve itself; the shifted solutions stay in the context's workspaces
+// (*xs_out), and are exported to x when x is given.
+static int ms_run(iro_ctx* c, int op, double mass, double csw, const double* b, int nshift,
+                  const double* shifts, double* x, double precision, int max_iter,
+                  iro_solver_out* out, int* nconv, std::vector<DevField*>* xs_out,
+                  DevField** b_out) {
   CK(cudaSetDevice(device(c)));
   auto t0 = std::chrono::steady_clock::now();
   const int sub = op_subset(op);
@@ -322,8 +323,10 @@ extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double c
     const double d1 = sn[0] / bn[0];
     if (d1 > dmax) dmax = d1;
     const size_t nfield = size_t(24) * size_t(full ? 2 * vh(c) : vh(c));
-    RC(export_field(c, *XS[k], full, x + size_t(k) * nfield));
+    if (x) RC(export_field(c, *XS[k], full, x + size_t(k) * nfield));
   }
+  if (xs_out) *xs_out = XS;
+  if (b_out) *b_out = B;
   auto t1 = std::chrono::steady_clock::now();
   out->diff = std::sqrt(dmax);
   out->iterations = m.conv_iter;
@@ -333,6 +336,52 @@ extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double c
   *nconv = m.conv_iter;
   if (m.conv_iter < 0) return set_error(c, IRO_NOT_CONVERGED, "Not converged.");
   return IRO_OK;
+}
+
+static bool ms_args_ok(iro_ctx* c, int op, const double* b, int nshift, const double* shifts,
+                       double precision, iro_solver_out* out, int* nconv) {
+  return c && b && shifts && out && nconv && nshift >= 1 && nshift <= MAXSHIFT &&
+         solver_op_ok(op) && precision > 0.0;
+}
+
+extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double csw,
+                                       const double* b, int nshift, const double* shifts,
+                                       double* x, double precision, int max_iter,
+                                       iro_solver_out* out, int* nconv) {
+  if (!x || !ms_args_ok(c, op, b, nshift, shifts, precision, out, nconv))
+    return set_error(c, IRO_BAD_ARG, "bad multishift arguments");
+  return ms_run(c, op, mass, csw, b, nshift, shifts, x, precision, max_iter, out, nconv, nullptr,
+                nullptr);
+}
+
+// RationalSolver_CG::solve (lib/Solver/rationalSolver_CG.cpp:12-39): the
+// multishift solve with the poles as shifts, then sol = c0 b + sum_i r_i x_i
+// in one pass over the shifted solutions on the device.
+extern "C" int iro_rational_cg_solve(iro_ctx* c, int op, double mass, double csw,
+                                     const double* b, int npole, const double* poles,
+                                     const double* residues, double c0, double* sol,
+                                     double precision, int max_iter, iro_solver_out* out,
+                                     int* nconv) {
+  if (!sol || !residues || !ms_args_ok(c, op, b, npole, poles, precision, out, nconv))
+    return set_error(c, IRO_BAD_ARG, "bad rational solver arguments");
+  CK(cudaSetDevice(device(c)));
+  std::vector<DevField*> xs;
+  DevField* B = nullptr;
+  const int rc = ms_run(c, op, mass, csw, b, npole, poles, nullptr, precision, max_iter, out,
+                        nconv, &xs, &B);
+  if (rc != IRO_OK && rc != IRO_NOT_CONVERGED) return rc;
+  const int sub = op_subset(op);
+  int wrc = IRO_OK;
+  DevField* Y = workspace(c, sub, PREC_DOUBLE, 1, 34, &wrc);
+  if (!Y) return wrc;
+  SField list{};
+  for (int k = 0; k < npole; ++k) {
+    list.f[k] = xs[k]->all();
+    list.a[k] = residues[k];
+  }
+  CK(launch_combine(B->sites(), c0, B->all(), npole, list, Y->all(), stream(c)));
+  RC(export_field(c, *Y, op_is_full(op), sol));
+  return rc;
 }
 
 // ---- mixed-precision reliable-update CG ----------------------------------------------
@@ -506,4 +555,71 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   }
   if (status) set_error(c, status, "mixed-precision CG not converged");
   return status;
+}
+
+// ---- even/odd inversion of the full operator -------------------------------------
+namespace {
+// the half `p` of a full-lattice field, as a field of its own
+DevField half_view(const DevField& F, int p) {
+  DevField h = F;
+  const SpinorPtr s = F.half(p);
+  h.subset = p;
+  h.data = s.data;
+  h.norm = s.norm;
+  h.bytes_data = F.bytes_data / 2;
+  h.bytes_norm = F.bytes_norm / 2;
+  return h;
+}
+}  // namespace
+
+// Inverter_WilsonLike::invert (lib/Dirac_ops/eoUtils.cpp:43-81), for nrhs
+// full-lattice sources at once.  With the full operator in blocks
+// D = [[A_ee, D_eo], [D_oe, A_oo]] (D_eo = -kappa H_eo; A = 1 for Wilson,
+// whose mult_ee_inv / mult_oo_inv are the identity, and the clover term for
+// clover):
+//   be  = b_e - D_eo A_oo^-1 b_o,
+//   y_e = M^-1 be by CG on M^dag M y_e = M^dag be (M the Schur operator),
+//   x_o = A_oo^-1 (b_o - D_oe y_e),
+// and sol = (y_e, x_o) in the full Format_F layout.  out[] holds the CG's
+// outputs, as the reference prints its SolverOutput.
+extern "C" int iro_eo_invert(iro_ctx* c, int op, double mass, double csw,
+                             const iro_cg_params* prm, const double* src, double* sol, int nrhs,
+                             iro_solver_out* out) {
+  if (!c || !src || !sol || !out || nrhs < 1 || nrhs > 16 || !cg_args_ok(prm, op) ||
+      (op != IRO_OP_WILSON_SCHUR_EE && op != IRO_OP_CLOVER_SCHUR_EE))
+    return set_error(c, IRO_BAD_ARG, "bad e/o inverter arguments");
+  CK(cudaSetDevice(device(c)));
+  const bool cl = op == IRO_OP_CLOVER_SCHUR_EE;
+  if (cl) RC(clover_ready(c, mass, csw));
+  int rc = IRO_OK;
+  DevField* F = workspace(c, 2, PREC_DOUBLE, nrhs, 50, &rc); if (!F) return rc;
+  DevField* BE = workspace(c, 0, PREC_DOUBLE, nrhs, 51, &rc); if (!BE) return rc;
+  DevField* RHS = workspace(c, 0, PREC_DOUBLE, nrhs, 52, &rc); if (!RHS) return rc;
+  DevField* YE = workspace(c, 0, PREC_DOUBLE, nrhs, 53, &rc); if (!YE) return rc;
+  DevField* TO = workspace(c, 1, PREC_DOUBLE, nrhs, 54, &rc); if (!TO) return rc;
+  cudaStream_t st = stream(c);
+  RC(import_field(c, src, true, *F));
+  DevField fe = half_view(*F, 0), fo = half_view(*F, 1);
+  // t_o = A_oo^-1 b_o;  be = b_e - D_eo t_o
+  const DevField* bo = &fo;
+  if (cl) {
+    CK(launch_clover_mult(vh(c), nrhs, clover(c, PREC_DOUBLE, 1, true), fo.half(1), TO->half(1), st));
+    bo = TO;
+  }
+  RC(apply(c, IRO_OP_WILSON_HOP_EO, mass, csw, false, *bo, *BE, nullptr, 0, nullptr));
+  RC(axpby(c, 1.0, fe, -1.0, *BE, *BE));
+  // M^dag M y_e = M^dag be
+  RC(apply(c, op, mass, csw, true, *BE, *RHS, nullptr, 0, nullptr));
+  const int solve_rc = cg_any(c, op, mass, csw, prm, RHS, YE, nrhs, out);
+  if (solve_rc != IRO_OK && solve_rc != IRO_NOT_CONVERGED) return solve_rc;
+  // x_o = A_oo^-1 (b_o - D_oe y_e), written over the odd half of F; y_e over the even half
+  RC(apply(c, IRO_OP_WILSON_HOP_OE, mass, csw, false, *YE, *TO, nullptr, 0, nullptr));
+  RC(axpby(c, 1.0, fo, -1.0, *TO, *TO));
+  if (cl)
+    CK(launch_clover_mult(vh(c), nrhs, clover(c, PREC_DOUBLE, 1, true), TO->half(1), fo.half(1), st));
+  else
+    RC(axpby(c, 1.0, *TO, 0.0, *TO, fo));
+  RC(axpby(c, 1.0, *YE, 0.0, *YE, fe));
+  RC(export_field(c, *F, true, sol));
+  return solve_rc;
 }

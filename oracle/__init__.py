@@ -85,6 +85,9 @@ class Port:
         lib.orc_cg.argtypes = [L4, _D, _I, D, D, _D, _D, D, _I, _D, ctypes.POINTER(_I)]
         lib.orc_multishift.argtypes = [L4, _D, _I, D, D, _D, _I, _D, _D, D, _I, _D,
                                        ctypes.POINTER(_I)]
+        lib.orc_eo_invert.argtypes = [L4, _D, D, _D, _D, D, _I, _D, ctypes.POINTER(_I)]
+        lib.orc_rational.argtypes = [L4, _D, _I, D, D, _D, _I, _D, _D, D, _D, D, _I, _D,
+                                     ctypes.POINTER(_I)]
 
     @staticmethod
     def _L(L):
@@ -145,6 +148,34 @@ class Port:
         return x.reshape(sh.size, b.size), nc.value, diff.value
 
 
+def _port_eo_invert(self, L, u, mass, src, prec, maxiter):
+    """Inverter_WilsonLike::invert (Wilson e/o) of one full-lattice source."""
+    src = np.ascontiguousarray(src, np.float64)
+    sol = np.empty_like(src)
+    diff = ctypes.c_double()
+    it = ctypes.c_int()
+    self.lib.orc_eo_invert(self._L(L), _p(u), mass, _p(src), _p(sol), prec, maxiter,
+                           ctypes.byref(diff), ctypes.byref(it))
+    return sol, it.value, diff.value
+
+
+def _port_rational(self, L, u, op, mass, csw, b, poles, residues, c0, prec, maxiter):
+    """RationalSolver_CG::solve: c0 b + sum_i r_i (A + p_i)^-1 b."""
+    b = np.ascontiguousarray(b, np.float64)
+    p = np.ascontiguousarray(poles, np.float64)
+    r = np.ascontiguousarray(residues, np.float64)
+    sol = np.empty_like(b)
+    diff = ctypes.c_double()
+    nc = ctypes.c_int()
+    self.lib.orc_rational(self._L(L), _p(u), op, mass, csw, _p(b), p.size, _p(p), _p(r), c0, _p(sol),
+                          prec, maxiter, ctypes.byref(diff), ctypes.byref(nc))
+    return sol, nc.value, diff.value
+
+
+Port.eo_invert = _port_eo_invert
+Port.rational = _port_rational
+
+
 class Ref:
     """The reference's own classes; one lattice per process (ref_init)."""
 
@@ -161,6 +192,9 @@ class Ref:
         lib.ref_multishift_solve.argtypes = [_D, _I, D, D, _D, _I, _D, _D, D, _I, _D,
                                              ctypes.POINTER(_I)]
         lib.ref_eo_mult_throughput.argtypes = [_D, D, _D, _D, _I, _I, _D]
+        lib.ref_eo_invert.argtypes = [_D, D, _D, _D, _I, D, _I]
+        lib.ref_rational_solve.argtypes = [_D, _I, D, D, _D, _I, _D, _D, D, _D, D, _I, _D,
+                                           ctypes.POINTER(_I)]
         self.L = None
 
     def init(self, L):
@@ -217,6 +251,25 @@ class Ref:
                                                 prec, maxiter, ctypes.byref(diff), ctypes.byref(nc)),
                   "ref_multishift_solve")
         return x.reshape(sh.size, b.size), nc.value, diff.value
+
+    def eo_invert(self, u, mass, srcs, prec, maxiter):
+        """Inverter_WilsonLike::invert of each full-lattice source (rows of srcs)."""
+        srcs = np.ascontiguousarray(np.atleast_2d(srcs), np.float64)
+        sol = np.empty_like(srcs)
+        self._chk(self.lib.ref_eo_invert(_p(u), mass, _p(srcs), _p(sol), srcs.shape[0], prec, maxiter),
+                  "ref_eo_invert")
+        return sol
+
+    def rational(self, u, op, mass, csw, b, poles, residues, c0, prec, maxiter):
+        p = np.ascontiguousarray(poles, np.float64)
+        r = np.ascontiguousarray(residues, np.float64)
+        sol = np.empty_like(b)
+        diff = ctypes.c_double()
+        nc = ctypes.c_int()
+        self._chk(self.lib.ref_rational_solve(_p(u), op, mass, csw, _p(b), p.size, _p(p), _p(r), c0,
+                                              _p(sol), prec, maxiter, ctypes.byref(diff),
+                                              ctypes.byref(nc)), "ref_rational_solve")
+        return sol, nc.value, diff.value
 
     def eo_mult_throughput(self, u, mass, f, nthreads, reps):
         out = np.empty_like(f)

@@ -557,3 +557,60 @@ int orc_multishift(const int L[4], const double* u, int op, double mass, double 
   free(A.tmp);
   return *nconv < 0 ? 1 : 0;
 }
+
+/* ---- callers of the solvers ------------------------------------------------ */
+
+/* EvenOddUtils::Inverter_WilsonLike::invert for Dirac_Wilson_EvenOdd with
+   Solver_CG (lib/Dirac_ops/eoUtils.cpp:43-81): be = b_e - Deo b_o; y_e by CG on
+   M^dag M y_e = M^dag be; b_o -= Doe y_e; sol = (y_e, b_o) in the full
+   lexicographic layout (mult_ee_inv / mult_oo_inv are the identity). */
+int orc_eo_invert(const int L[4], const double* u, double mass, const double* src, double* sol,
+                  double prec, int maxiter, double* diff, int* iters) {
+  Geom g;
+  geom_init(&g, L);
+  const long nh = 24 * g.Vh;
+  double* be = malloc(sizeof(double) * nh);
+  double* bo = malloc(sizeof(double) * nh);
+  double* t = malloc(sizeof(double) * nh);
+  double* rhs = malloc(sizeof(double) * nh);
+  double* ye = malloc(sizeof(double) * nh);
+  for (long hs = 0; hs < g.Vh; ++hs) {
+    memcpy(be + 24 * hs, src + 24 * g.eo_site[hs], sizeof(double) * 24);
+    memcpy(bo + 24 * hs, src + 24 * g.eo_site[g.Vh + hs], sizeof(double) * 24);
+  }
+  orc_wilson_hop(L, u, mass, 0, 0, bo, t);
+  for (long i = 0; i < nh; ++i) be[i] -= t[i];
+  orc_wilson_eo(L, u, mass, 1, be, rhs);
+  int rc = orc_cg(L, u, ORC_WILSON_EO, mass, 0.0, rhs, ye, prec, maxiter, diff, iters);
+  orc_wilson_hop(L, u, mass, 1, 0, ye, t);
+  for (long i = 0; i < nh; ++i) bo[i] -= t[i];
+  for (long hs = 0; hs < g.Vh; ++hs) {
+    memcpy(sol + 24 * g.eo_site[hs], ye + 24 * hs, sizeof(double) * 24);
+    memcpy(sol + 24 * g.eo_site[g.Vh + hs], bo + 24 * hs, sizeof(double) * 24);
+  }
+  free(be);
+  free(bo);
+  free(t);
+  free(rhs);
+  free(ye);
+  geom_free(&g);
+  return rc;
+}
+
+/* RationalSolver_CG::solve (lib/Solver/rationalSolver_CG.cpp:12-39):
+   sol = c0 b + sum_i r_i x_i with x_i from the multishift solve at the poles. */
+int orc_rational(const int L[4], const double* u, int op, double mass, double csw,
+                 const double* b, int npole, const double* poles, const double* residues,
+                 double c0, double* sol, double prec, int maxiter, double* diff, int* nconv) {
+  const long V = (long)L[0] * L[1] * L[2] * L[3];
+  const long n = (op == ORC_WILSON_EO) ? 12 * V : 24 * V;
+  double* x = malloc(sizeof(double) * n * npole);
+  int rc = orc_multishift(L, u, op, mass, csw, b, npole, poles, x, prec, maxiter, diff, nconv);
+  for (long i = 0; i < n; ++i) {
+    double v = c0 * b[i];
+    for (int k = 0; k < npole; ++k) v += residues[k] * x[k * n + i];
+    sol[i] = v;
+  }
+  free(x);
+  return rc;
+}

@@ -32,6 +32,12 @@ int orc_multishift(const int L[4], const double* u, int op, double mass, double 
                    const double* b, int nshift, const double* shifts, double* x, double prec,
                    int maxiter, double* diff, int* nconv);
 
+int orc_eo_invert(const int L[4], const double* u, double mass, const double* src, double* sol,
+                  double prec, int maxiter, double* diff, int* iters);
+int orc_rational(const int L[4], const double* u, int op, double mass, double csw,
+                 const double* b, int npole, const double* poles, const double* residues,
+                 double c0, double* sol, double prec, int maxiter, double* diff, int* nconv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,7 @@
 #include "Dirac_ops/dirac_wilson.hpp"
 #include "Dirac_ops/dirac_wilson_EvenOdd.hpp"
 #include "Dirac_ops/dirac_clover.hpp"
+#include "Dirac_ops/eoUtils.hpp"
 #include "Fopr/fopr.h"
 #include "Solver/solver_CG.hpp"
 #include "Solver/multiShiftSolver_CG.hpp"
@@ -251,6 +252,67 @@ int ref_multishift_solve(const double* u, int op, double mass, double csw, const
     int nc = -1;
     SolverOutput o = slv.solve(xs, fb, sig, d, nc);
     for (int i = 0; i < nshift; ++i) store(xs[i], x + i * n);
+    *diff = o.diff;
+    *nconv = nc;
+    delete D;
+    return 0;
+  });
+}
+
+// EvenOddUtils::Inverter_WilsonLike(Dirac_Wilson_EvenOdd, Solver_CG on
+// Fopr_DdagD)::invert (lib/Dirac_ops/eoUtils.cpp:43-81) for `nsrc`
+// consecutive full-lattice sources, one after the other, as
+// Qprop_EvenOdd::calc does (lib/Measurements/FermionicM/qprop_EvenOdd.cpp:10-21).
+int ref_eo_invert(const double* u, double mass, const double* src, double* sol, int nsrc,
+                  double prec, int maxiter) {
+  return run_big_stack([=]() {
+    Quiet q;
+    Field U = make_field(u, gsize());
+    Dirac_Wilson_EvenOdd<Dirac_Wilson> D(mass, &U);
+    Fopr_DdagD A(&D);
+    Solver_CG slv(prec, maxiter, &A);
+    EvenOddUtils::Inverter_WilsonLike inv(&D, &slv);
+    const size_t n = fsize_full();
+    for (int k = 0; k < nsrc; ++k) {
+      Field b = make_field(src + k * n, n);
+      Field x(n);
+      inv.invert(x, b);
+      store(x, sol + k * n);
+    }
+    return 0;
+  });
+}
+
+// RationalSolver_CG::solve (lib/Solver/rationalSolver_CG.cpp:12-39) with the
+// reference's MultiShiftSolver_CG: the reference builds the residues, poles
+// and constant with a GMP Remez algorithm (lib/Tools/RationalApprox), which
+// needs GMP/MPFR and is not built here, so they are arguments and the
+// reconstruction sol = c0 b + sum_i r_i x_i of rationalSolver_CG.cpp:29-36 is
+// restated after the reference's multishift solve.
+int ref_rational_solve(const double* u, int op, double mass, double csw, const double* b,
+                       int npole, const double* poles, const double* residues, double c0,
+                       double* sol, double prec, int maxiter, double* diff, int* nconv) {
+  return run_big_stack([=]() {
+    Quiet q;
+    Field U = make_field(u, gsize());
+    Dirac* D = make_dirac(op, mass, csw, &U);
+    size_t n = D->fsize();
+    Field fb = make_field(b, n);
+    Fopr_DdagD A(D);
+    MultiShiftSolver_CG slv(&A, prec, maxiter);
+    std::vector<Field> xs(npole, Field(n));
+    std::vector<double> sig(poles, poles + npole);
+    double d = 0.0;
+    int nc = -1;
+    SolverOutput o = slv.solve(xs, fb, sig, d, nc);
+    Field s = fb;
+    s *= c0;
+    for (int i = 0; i < npole; ++i) {
+      Field t = xs[i];
+      t *= residues[i];
+      s += t;
+    }
+    store(s, sol);
     *diff = o.diff;
     *nconv = nc;
     delete D;

@@ -58,3 +58,30 @@ def test_multishift(port, golden_full, name, op, src):
     for k in range(len(g["shifts"])):
         assert rel(x[k], g[f"ms_{name}_x"][k]) < TOL_SOL
     assert abs(diff - float(g[f"ms_{name}_diff"])) < 5e-2 * float(g[f"ms_{name}_diff"])
+
+
+def test_eo_invert(port, golden_full):
+    """Inverter_WilsonLike::invert (eoUtils.cpp:43-81) of the Gaussian source
+    and of the 12 point sources of Qprop_EvenOdd::calc."""
+    g = golden_full
+    L, u, m = g["L"], g["u"], float(g["mass"])
+    x, it, diff = port.eo_invert(L, u, m, g["f_full"], 1e-20, 5000)
+    assert rel(x, g["eoinv_x"]) < TOL_SOL
+    site = int(g["qprop_site"])
+    V = int(np.prod(L))
+    for k in (0, 5, 11):
+        s, c = divmod(k, 3)
+        src = np.zeros(24 * V)
+        src[24 * site + 2 * (c + 3 * s)] = 1.0
+        xk, _, _ = port.eo_invert(L, u, m, src, 1e-20, 5000)
+        assert rel(xk, g["qprop_x"][k]) < TOL_SOL
+
+
+@pytest.mark.parametrize("name,op,src", [("wilson_full", 0, "f_full"), ("wilson_eo", 1, "f_half")])
+def test_rational(port, golden_full, name, op, src):
+    """RationalSolver_CG::solve reconstruction c0 b + sum r_i x_i."""
+    g = golden_full
+    x, nc, diff = port.rational(g["L"], g["u"], op, float(g["mass"]), float(g["csw"]), g[src],
+                                g["rat_poles"], g["rat_res"], float(g["rat_c0"]), 1e-20, 5000)
+    assert nc == int(g[f"rat_{name}_nconv"])
+    assert rel(x, g[f"rat_{name}_x"]) < TOL_SOL
