@@ -242,6 +242,17 @@ int iro_rational_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const d
 int iro_eo_invert(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
                   const double* src, double* sol, int nrhs, iro_solver_out* out);
 
+/* Molecular-dynamics force of the Wilson operator, FP64:
+   op = IRO_OP_WILSON_FULL: Dirac_Wilson::md_force(eta, zeta)
+        (lib/Dirac_ops/dirac_wilson.cpp:41-91), eta and zeta full-lattice
+        Format_F arrays;
+   op = IRO_OP_WILSON_SCHUR_EE: Dirac_Wilson_EvenOdd::md_force(eta, zeta)
+        (lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:95-117), eta and zeta even
+        halves (24*V/2 doubles).
+   force receives the Format_G field (72*V doubles), overwritten. */
+int iro_md_force(iro_ctx* ctx, int op, double mass, const double* eta, const double* zeta,
+                 double* force);
+
 /* ---- learned preconditioner and flexible GCR --------------------------------
    No counterpart in the reference (its solvers are CG, BiCGStab and
    multishift CG, lib/Solver/solver_Factory.cpp:10-45).  A gauge-equivariant

@@ -783,6 +783,9 @@ bool op_is_full(int op) { return is_full(op); }
 int op_subset(int op) { return input_subset(op); }
 bool op_ok(int op) { return op_valid(op); }
 int clover_ready(iro_ctx* c, double mass, double csw) { return ensure_clover(c, mass, csw); }
+GaugePtr gauge_double(iro_ctx* c) { return gauge_ptr(c, PREC_DOUBLE); }
+int gauge_recon(iro_ctx* c) { return c->recon; }
+bool gauge_loaded(iro_ctx* c) { return c->has_gauge; }
 CloverPtr clover(iro_ctx* c, int prec, int p, bool inverse) { return clover_ptr(c, prec, p, inverse); }
 }  // namespace host
 }  // namespace iro

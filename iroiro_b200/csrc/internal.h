@@ -151,6 +151,12 @@ cudaError_t launch_combine(int64_t sites, double c0, SpinorPtr b, int n, const S
 cudaError_t launch_clover_mult(int64_t Vh, int nrhs, CloverPtr cl, SpinorPtr in, SpinorPtr out,
                                cudaStream_t st);
 
+// ---- molecular-dynamics force (forces.cu) ------------------------------------------
+// F[mu][lex site][18] += w (1 - g_mu) U_mu(x) psi(x+mu) (x) chi(x)^dag over the
+// sites x of parity p (gamma5 on both fields when g5)
+cudaError_t launch_force(const Geom& g, const GaugePtr& gauge, int recon, int p, SpinorPtr psi,
+                         SpinorPtr chi, int g5, double w, double* F, cudaStream_t st);
+
 // ---- learned preconditioner (learned.cu) -------------------------------------------
 struct PtcGeo;
 constexpr int kMaxVec = 16;

@@ -39,6 +39,11 @@ bool op_ok(int op);
 DevField* field_dev(iro_field* f);
 int clover_ready(iro_ctx* c, double mass, double csw);
 CloverPtr clover(iro_ctx* c, int prec, int p, bool inverse);
+GaugePtr gauge_double(iro_ctx* c);
+int gauge_recon(iro_ctx* c);
+bool gauge_loaded(iro_ctx* c);
+const Geom& geom(iro_ctx* c);
+int64_t volume(iro_ctx* c);
 }  // namespace host
 }  // namespace iro
 
@@ -622,4 +627,59 @@ extern "C" int iro_eo_invert(iro_ctx* c, int op, double mass, double csw,
   RC(axpby(c, 1.0, *YE, 0.0, *YE, fe));
   RC(export_field(c, *F, true, sol));
   return solve_rc;
+}
+
+// ---- molecular-dynamics force ----------------------------------------------------
+// Dirac_Wilson::md_force (lib/Dirac_ops/dirac_wilson.cpp:41-58):
+//   F = -kappa sum_{x, mu} [mkfrc(eta, zeta) + mkfrc(g5 zeta, g5 eta)]
+// Dirac_Wilson_EvenOdd::md_force (lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:95-117):
+//   A = Doe eta, B = Doe^dag zeta (odd);
+//   F = kappa [Deo.p(A, zeta) + Doe.m(A, zeta) + Doe.p(eta, B) + Deo.m(eta, B)]
+// with X.p(e, z) = mkfrc(e, z) and X.m(e, z) = mkfrc(g5 z, g5 e) on the
+// output sites of X (even for Deo, odd for Doe), in that order.
+extern "C" int iro_md_force(iro_ctx* c, int op, double mass, const double* eta,
+                            const double* zeta, double* force) {
+  if (!c || !eta || !zeta || !force || (op != IRO_OP_WILSON_FULL && op != IRO_OP_WILSON_SCHUR_EE))
+    return set_error(c, IRO_BAD_ARG, "bad md_force arguments");
+  if (!gauge_loaded(c)) return set_error(c, IRO_NO_GAUGE, "no gauge field uploaded");
+  CK(cudaSetDevice(device(c)));
+  const bool full = op == IRO_OP_WILSON_FULL;
+  const double k = 0.5 / (4.0 + mass);
+  int rc = IRO_OK;
+  const int sub = full ? 2 : 0;
+  DevField* E = workspace(c, sub, PREC_DOUBLE, 1, 60, &rc); if (!E) return rc;
+  DevField* Z = workspace(c, sub, PREC_DOUBLE, 1, 61, &rc); if (!Z) return rc;
+  cudaStream_t st = stream(c);
+  RC(import_field(c, eta, full, *E));
+  RC(import_field(c, zeta, full, *Z));
+  const size_t nF = size_t(72) * size_t(volume(c));
+  double* F = nullptr;
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&F), nF * sizeof(double), st));
+  struct FreeF {
+    double* p;
+    cudaStream_t s;
+    ~FreeF() { if (p) cudaFreeAsync(p, s); }
+  } guard{F, st};
+  CK(cudaMemsetAsync(F, 0, nF * sizeof(double), st));
+  const Geom& g = geom(c);
+  const GaugePtr U = gauge_double(c);
+  const int recon = gauge_recon(c);
+  if (full) {
+    for (int p = 0; p < 2; ++p) {
+      CK(launch_force(g, U, recon, p, E->half(1 - p), Z->half(p), 0, -k, F, st));
+      CK(launch_force(g, U, recon, p, Z->half(1 - p), E->half(p), 1, -k, F, st));
+    }
+  } else {
+    DevField* A = workspace(c, 1, PREC_DOUBLE, 1, 62, &rc); if (!A) return rc;
+    DevField* B = workspace(c, 1, PREC_DOUBLE, 1, 63, &rc); if (!B) return rc;
+    RC(apply(c, IRO_OP_WILSON_HOP_OE, mass, 0.0, false, *E, *A, nullptr, 0, nullptr));
+    RC(apply(c, IRO_OP_WILSON_HOP_OE, mass, 0.0, true, *Z, *B, nullptr, 0, nullptr));
+    CK(launch_force(g, U, recon, 0, A->half(1), Z->half(0), 0, k, F, st));
+    CK(launch_force(g, U, recon, 1, Z->half(0), A->half(1), 1, k, F, st));
+    CK(launch_force(g, U, recon, 1, E->half(0), B->half(1), 0, k, F, st));
+    CK(launch_force(g, U, recon, 0, B->half(1), E->half(0), 1, k, F, st));
+  }
+  CK(cudaMemcpyAsync(force, F, nF * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return IRO_OK;
 }

@@ -86,6 +86,7 @@ class Port:
         lib.orc_multishift.argtypes = [L4, _D, _I, D, D, _D, _I, _D, _D, D, _I, _D,
                                        ctypes.POINTER(_I)]
         lib.orc_eo_invert.argtypes = [L4, _D, D, _D, _D, D, _I, _D, ctypes.POINTER(_I)]
+        lib.orc_md_force.argtypes = [L4, _D, D, _I, _D, _D, _D]
         lib.orc_rational.argtypes = [L4, _D, _I, D, D, _D, _I, _D, _D, D, _D, D, _I, _D,
                                      ctypes.POINTER(_I)]
 
@@ -172,7 +173,16 @@ def _port_rational(self, L, u, op, mass, csw, b, poles, residues, c0, prec, maxi
     return sol, nc.value, diff.value
 
 
+def _port_md_force(self, L, u, mass, eo, eta, zeta):
+    """md_force of the full (eo=False) or e/o (eo=True) Wilson operator."""
+    F = np.empty(72 * int(np.prod(L)))
+    self.lib.orc_md_force(self._L(L), _p(u), mass, 1 if eo else -1, _p(np.ascontiguousarray(eta)),
+                          _p(np.ascontiguousarray(zeta)), _p(F))
+    return F
+
+
 Port.eo_invert = _port_eo_invert
+Port.md_force = _port_md_force
 Port.rational = _port_rational
 
 
@@ -193,6 +203,7 @@ class Ref:
                                              ctypes.POINTER(_I)]
         lib.ref_eo_mult_throughput.argtypes = [_D, D, _D, _D, _I, _I, _D]
         lib.ref_eo_invert.argtypes = [_D, D, _D, _D, _I, D, _I]
+        lib.ref_md_force.argtypes = [_D, _I, D, _D, _D, _D]
         lib.ref_rational_solve.argtypes = [_D, _I, D, D, _D, _I, _D, _D, D, _D, D, _I, _D,
                                            ctypes.POINTER(_I)]
         self.L = None
@@ -270,6 +281,12 @@ class Ref:
                                               _p(sol), prec, maxiter, ctypes.byref(diff),
                                               ctypes.byref(nc)), "ref_rational_solve")
         return sol, nc.value, diff.value
+
+    def md_force(self, u, op, mass, eta, zeta):
+        """Dirac_Wilson[_EvenOdd]::md_force(eta, zeta) as a Format_G array."""
+        F = np.empty(72 * int(np.prod(self.L)))
+        self._chk(self.lib.ref_md_force(_p(u), op, mass, _p(eta), _p(zeta), _p(F)), "ref_md_force")
+        return F
 
     def eo_mult_throughput(self, u, mass, f, nthreads, reps):
         out = np.empty_like(f)

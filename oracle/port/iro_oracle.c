@@ -614,3 +614,92 @@ int orc_rational(const int L[4], const double* u, int op, double mass, double cs
   free(x);
   return rc;
 }
+
+/* ---- molecular-dynamics force --------------------------------------------- */
+
+/* Dirac_Wilson::mkfrc (lib/Dirac_ops/dirac_wilson.cpp:60-91) on the output
+   sites of parity pout (-1: every site): xie = (1 - gamma_mu) U_mu(x) eta(x+mu)
+   (mult_p[mu], dirac_wilson_improved.code), F[mu](x)_{ab} += sum_s xie_{a,s}
+   conj(zeta_{b,s}); half fields are indexed by hs as in hop_accumulate. */
+static void mkfrc(const Geom* g, const double* u, int pout, const double* eta, const double* zeta,
+                  double* F) {
+  spin_init();
+  const long nout = pout < 0 ? g->V : g->Vh;
+  for (int mu = 0; mu < 4; ++mu)
+    for (long o = 0; o < nout; ++o) {
+      const long x = pout < 0 ? o : g->eo_site[pout * g->Vh + o];
+      const long y = neighbour(g, x, mu, 1);
+      const long yi = pout < 0 ? y : g->half_of[y];
+      cplx uf[4][3], xie[4][3];
+      for (int s = 0; s < 4; ++s)
+        for (int a = 0; a < 3; ++a) {
+          cplx acc = 0;
+          for (int b = 0; b < 3; ++b) acc += uget(u, g->V, x, mu, a, b) * fget(eta, yi, s, b);
+          uf[s][a] = acc;
+        }
+      for (int s = 0; s < 4; ++s)
+        for (int a = 0; a < 3; ++a) {
+          cplx v = uf[s][a];
+          for (int t = 0; t < 4; ++t) v -= GAM[mu][s][t] * uf[t][a];
+          xie[s][a] = v;
+        }
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          cplx acc = 0;
+          for (int s = 0; s < 4; ++s) acc += xie[s][a] * conj(fget(zeta, o, s, b));
+          double* p = F + 18 * (x + g->V * mu) + 2 * (3 * a + b);
+          p[0] += creal(acc);
+          p[1] += cimag(acc);
+        }
+    }
+}
+
+/* Dirac_Wilson::md_force (eo=-1, full lattice; dirac_wilson.cpp:41-58) and
+   Dirac_Wilson_EvenOdd::md_force (eo=1, even halves;
+   dirac_wilson_EvenOdd.hpp:95-117). */
+int orc_md_force(const int L[4], const double* u, double mass, int eo, const double* eta,
+                 const double* zeta, double* F) {
+  Geom g;
+  geom_init(&g, L);
+  const double k = kappa_of(mass);
+  memset(F, 0, sizeof(double) * 72 * g.V);
+  if (eo < 0) {
+    const long n = 24 * g.V;
+    double* e5 = malloc(sizeof(double) * n);
+    double* z5 = malloc(sizeof(double) * n);
+    orc_gamma5(g.V, eta, e5);
+    orc_gamma5(g.V, zeta, z5);
+    mkfrc(&g, u, -1, eta, zeta, F);
+    mkfrc(&g, u, -1, z5, e5, F);
+    for (long i = 0; i < 72 * g.V; ++i) F[i] *= -k;
+    free(e5);
+    free(z5);
+  } else {
+    const long n = 24 * g.Vh;
+    double* A = malloc(sizeof(double) * n);  /* Doe eta */
+    double* B = malloc(sizeof(double) * n);  /* Doe^dag zeta */
+    double* a5 = malloc(sizeof(double) * n);
+    double* b5 = malloc(sizeof(double) * n);
+    double* e5 = malloc(sizeof(double) * n);
+    double* z5 = malloc(sizeof(double) * n);
+    orc_wilson_hop(L, u, mass, 1, 0, eta, A);
+    orc_wilson_hop(L, u, mass, 1, 1, zeta, B);
+    orc_gamma5(g.Vh, A, a5);
+    orc_gamma5(g.Vh, B, b5);
+    orc_gamma5(g.Vh, eta, e5);
+    orc_gamma5(g.Vh, zeta, z5);
+    mkfrc(&g, u, 0, A, zeta, F);   /* Deo.md_force_p(A, zeta) */
+    mkfrc(&g, u, 1, z5, a5, F);    /* Doe.md_force_m(A, zeta) */
+    mkfrc(&g, u, 1, eta, B, F);    /* Doe.md_force_p(eta, B) */
+    mkfrc(&g, u, 0, b5, e5, F);    /* Deo.md_force_m(eta, B) */
+    for (long i = 0; i < 72 * g.V; ++i) F[i] *= k;
+    free(A);
+    free(B);
+    free(a5);
+    free(b5);
+    free(e5);
+    free(z5);
+  }
+  geom_free(&g);
+  return 0;
+}

@@ -38,6 +38,9 @@ int orc_rational(const int L[4], const double* u, int op, double mass, double cs
                  const double* b, int npole, const double* poles, const double* residues,
                  double c0, double* sol, double prec, int maxiter, double* diff, int* nconv);
 
+int orc_md_force(const int L[4], const double* u, double mass, int eo, const double* eta,
+                 const double* zeta, double* F);
+
 #ifdef __cplusplus
 }
 #endif

@@ -320,6 +320,24 @@ int ref_rational_solve(const double* u, int op, double mass, double csw, const d
   });
 }
 
+// Dirac_Wilson::md_force (op OP_WILSON_FULL, lib/Dirac_ops/dirac_wilson.cpp:52-58)
+// or Dirac_Wilson_EvenOdd::md_force (op OP_WILSON_EO,
+// lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:108-117); `force` gets gsize() doubles.
+int ref_md_force(const double* u, int op, double mass, const double* eta, const double* zeta,
+                 double* force) {
+  return run_big_stack([=]() {
+    Quiet q;
+    Field U = make_field(u, gsize());
+    Dirac* D = make_dirac(op, mass, 0.0, &U);
+    Field e = make_field(eta, D->fsize());
+    Field z = make_field(zeta, D->fsize());
+    Field F = D->md_force(e, z);
+    store(F, force);
+    delete D;
+    return 0;
+  });
+}
+
 // Throughput of Dirac_Wilson_EvenOdd<Dirac_Wilson>::mult: `nthreads`
 // independent workers, each applying the operator `reps` times to its own
 // copy of `in` (the reference's kernel is single-threaded per process, so

@@ -85,3 +85,12 @@ def test_rational(port, golden_full, name, op, src):
                                 g["rat_poles"], g["rat_res"], float(g["rat_c0"]), 1e-20, 5000)
     assert nc == int(g[f"rat_{name}_nconv"])
     assert rel(x, g[f"rat_{name}_x"]) < TOL_SOL
+
+
+def test_md_force(port, golden):
+    """Dirac_Wilson::md_force and Dirac_Wilson_EvenOdd::md_force."""
+    g = golden
+    L, u, m = g["L"], g["u"], float(g["mass"])
+    assert rel(port.md_force(L, u, m, False, g["force_eta"], g["force_zeta"]), g["force_full"]) < TOL_FP64
+    assert rel(port.md_force(L, u, m, True, g["force_eta_half"], g["force_zeta_half"]),
+               g["force_eo"]) < TOL_FP64
