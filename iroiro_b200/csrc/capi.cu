@@ -260,6 +260,7 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
     }
     HopLaunch T = L;
     T.red_mask = 0;
+    T.cg = 0;  // tuning launches must not touch the solver's fields
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -297,7 +298,11 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
 // reduction to the last kernel of the operator (|out|^2, |xin|^2, (xin,out)),
 // and `skip` lets converged right-hand sides be left untouched.
 int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in,
-              DevField& out, const Reduce* red, int red_mask, const int* skip) {
+              DevField& out, const Reduce* red, int red_mask, const int* skip,
+              const CGFuse* fuse = nullptr) {
+  if (fuse && (!red || op == IRO_OP_WILSON_HOP_EO || op == IRO_OP_WILSON_HOP_OE ||
+               op == IRO_OP_CLOVER_HOP_OE_INV))
+    return fail(c, IRO_BAD_ARG, "fused CG update needs a full or Schur operator and a reduction");
   if (!c->has_gauge) return fail(c, IRO_NO_GAUGE, "no gauge field uploaded");
   if (!op_valid(op)) return fail(c, IRO_BAD_ARG, "unknown operator");
   if (in.prec != out.prec || in.nrhs != out.nrhs)
@@ -365,6 +370,13 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       if (cl) L2.clov[0] = clover_ptr(c, prec, 0, false);
       L2.scale = k;
       if (red) { L2.red = *red; L2.red_mask = red_mask; }
+      if (fuse) {
+        L2.cg = 1;
+        L2.cst = fuse->st;
+        L2.cx[0] = fuse->x->half(0);
+        L2.cr[0] = fuse->r->half(0);
+        L2.cp[0] = fuse->p->half(0);
+      }
       { int rt = launch_tuned(c, L2); if (rt) return rt; }
     } break;
     case IRO_OP_WILSON_FULL:
@@ -381,6 +393,15 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       L.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
       L.scale = -k;
       if (red) { L.red = *red; L.red_mask = red_mask; }
+      if (fuse) {
+        L.cg = 1;
+        L.cst = fuse->st;
+        for (int y = 0; y < 2; ++y) {
+          L.cx[y] = fuse->x->half(y);
+          L.cr[y] = fuse->r->half(y);
+          L.cp[y] = fuse->p->half(y);
+        }
+      }
       { int rt = launch_tuned(c, L); if (rt) return rt; }
     } break;
   }
@@ -746,6 +767,10 @@ namespace host {
 int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in, DevField& out,
           const Reduce* red, int red_mask, const int* skip) {
   return apply_dev(c, op, mass, csw, dag, in, out, red, red_mask, skip);
+}
+int apply_cg(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in,
+             DevField& out, const Reduce& red, const int* skip, const CGFuse& fuse) {
+  return apply_dev(c, op, mass, csw, dag, in, out, &red, 0, skip, &fuse);
 }
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc) {
   return ws(c, subset, prec, nrhs, slot, rc);

@@ -153,6 +153,12 @@ struct HopParams {
   int red_mask;
   Reduce red;
   const int* skip;  // per-rhs converged flags, or null
+  // fused CG update (Solver_CG::solve_step's x/r update, solver_CG.cpp:120-140)
+  // on the operator's output s: r -= alpha s, x += alpha p, red[0] = |r|^2;
+  // s itself is not stored.  Off when cg == 0.
+  int cg;
+  SpinorPtr cx[2], cr[2], cp[2];  // indexed like out[]
+  const CGState* cst;
 };
 
 // VAR bit 0: at least two 256-thread blocks per SM (register cap 128);
@@ -216,6 +222,25 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_kernel(HopParams P
 #pragma unroll
       for (int k = 0; k < 12; ++k) acc[k] = ax[k] + acc[k];
     }
+    if (P.cg) {
+      // r -= alpha s; x += alpha p; |r|^2 (the solver's ST_CG_BETA totals)
+      const R a = R(P.cst[r].alpha);
+      Cx<R> rv[12], pv[12], xv2[12];
+      SpinorIO<SP>::load(P.cr[yi], tid, rv);
+      SpinorIO<SP>::load(P.cp[yi], tid, pv);
+      SpinorIO<SP>::load(P.cx[yi], tid, xv2);
+      double rr = 0.0;
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        rv[k] = rv[k] - a * acc[k];
+        xv2[k] = xv2[k] + a * pv[k];
+        rr += double(rv[k].re) * rv[k].re + double(rv[k].im) * rv[k].im;
+      }
+      SpinorIO<SP>::store(P.cr[yi], tid, rv);
+      SpinorIO<SP>::store(P.cx[yi], tid, xv2);
+      red[0] += rr;
+      continue;
+    }
     SpinorIO<SP>::store(P.out[yi], tid, acc);
     if (P.red_mask) {
       double o2 = 0.0, x2 = 0.0, xo = 0.0;
@@ -234,8 +259,9 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_kernel(HopParams P
       red[2] += xo;
     }
   }
-  if (P.red_mask) block_reduce_finish<3>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,
-                                         gridDim.x * gridDim.y);
+  if (P.red_mask || P.cg)
+    block_reduce_finish<3>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,
+                           gridDim.x * gridDim.y);
 }
 
 }  // namespace iro

@@ -26,6 +26,13 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   P.red_mask = L.red_mask;
   P.red = L.red;
   P.skip = L.skip;
+  P.cg = L.cg;
+  P.cst = L.cst;
+  for (int i = 0; i < 2; ++i) {
+    P.cx[i] = L.cx[i];
+    P.cr[i] = L.cr[i];
+    P.cp[i] = L.cp[i];
+  }
   LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks, L.block_cap);
   dim3 grid(c.grid, L.nparity);
   hop_kernel<SP, GP, RECON, DAG, EPI, SP, VAR><<<grid, c.block, 0, st>>>(P);
@@ -54,6 +61,13 @@ static cudaError_t hop_go_pair(const HopLaunch& L, cudaStream_t st) {
     P.red_mask = L.red_mask;
     P.red = L.red;
     P.skip = L.skip;
+    P.cg = L.cg;
+    P.cst = L.cst;
+    for (int i = 0; i < 2; ++i) {
+      P.cx[i] = L.cx[i];
+      P.cr[i] = L.cr[i];
+      P.cp[i] = L.cp[i];
+    }
     LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
     dim3 grid(c.grid, L.nparity);
     hop_pair_kernel<SP, DAG, EPI, VAR><<<grid, c.block, 0, st>>>(P);
@@ -83,6 +97,13 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
     P.red_mask = L.red_mask;
     P.red = L.red;
     P.skip = L.skip;
+    P.cg = L.cg;
+    P.cst = L.cst;
+    for (int i = 0; i < 2; ++i) {
+      P.cx[i] = L.cx[i];
+      P.cr[i] = L.cr[i];
+      P.cp[i] = L.cp[i];
+    }
     LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
     const int smem = stage_bytes<SP>() * c.block;
     static int opted = 0;  // largest dynamic shared memory already allowed

@@ -407,6 +407,31 @@ __device__ __forceinline__ void pair_epilogue(const HopParams& P, int yi, int hs
     for (int k = 0; k < 12; ++k)
       acc[k] = {pfma(sc, acc[k].re, ax[k].re), pfma(sc, acc[k].im, ax[k].im)};
   }
+  if (P.cg) {
+    // r -= alpha s; x += alpha p; |r|^2.  A lane whose right-hand side has left
+    // the iteration gets alpha = 0 (its values are re-stored unchanged).
+    const int r0 = int(e0 % P.nrhs);
+    const float2 a = make_float2(P.skip && P.skip[r0] ? 0.f : float(P.cst[r0].alpha),
+                                 P.skip && P.skip[r0 + 1] ? 0.f : float(P.cst[r0 + 1].alpha));
+    Cp rv[12], pv[12], xw[12];
+    PairIO<SP>::load_scaled(P.cr[yi], e0, rv);
+    PairIO<SP>::load_scaled(P.cp[yi], e0, pv);
+    PairIO<SP>::load_scaled(P.cx[yi], e0, xw);
+    float2 rr = bc(0.f);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      const float2 na = pmul(a, bc(-1.f));
+      rv[k] = {pfma(na, acc[k].re, rv[k].re), pfma(na, acc[k].im, rv[k].im)};
+      xw[k] = {pfma(a, pv[k].re, xw[k].re), pfma(a, pv[k].im, xw[k].im)};
+      rr = pfma(rv[k].re, rv[k].re, rr);
+      rr = pfma(rv[k].im, rv[k].im, rr);
+    }
+    PairIO<SP>::store(P.cr[yi], e0, rv);
+    PairIO<SP>::store(P.cx[yi], e0, xw);
+    red[0] += rr.x;
+    red[3] += rr.y;
+    return;
+  }
   PairIO<SP>::store(P.out[yi], e0, acc);
   if (P.red_mask) {
     float2 o2 = bc(0.f), x2 = bc(0.f), xo = bc(0.f);
@@ -474,7 +499,7 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_pair_kernel(HopPar
     }
     pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, acc, red);
   }
-  if (P.red_mask)
+  if (P.red_mask || P.cg)
     block_reduce_finish<3, 2>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,
                               gridDim.x * gridDim.y);
 }

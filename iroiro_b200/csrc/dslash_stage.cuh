@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_stage_kernel(HopPa
     }
     cp_wait<0>();
   }
-  if (P.red_mask)
+  if (P.red_mask || P.cg)
     block_reduce_finish<3, 2>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,
                               gridDim.x * gridDim.y);
 }

@@ -55,8 +55,20 @@ struct HopLaunch {
   int max_blocks;
   int variant;    // kernel variant (see hop_kernel), chosen by the autotuner
   int block_cap;  // largest block size (128 or 256), chosen by the autotuner
+  // fused CG update on the output (see HopParams::cg)
+  int cg = 0;
+  SpinorPtr cx[2], cr[2], cp[2];
+  const CGState* cst = nullptr;
 };
 cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st);
+
+// the fields of the CG update fused into the last launch of D^dag D
+struct CGFuse {
+  const DevField* x;
+  const DevField* r;
+  const DevField* p;
+  const CGState* st;
+};
 
 // ---- linear algebra on fields ------------------------------------------------
 // v = a*x + b*y for nrhs fields of one parity (scalars uniform)

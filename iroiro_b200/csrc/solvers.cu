@@ -16,6 +16,8 @@ namespace iro {
 namespace host {
 int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in, DevField& out,
           const Reduce* red, int red_mask, const int* skip);
+int apply_cg(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in,
+             DevField& out, const Reduce& red, const int* skip, const CGFuse& fuse);
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
 int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
 int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
@@ -149,11 +151,11 @@ int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* 
   Reduce rbeta = reduce(c, ST_CG_BETA, prm->max_iter);
   auto body = [&](int n) -> int {
     for (int i = 0; i < n; ++i) {
-      // s = D^dag (D p), (p, s) = |D p|^2
+      // (p, A p) = |D p|^2; then D^dag (D p) with x += alpha p, r -= alpha A p
+      // and (r, r) fused into its last launch
       RC(apply(c, op, mass, csw, false, *P, *Q, &ralpha, RED_OUT2, skip));
-      RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
-      CK(launch_cg_xr(PREC_DOUBLE, X->sites(), nrhs, X->all(), R->all(), P->all(), S->all(),
-                      static_cast<const CGState*>(state(c)), rbeta, max_blocks(c), st));
+      RC(apply_cg(c, op, mass, csw, true, *Q, *S, rbeta, skip,
+                  CGFuse{X, R, P, static_cast<const CGState*>(state(c))}));
       CK(launch_cg_p(PREC_DOUBLE, P->sites(), nrhs, P->all(), R->all(),
                      static_cast<const CGState*>(state(c)), done(c), st));
     }
@@ -448,9 +450,8 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   auto body = [&](int n) -> int {
     for (int i = 0; i < n; ++i) {
       RC(apply(c, op, mass, csw, false, *Pl, *Ql, &ralpha, RED_OUT2, skip));
-      RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, skip));
-      CK(launch_cg_xr(pl, Xl->sites(), nrhs, Xl->all(), Rl->all(), Pl->all(), Sl->all(),
-                      static_cast<const CGState*>(state(c)), rbeta, max_blocks(c), st));
+      RC(apply_cg(c, op, mass, csw, true, *Ql, *Sl, rbeta, skip,
+                  CGFuse{Xl, Rl, Pl, static_cast<const CGState*>(state(c))}));
       CK(launch_cg_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(),
                      static_cast<const CGState*>(state(c)), done(c), st));
     }
@@ -538,6 +539,20 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
     bool all_left = true;
     for (int r = 0; r < nrhs; ++r) all_left = all_left && hdone[r] != RUNNING;
     if (all_left) break;
+  }
+  // every right-hand side converged on an FP64 true residual just computed at
+  // its last reliable update (x merged, r = b - A x): that residual is final
+  bool all_conv = true;
+  for (int r = 0; r < nrhs; ++r) all_conv = all_conv && hdone[r] == CONVERGED;
+  if (all_conv) {
+    for (int r = 0; r < nrhs; ++r) {
+      const double bb = hs[r].target / prm->precision;  // target = precision |b|^2
+      out[r].diff = std::sqrt(hs[r].rr / bb);
+      out[r].iterations = hs[r].conv_iter;
+      out[r].reliable_updates = updates[r];
+      out[r].operator_applies = hs[r].iter + 2 * updates[r] + 1;
+    }
+    return IRO_OK;
   }
   // fold any remaining low-precision correction in, then the FP64 true residual
   std::vector<int> ones(nrhs, 1);
