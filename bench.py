@@ -390,6 +390,86 @@ def learned_solves(torch, device, nfields=24, epochs=15, widths=(4, 8, 8, 4), nk
     return out
 
 
+def callers(torch, device):
+    """The callers of the solvers (through the public API, host arrays in the
+    reference's layouts, so host<->device copies are inside the times):
+    Qprop_EvenOdd on the 12 point sources at 32^3x64 as one mixed-precision
+    block against the reference's 12 sequential FP64 inversions; the
+    RationalSolver_CG with 12 poles and the Wilson e/o MD force at 24^3x48."""
+    import iroiro_b200 as ib
+    out = {}
+    Lb = [32, 32, 32, 64]
+    Vb = int(np.prod(Lb))
+    ctx = ib.Context(Lb, device)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    u = ib.synth_gauge(Lb, EPS, SEED + 7, gauge_transform=False)
+    ctx.upload_gauge(u, force=True)
+    D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+    rng = np.random.default_rng(SEED)
+    sp = [int(v) for v in rng.integers(0, 32, 3)] + [int(rng.integers(0, 64))]
+    src = ib.Source_local(sp, Lb)
+    res = {}
+    for name, inner, delta in (("block12_half", "half", 0.03), ("block12_double", "double", 0.1)):
+        qp = ib.Qprop_EvenOdd(D, ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner, delta=delta))
+        qp.calc(src)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        xs = qp.calc(src)
+        torch.cuda.synchronize()
+        res[name] = {"ms": round((time.perf_counter() - t) * 1e3, 1),
+                     "true_residual_max": max(o.diff for o in qp.last_outputs),
+                     "iterations": max(o.Iterations for o in qp.last_outputs)}
+        if name == "block12_half":
+            x_half = xs
+    # the reference's way: one FP64 e/o inversion per source
+    inv = ib.Inverter_WilsonLike(D, ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D)))
+    sol = np.empty(24 * Vb)
+    inv.invert(sol, src.mksrc(0, 0))
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    err = 0.0
+    for k in range(12):
+        inv.invert(sol, src.mksrc(k // 3, k % 3))
+        err = max(err, float(np.linalg.norm(x_half[k] - sol) / np.linalg.norm(sol)))
+    torch.cuda.synchronize()
+    res["sequential12_fp64_ms"] = round((time.perf_counter() - t) * 1e3, 1)
+    res["block12_half_error_vs_fp64"] = err
+    res["speedup_block12_half_vs_sequential_fp64"] = round(res["sequential12_fp64_ms"] /
+                                                           res["block12_half"]["ms"], 2)
+    out["qprop_evenodd_32x32x32x64"] = res
+    ctx.close()
+    # RationalSolver_CG and md_force at 24^3x48
+    ctx = ib.Context(L, device)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    u = ib.synth_gauge(L, EPS, SEED, gauge_transform=True)
+    ctx.upload_gauge(u, force=True)
+    D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+    Vh = int(np.prod(L)) // 2
+    b = ib.synth_gaussian(Vh, SEED + 11)
+    poles = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
+    ra = ib.RationalApprox(0.5, [0.1 / (k + 1) for k in range(12)], poles)
+    rs = ib.RationalSolver_CG(ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 20000), ra)
+    sol = np.empty_like(b)
+    rs.solve(sol, b)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    o = rs.solve(sol, b)
+    torch.cuda.synchronize()
+    out["rational_12poles_24x24x24x48"] = {"ms": round((time.perf_counter() - t) * 1e3, 1),
+                                           "nconv": o.Nconv, "true_residual_max": o.diff}
+    e, z = ib.synth_gaussian(Vh, SEED + 12), ib.synth_gaussian(Vh, SEED + 13)
+    D.md_force(e, z)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(5):
+        D.md_force(e, z)
+    torch.cuda.synchronize()
+    out["md_force_evenodd_24x24x24x48_ms"] = round((time.perf_counter() - t) * 1e3 / 5, 2)
+    out["md_force_note"] = "host arrays: 2 spinors in, the 72*V-double Format_G force out (382 MB)"
+    ctx.close()
+    return out
+
+
 def mixed48(torch, device):
     """Mixed-precision configuration: 48^3x96 even-odd Wilson-clover
     (csw=1.0, kappa=0.124, eps=0.25 field), 12 Gaussian right-hand sides
@@ -588,6 +668,9 @@ def run_ours(args, world, rank, local):
     mixed = {}
     if args.mixed48:
         mixed = mixed48(torch, local)
+    caller_res = {}
+    if not args.no_solve and not args.no_callers:
+        caller_res = callers(torch, local)
 
     lib.iro_field_destroy(fin)
     lib.iro_field_destroy(fout)
@@ -622,6 +705,7 @@ def run_ours(args, world, rank, local):
         "batched": batched,
         "learned": learned_res,
         "mixed48": mixed,
+        "callers": caller_res,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
@@ -671,6 +755,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-callers", action="store_true")
     ap.add_argument("--mixed48", action="store_true",
                     help="also run the 48^3x96 mixed-precision 12-RHS configuration (~1 min)")
     ap.add_argument("--kernel", default=None, help="profiling driver: OP,PREC,NRHS")
