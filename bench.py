@@ -720,9 +720,11 @@ def kernel_only(args):
     import ctypes
     import torch
     import iroiro_b200 as ib
+    Lk = [int(v) for v in args.lattice.split(",")]
+    if args.kernel.startswith("ptc,") or args.kernel == "md_force_eo":
+        return kernel_only_other(args, Lk)
     opn, prec, nrhs = args.kernel.split(",")
     nrhs = int(nrhs)
-    Lk = [int(v) for v in args.lattice.split(",")]
     op = {"wilson_eo": ib.OP_WILSON_SCHUR_EE, "clover_eo": ib.OP_CLOVER_SCHUR_EE,
           "wilson_full": ib.OP_WILSON_FULL}[opn]
     sub = 2 if op == ib.OP_WILSON_FULL else 0
@@ -742,6 +744,40 @@ def kernel_only(args):
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     print(json.dumps({"kernel": args.kernel, "lattice": Lk, "autotune": ctx.autotune_report()}))
+    return 0
+
+
+def kernel_only_other(args, Lk):
+    """Profiling driver for the other kernels: --kernel ptc,4-16-16-16-4 applies
+    that network `steps` times to an FP32 field; --kernel md_force_eo computes
+    one even/odd Wilson MD force; both inside cudaProfilerStart/Stop."""
+    import torch
+    import iroiro_b200 as ib
+    from iroiro_b200 import learned
+    V = int(np.prod(Lk))
+    ctx = ib.Context(Lk, 0)
+    u = ib.synth_gauge(Lk, EPS, SEED, gauge_transform=True)
+    ctx.upload_gauge(u, force=True)
+    if args.kernel.startswith("ptc,"):
+        widths = tuple(int(v) for v in args.kernel.split(",")[1].split("-"))
+        net = learned.PTCNet(ctx, widths, learned.init_weights(widths, 1, 0.3))
+        a = ib.DeviceField(ctx, 2, "single").upload(ib.synth_gaussian(V, SEED + 1))
+        b = ib.DeviceField(ctx, 2, "single")
+        run = lambda: ctx.check(net.L.iro_ptc_apply_field(ctx.h, net.h, a.h, b.h), "apply")
+        reps = args.steps
+    else:
+        D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+        e, z = ib.synth_gaussian(V // 2, SEED + 1), ib.synth_gaussian(V // 2, SEED + 2)
+        run = lambda: D.md_force(e, z)
+        reps = 1
+    run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for _ in range(reps):
+        run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"kernel": args.kernel, "lattice": Lk}))
     return 0
 
 
