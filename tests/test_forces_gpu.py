@@ -33,3 +33,35 @@ def test_md_force_vs_oracle_8x8x8x16(port):
     eh, zh = ib.synth_gaussian(V // 2, 80), ib.synth_gaussian(V // 2, 81)
     Fe = ib.Dirac_Wilson_EvenOdd(m, u, ctx=ctx).md_force(eh, zh)
     assert rel(Fe, port.md_force(L, u, m, True, eh, zh)) < TOL_FP64
+
+
+def test_md_force_is_the_derivative_of_the_operator():
+    """Re Tr(X F_mu(x)) = d/de Re(zeta^dag D(U_mu(x) -> (1 + e X) U_mu(x)) eta)
+    for the full Wilson operator, by central differences on the GPU operator
+    itself (the perturbed links are not SU(3): FP64 full-matrix storage)."""
+    L = [4, 4, 4, 8]
+    V = int(np.prod(L))
+    u = ib.synth_gauge(L, 0.2, 91, gauge_transform=True)
+    m = 0.5 / 0.12 - 4
+    ctx = ib.Context(L, 0)
+    e, z = ib.synth_gaussian(V, 92), ib.synth_gaussian(V, 93)
+    F = ib.Dirac_Wilson(m, u, ctx=ctx).md_force(e, z).reshape(4, V, 3, 3, 2)
+    rng = np.random.default_rng(94)
+    cz = z[0::2] + 1j * z[1::2]
+    for _ in range(3):
+        x, mu = int(rng.integers(V)), int(rng.integers(4))
+        X = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+
+        def f(eps):
+            U = u.reshape(4, V, 3, 3, 2)
+            Uc = (U[..., 0] + 1j * U[..., 1]).copy()
+            Uc[mu, x] = (np.eye(3) + eps * X) @ Uc[mu, x]
+            up = np.stack([Uc.real, Uc.imag], -1).ravel()
+            ctx.upload_gauge(up, force=True)
+            De = ctx.apply(ib.OP_WILSON_FULL, m, 0.0, 0, e)
+            return float(np.vdot(cz, De[0::2] + 1j * De[1::2]).real)
+
+        h = 1e-5
+        fd = (f(h) - f(-h)) / (2 * h)
+        an = float(np.trace(X @ (F[mu, x, ..., 0] + 1j * F[mu, x, ..., 1])).real)
+        assert abs(fd - an) < 1e-6 * max(1.0, abs(an)), (fd, an)
