@@ -244,6 +244,44 @@ def run_reference(args, world, rank):
     return 0
 
 
+def schur_fp64_32(torch, device, steps, peak):
+    """FP64 e/o Wilson Schur operator at 32^3x64, L2 flushed before every
+    application, CUDA events on the launching stream."""
+    import iroiro_b200 as ib
+    Lb = [32, 32, 32, 64]
+    Vh = int(np.prod(Lb)) // 2
+    ctx = ib.Context(Lb, device)
+    st = torch.cuda.current_stream()
+    ctx.set_stream(st.cuda_stream)
+    ctx.upload_gauge(ib.synth_gauge(Lb, EPS, SEED + 5, gauge_transform=True), force=True)
+    a = ib.DeviceField(ctx, 0, "double").upload(ib.synth_gaussian(Vh, SEED + 6))
+    b = ib.DeviceField(ctx, 0, "double")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=torch.device("cuda", device))
+    lib = ctx._lib
+    for _ in range(3):
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, a.h, b.h), "apply")
+    torch.cuda.synchronize()
+    n = max(10, min(steps, 500))
+    tot = 0.0
+    for _ in range(n):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(st)
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, a.h, b.h), "apply")
+        e.record(st)
+        e.synchronize()
+        tot += s.elapsed_time(e)
+    ms = tot / n
+    alg = (2 * BYTES_HOP + BYTES_XPAY) * Vh / (ms * 1e-3) / 1e9
+    traffic = traffic_per_launch(Vh)
+    out = {"ms_per_op": round(ms, 4), "GBps": round(alg, 1), "frac_of_measured_hbm": round(alg / peak, 3)}
+    if traffic:
+        dram = traffic / (ms * 1e-3) / 1e9
+        out.update({"dram_GBps": round(dram, 1), "dram_frac_of_measured_hbm": round(dram / peak, 3)})
+    ctx.close()
+    return out
+
+
 def timed_solves(ctx, D, b, nrhs, torch, inners=("double", "single", "half"), prec=1e-20,
                  delta=0.1):
     """Wall time of iro_cg_solve_field to a 1e-10 FP64 true residual for the
@@ -651,6 +689,10 @@ def run_ours(args, world, rank, local):
                           "frac_of_measured_hbm": round(bps * Vh / (ms * 1e-3) / 1e9 / peak, 3)}
         lib.iro_field_destroy(a)
         lib.iro_field_destroy(b)
+
+    # the FP64 Schur operator on the 32^3x64 lattice of the north-star Dslash
+    # target (same protocol; DRAM bytes per site from the 24^3x48 ncu summary)
+    variants["wilson_fp64_32x32x32x64"] = schur_fp64_32(torch, local, args.steps, peak)
 
     # time to a 1e-10 FP64 true residual, e/o Wilson-clover, FP64 CG vs mixed
     # precision; fields resident on the device (iro_cg_solve_field)

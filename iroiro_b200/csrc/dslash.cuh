@@ -163,9 +163,18 @@ struct HopParams {
 
 // VAR bit 0: at least two 256-thread blocks per SM (register cap 128);
 // VAR bit 1: the four directions as a rolled loop (no hoisting of one
-// direction's loads over another's, fewer live registers).
+// direction's loads over another's, fewer live registers);
+// VAR bit 2 (FP64 only): 128-thread blocks, at least three per SM (register
+// cap 168: between the uncapped 254 and the spilling 128).
+template <int VAR>
+struct HopBounds {
+  static constexpr int threads = (VAR & 4) ? 128 : 256;
+  static constexpr int blocks = (VAR & 4) ? 3 : ((VAR & 1) ? 2 : 1);
+};
+
 template <int SP, int GP, int RECON, bool DAG, int EPI, int CP, int VAR>
-__global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_kernel(HopParams P) {
+__global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::blocks)
+    hop_kernel(HopParams P) {
   using R = typename SpinorIO<SP>::Real;
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;

@@ -33,7 +33,9 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
     P.cr[i] = L.cr[i];
     P.cp[i] = L.cp[i];
   }
-  LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks, L.block_cap);
+  LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks,
+                           L.block_cap < HopBounds<VAR>::threads ? L.block_cap
+                                                                 : HopBounds<VAR>::threads);
   dim3 grid(c.grid, L.nparity);
   hop_kernel<SP, GP, RECON, DAG, EPI, SP, VAR><<<grid, c.block, 0, st>>>(P);
   return cudaGetLastError();
@@ -119,9 +121,10 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
   }
 }
 
-// variant bits 0-1: see hop_kernel; variants 4/5: two right-hand sides per
-// thread (5 with the two-blocks-per-SM register cap); 6/7: the same with the
-// neighbours staged through shared memory
+// variant bits 0-1: see hop_kernel; FP32/FP16: variants 4/5 two right-hand
+// sides per thread (5 with the two-blocks-per-SM register cap), 6/7 the same
+// with the neighbours staged through shared memory; FP64: variants 4/5 the
+// 168-register, 128-thread hop_kernel (5 with the rolled direction loop)
 template <int SP, int GP, int RECON, bool DAG, int EPI>
 static cudaError_t hop_var(const HopLaunch& L, cudaStream_t st) {
   switch (L.variant & 7) {
@@ -129,10 +132,18 @@ static cudaError_t hop_var(const HopLaunch& L, cudaStream_t st) {
     case 1: return hop_go<SP, GP, RECON, DAG, EPI, 1>(L, st);
     case 2: return hop_go<SP, GP, RECON, DAG, EPI, 2>(L, st);
     case 3: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
-    case 4: return hop_go_pair<SP, RECON, DAG, EPI, 0>(L, st);
-    case 5: return hop_go_pair<SP, RECON, DAG, EPI, 1>(L, st);
-    case 6: return hop_go_stage<SP, RECON, DAG, EPI, 0>(L, st);
-    default: return hop_go_stage<SP, RECON, DAG, EPI, 1>(L, st);
+    case 4:
+      if constexpr (SP == PREC_DOUBLE) return hop_go<SP, GP, RECON, DAG, EPI, 4>(L, st);
+      else return hop_go_pair<SP, RECON, DAG, EPI, 0>(L, st);
+    case 5:
+      if constexpr (SP == PREC_DOUBLE) return hop_go<SP, GP, RECON, DAG, EPI, 6>(L, st);
+      else return hop_go_pair<SP, RECON, DAG, EPI, 1>(L, st);
+    case 6:
+      if constexpr (SP == PREC_DOUBLE) return cudaErrorInvalidValue;
+      else return hop_go_stage<SP, RECON, DAG, EPI, 0>(L, st);
+    default:
+      if constexpr (SP == PREC_DOUBLE) return cudaErrorInvalidValue;
+      else return hop_go_stage<SP, RECON, DAG, EPI, 1>(L, st);
   }
 }
 
