@@ -246,7 +246,8 @@ def run_reference(args, world, rank):
 
 def schur_fp64_32(torch, device, steps, peak):
     """FP64 e/o Wilson Schur operator at 32^3x64, L2 flushed before every
-    application, CUDA events on the launching stream."""
+    application, CUDA events on the launching stream; DRAM bytes per site
+    from the ncu summary of this lattice."""
     import iroiro_b200 as ib
     Lb = [32, 32, 32, 64]
     Vh = int(np.prod(Lb)) // 2
@@ -273,7 +274,11 @@ def schur_fp64_32(torch, device, steps, peak):
         tot += s.elapsed_time(e)
     ms = tot / n
     alg = (2 * BYTES_HOP + BYTES_XPAY) * Vh / (ms * 1e-3) / 1e9
-    traffic = traffic_per_launch(Vh)
+    traffic = None
+    p = ROOT / "profiles" / "hop_fp64_32x32x32x64_dram.txt"
+    if p.exists():
+        m = re.search(r"^dram_bytes_per_site_schur_32x32x32x64:\s*([0-9.]+)", p.read_text(), re.M)
+        traffic = float(m.group(1)) * Vh if m else None
     out = {"ms_per_op": round(ms, 4), "GBps": round(alg, 1), "frac_of_measured_hbm": round(alg / peak, 3)}
     if traffic:
         dram = traffic / (ms * 1e-3) / 1e9
@@ -690,8 +695,7 @@ def run_ours(args, world, rank, local):
         lib.iro_field_destroy(a)
         lib.iro_field_destroy(b)
 
-    # the FP64 Schur operator on the 32^3x64 lattice of the north-star Dslash
-    # target (same protocol; DRAM bytes per site from the 24^3x48 ncu summary)
+    # the FP64 Schur operator on the 32^3x64 lattice (same protocol)
     variants["wilson_fp64_32x32x32x64"] = schur_fp64_32(torch, local, args.steps, peak)
 
     # time to a 1e-10 FP64 true residual, e/o Wilson-clover, FP64 CG vs mixed
