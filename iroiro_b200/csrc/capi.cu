@@ -242,8 +242,8 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
   // two right-hand sides per thread (variant bit 2) needs FP32/FP16 storage,
   // reconstruct-12 links and an even number of right-hand sides
   const bool pair_ok = L.prec != PREC_DOUBLE && L.recon == 12 && L.nrhs % 2 == 0;
-  // FP64: variants 4, 5 (168-register hop kernel); FP32/FP16: 4..7 when pairs apply
-  const int nvar = L.prec == PREC_DOUBLE ? 6 : (pair_ok ? 8 : 4);
+  // FP64: variants 4, 5 (168-register hop kernel); FP32/FP16: 4..9 when pairs apply
+  const int nvar = L.prec == PREC_DOUBLE ? 6 : (pair_ok ? 10 : 4);
   if (forced) {
     int v = 0, b = 256;
     std::sscanf(forced, "%d,%d", &v, &b);

@@ -121,29 +121,35 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
   }
 }
 
-// variant bits 0-1: see hop_kernel; FP32/FP16: variants 4/5 two right-hand
-// sides per thread (5 with the two-blocks-per-SM register cap), 6/7 the same
-// with the neighbours staged through shared memory; FP64: variants 4/5 the
-// 168-register, 128-thread hop_kernel (5 with the rolled direction loop)
+// Variants 0-3: hop_kernel (bits: see there).  FP32/FP16 with even nrhs:
+// 4-7 two right-hand sides per thread with the register cap none / 128 /
+// 152 / 168, 8-9 the same with the neighbours staged through shared memory.
+// FP64: 4/5 the 168-register 128-thread hop_kernel (5 with the rolled loop).
 template <int SP, int GP, int RECON, bool DAG, int EPI>
 static cudaError_t hop_var(const HopLaunch& L, cudaStream_t st) {
-  switch (L.variant & 7) {
+  switch (L.variant) {
     case 0: return hop_go<SP, GP, RECON, DAG, EPI, 0>(L, st);
     case 1: return hop_go<SP, GP, RECON, DAG, EPI, 1>(L, st);
     case 2: return hop_go<SP, GP, RECON, DAG, EPI, 2>(L, st);
     case 3: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
-    case 4:
-      if constexpr (SP == PREC_DOUBLE) return hop_go<SP, GP, RECON, DAG, EPI, 4>(L, st);
-      else return hop_go_pair<SP, RECON, DAG, EPI, 0>(L, st);
-    case 5:
-      if constexpr (SP == PREC_DOUBLE) return hop_go<SP, GP, RECON, DAG, EPI, 6>(L, st);
-      else return hop_go_pair<SP, RECON, DAG, EPI, 1>(L, st);
-    case 6:
-      if constexpr (SP == PREC_DOUBLE) return cudaErrorInvalidValue;
-      else return hop_go_stage<SP, RECON, DAG, EPI, 0>(L, st);
-    default:
-      if constexpr (SP == PREC_DOUBLE) return cudaErrorInvalidValue;
-      else return hop_go_stage<SP, RECON, DAG, EPI, 1>(L, st);
+    default: break;
+  }
+  if constexpr (SP == PREC_DOUBLE) {
+    switch (L.variant) {
+      case 4: return hop_go<SP, GP, RECON, DAG, EPI, 4>(L, st);
+      case 5: return hop_go<SP, GP, RECON, DAG, EPI, 6>(L, st);
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    switch (L.variant) {
+      case 4: return hop_go_pair<SP, RECON, DAG, EPI, 0>(L, st);
+      case 5: return hop_go_pair<SP, RECON, DAG, EPI, 1>(L, st);
+      case 6: return hop_go_pair<SP, RECON, DAG, EPI, 2>(L, st);
+      case 7: return hop_go_pair<SP, RECON, DAG, EPI, 3>(L, st);
+      case 8: return hop_go_stage<SP, RECON, DAG, EPI, 0>(L, st);
+      case 9: return hop_go_stage<SP, RECON, DAG, EPI, 1>(L, st);
+      default: return cudaErrorInvalidValue;
+    }
   }
 }
 

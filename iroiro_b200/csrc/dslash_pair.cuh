@@ -460,8 +460,15 @@ __device__ __forceinline__ void pair_epilogue(const HopParams& P, int yi, int hs
 // flagged converged; a pair with one converged member still writes it (its
 // outputs are scratch, and the solvers' stage updates ignore its sums).
 // Per-site sums of the reductions are formed in FP32 and accumulated in FP64.
+// VAR selects the register cap: none, 128, 152 or 168 registers per thread
+// (the autotuner trades ILP against resident warps).
+template <int VAR>
+struct PairCap {
+  static constexpr int regs = VAR == 1 ? 128 : (VAR == 2 ? 152 : (VAR == 3 ? 168 : 255));
+};
+
 template <int SP, bool DAG, int EPI, int VAR>
-__global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_pair_kernel(HopParams P) {
+__global__ void __launch_bounds__(256) __maxnreg__(PairCap<VAR>::regs) hop_pair_kernel(HopParams P) {
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;
   const int nrhs = P.nrhs;
@@ -481,22 +488,10 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_pair_kernel(HopPar
     Cp acc[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = {bc(0.f), bc(0.f)};
-    if (VAR & 2) {
-#pragma unroll 1
-      for (int mu = 0; mu < 4; ++mu) {
-        switch (mu) {
-          case 0: hop_dir_pair<0, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
-          case 1: hop_dir_pair<1, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
-          case 2: hop_dir_pair<2, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
-          default: hop_dir_pair<3, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc); break;
-        }
-      }
-    } else {
-      hop_dir_pair<0, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
-      hop_dir_pair<1, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
-      hop_dir_pair<2, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
-      hop_dir_pair<3, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
-    }
+    hop_dir_pair<0, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+    hop_dir_pair<1, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+    hop_dir_pair<2, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
+    hop_dir_pair<3, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
     pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, acc, red);
   }
   if (P.red_mask || P.cg)

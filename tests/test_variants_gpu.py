@@ -2,8 +2,9 @@
 (IRO_HOP_VARIANT, read once per process, so each variant runs in its own
 subprocess): 12-RHS FP32/FP16 operators against the FP64 single-RHS operator,
 and a 12-RHS mixed-precision CG whose fused reductions drive the solve.
-Variants 4-5 are the two-right-hand-sides-per-thread kernel, 6-7 the same
-with its neighbours staged through shared memory."""
+Variants 4-7 are the two-right-hand-sides-per-thread kernel with four
+register caps, 8-9 the same with its neighbours staged through shared memory;
+for FP64 the forced number is taken modulo its 6 variants."""
 import json
 import os
 import subprocess
@@ -60,7 +61,7 @@ print("RESULT " + json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("variant", ["0,256", "4,256", "5,128", "6,128", "6,256", "7,128"])
+@pytest.mark.parametrize("variant", ["0,256", "4,256", "5,128", "6,128", "7,256", "8,128", "9,256"])
 def test_forced_variant(variant):
     env = dict(os.environ, IRO_HOP_VARIANT=variant)
     r = subprocess.run([sys.executable, "-c", SCRIPT, str(ROOT)], env=env, capture_output=True,
@@ -69,9 +70,12 @@ def test_forced_variant(variant):
     line = [l for l in r.stdout.splitlines() if l.startswith("RESULT ")][-1]
     res = json.loads(line[len("RESULT "):])
     v = int(variant.split(",")[0])
+    fp64_v = v % 6
     # the forced variant ran (pair variants only where the shape allows them)
     for t in res["autotune"]:
-        if t["prec"] != 0 and t["nrhs"] % 2 == 0:
+        if t["prec"] == 0:
+            assert t["variant"] == fp64_v, t
+        elif t["nrhs"] % 2 == 0:
             assert t["variant"] == v, t
     for key, err in res["ops"].items():
         tol = TOL_FP32 if key.endswith("single") else TOL_FP16
