@@ -144,6 +144,7 @@ int ensure_stage(iro_ctx* c, size_t bytes) {
 Reduce make_reduce(iro_ctx* c, int stage, int max_iter) {
   Reduce r;
   r.partials = c->partials;
+  r.gpartials = c->partials + kPartialsPerBlock * size_t(c->max_blocks) * 2;
   r.counter = c->counter;
   r.out = c->redout;
   r.stage = stage;
@@ -234,6 +235,18 @@ HopLaunch base_launch(iro_ctx* c, int prec, bool dag, int nrhs) {
 // launch is idempotent) before the real launch; during stream capture the
 // default configuration is used.  IRO_HOP_VARIANT="<variant>,<block>" fixes
 // the choice.
+// FP64 variants 6..11 are variants 0..5 on the stored 18-real links of an
+// SU(3) gauge field (no third-row reconstruction: fewer FP64 operations,
+// more link bytes).
+static cudaError_t launch_variant(iro_ctx* c, HopLaunch L, cudaStream_t st) {
+  if (L.prec == PREC_DOUBLE && L.variant >= 6) {
+    L.variant -= 6;
+    L.recon = 18;
+    L.gauge.a = c->ga.d18;
+  }
+  return launch_hop(L, st);
+}
+
 int launch_tuned(iro_ctx* c, HopLaunch L) {
   auto key = std::make_tuple(L.prec, L.recon, int(L.dag), L.epi, L.nrhs, L.nparity);
   cudaStream_t st = c->stream;
@@ -242,8 +255,9 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
   // two right-hand sides per thread (variant bit 2) needs FP32/FP16 storage,
   // reconstruct-12 links and an even number of right-hand sides
   const bool pair_ok = L.prec != PREC_DOUBLE && L.recon == 12 && L.nrhs % 2 == 0;
-  // FP64: variants 4, 5 (168-register hop kernel); FP32/FP16: 4..9 when pairs apply
-  const int nvar = L.prec == PREC_DOUBLE ? 6 : (pair_ok ? 10 : 4);
+  // FP64: variants 4, 5 (168-register hop kernel), 6..11 on 18-real links of
+  // an SU(3) field; FP32/FP16: 4..9 when pairs apply
+  const int nvar = L.prec == PREC_DOUBLE ? (L.recon == 12 ? 12 : 6) : (pair_ok ? 10 : 4);
   if (forced) {
     int v = 0, b = 256;
     std::sscanf(forced, "%d,%d", &v, &b);
@@ -271,9 +285,9 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
       for (int b : {256, 128}) {
         T.variant = v;
         T.block_cap = b;
-        CK(launch_hop(T, st));  // warm-up
+        CK(launch_variant(c, T, st));  // warm-up
         CK(cudaEventRecord(e0, st));
-        for (int i = 0; i < 3; ++i) CK(launch_hop(T, st));
+        for (int i = 0; i < 3; ++i) CK(launch_variant(c, T, st));
         CK(cudaEventRecord(e1, st));
         CK(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -291,7 +305,7 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
   }
   L.variant = it->second.first;
   L.block_cap = it->second.second;
-  CK(launch_hop(L, st));
+  CK(launch_variant(c, L, st));
   return IRO_OK;
 }
 
@@ -374,9 +388,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       if (fuse) {
         L2.cg = 1;
         L2.cst = fuse->st;
-        L2.cx[0] = fuse->x->half(0);
         L2.cr[0] = fuse->r->half(0);
-        L2.cp[0] = fuse->p->half(0);
       }
       { int rt = launch_tuned(c, L2); if (rt) return rt; }
     } break;
@@ -397,11 +409,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       if (fuse) {
         L.cg = 1;
         L.cst = fuse->st;
-        for (int y = 0; y < 2; ++y) {
-          L.cx[y] = fuse->x->half(y);
-          L.cr[y] = fuse->r->half(y);
-          L.cp[y] = fuse->p->half(y);
-        }
+        for (int y = 0; y < 2; ++y) L.cr[y] = fuse->r->half(y);
       }
       { int rt = launch_tuned(c, L); if (rt) return rt; }
     } break;
@@ -539,9 +547,11 @@ int iro_ctx_create(const int L[4], int device, iro_ctx** out) {
     c->max_blocks = c->sms * 8;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->own_stream = true;
-    CK(cudaMalloc(&c->partials, sizeof(double) * kPartialsPerBlock * c->max_blocks * 2));
-    CK(cudaMalloc(&c->counter, sizeof(unsigned)));
-    CK(cudaMemset(c->counter, 0, sizeof(unsigned)));
+    // block partials of up to 2 * max_blocks blocks, then their group partials
+    const size_t groups = size_t(2 * c->max_blocks + kReduceGroup - 1) / kReduceGroup;
+    CK(cudaMalloc(&c->partials, sizeof(double) * kPartialsPerBlock * (2 * c->max_blocks + groups)));
+    CK(cudaMalloc(&c->counter, sizeof(unsigned) * (1 + groups)));
+    CK(cudaMemset(c->counter, 0, sizeof(unsigned) * (1 + groups)));
     CK(cudaMalloc(&c->redout, sizeof(double) * kPartialsPerBlock));
     CK(cudaMalloc(&c->state, sizeof(MSState) > sizeof(CGState) * kMaxRhs ? sizeof(MSState) : sizeof(CGState) * kMaxRhs));
     CK(cudaMalloc(&c->done, sizeof(int) * 64));

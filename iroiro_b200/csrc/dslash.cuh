@@ -153,11 +153,12 @@ struct HopParams {
   int red_mask;
   Reduce red;
   const int* skip;  // per-rhs converged flags, or null
-  // fused CG update (Solver_CG::solve_step's x/r update, solver_CG.cpp:120-140)
-  // on the operator's output s: r -= alpha s, x += alpha p, red[0] = |r|^2;
-  // s itself is not stored.  Off when cg == 0.
+  // fused CG update (Solver_CG::solve_step's r update, solver_CG.cpp:120-140)
+  // on the operator's output s: r -= alpha s, red[0] = |r|^2; s itself is
+  // not stored.  x += alpha p is left to the p update (cg_p_kernel), which
+  // reads p anyway.  Off when cg == 0.
   int cg;
-  SpinorPtr cx[2], cr[2], cp[2];  // indexed like out[]
+  SpinorPtr cr[2];  // indexed like out[]
   const CGState* cst;
 };
 
@@ -232,21 +233,17 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
       for (int k = 0; k < 12; ++k) acc[k] = ax[k] + acc[k];
     }
     if (P.cg) {
-      // r -= alpha s; x += alpha p; |r|^2 (the solver's ST_CG_BETA totals)
+      // r -= alpha s; |r|^2 (the solver's ST_CG_BETA totals)
       const R a = R(P.cst[r].alpha);
-      Cx<R> rv[12], pv[12], xv2[12];
+      Cx<R> rv[12];
       SpinorIO<SP>::load(P.cr[yi], tid, rv);
-      SpinorIO<SP>::load(P.cp[yi], tid, pv);
-      SpinorIO<SP>::load(P.cx[yi], tid, xv2);
       double rr = 0.0;
 #pragma unroll
       for (int k = 0; k < 12; ++k) {
         rv[k] = rv[k] - a * acc[k];
-        xv2[k] = xv2[k] + a * pv[k];
         rr += double(rv[k].re) * rv[k].re + double(rv[k].im) * rv[k].im;
       }
       SpinorIO<SP>::store(P.cr[yi], tid, rv);
-      SpinorIO<SP>::store(P.cx[yi], tid, xv2);
       red[0] += rr;
       continue;
     }

@@ -29,9 +29,7 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   P.cg = L.cg;
   P.cst = L.cst;
   for (int i = 0; i < 2; ++i) {
-    P.cx[i] = L.cx[i];
     P.cr[i] = L.cr[i];
-    P.cp[i] = L.cp[i];
   }
   LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks,
                            L.block_cap < HopBounds<VAR>::threads ? L.block_cap
@@ -66,9 +64,7 @@ static cudaError_t hop_go_pair(const HopLaunch& L, cudaStream_t st) {
     P.cg = L.cg;
     P.cst = L.cst;
     for (int i = 0; i < 2; ++i) {
-      P.cx[i] = L.cx[i];
       P.cr[i] = L.cr[i];
-      P.cp[i] = L.cp[i];
     }
     LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
     dim3 grid(c.grid, L.nparity);
@@ -102,9 +98,7 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
     P.cg = L.cg;
     P.cst = L.cst;
     for (int i = 0; i < 2; ++i) {
-      P.cx[i] = L.cx[i];
       P.cr[i] = L.cr[i];
-      P.cp[i] = L.cp[i];
     }
     LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
     const int smem = stage_bytes<SP>() * c.block;

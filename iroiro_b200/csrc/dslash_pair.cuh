@@ -370,7 +370,7 @@ __device__ __forceinline__ void hop_dir_pair(const GaugePtr& gauge, const Spinor
 // per-site FP32 sums of the reductions added to red[] in FP64.
 template <int SP, int EPI>
 __device__ __forceinline__ void pair_epilogue(const HopParams& P, int yi, int hs, int64_t e0,
-                                              Cp acc[12], double red[6]) {
+                                              int r0, Cp acc[12], double red[6]) {
   const float2 sc = bc(float(P.scale));
   Cp xv[12];
   if (EPI == EPI_SCALE || EPI == EPI_SCALE_CLOV) {
@@ -408,26 +408,20 @@ __device__ __forceinline__ void pair_epilogue(const HopParams& P, int yi, int hs
       acc[k] = {pfma(sc, acc[k].re, ax[k].re), pfma(sc, acc[k].im, ax[k].im)};
   }
   if (P.cg) {
-    // r -= alpha s; x += alpha p; |r|^2.  A lane whose right-hand side has left
-    // the iteration gets alpha = 0 (its values are re-stored unchanged).
-    const int r0 = int(e0 % P.nrhs);
-    const float2 a = make_float2(P.skip && P.skip[r0] ? 0.f : float(P.cst[r0].alpha),
-                                 P.skip && P.skip[r0 + 1] ? 0.f : float(P.cst[r0 + 1].alpha));
-    Cp rv[12], pv[12], xw[12];
+    // r -= alpha s; |r|^2.  A lane whose right-hand side has left the
+    // iteration gets alpha = 0 (its residual is re-stored unchanged).
+    const float2 na = make_float2(P.skip && P.skip[r0] ? 0.f : -float(P.cst[r0].alpha),
+                                  P.skip && P.skip[r0 + 1] ? 0.f : -float(P.cst[r0 + 1].alpha));
+    Cp rv[12];
     PairIO<SP>::load_scaled(P.cr[yi], e0, rv);
-    PairIO<SP>::load_scaled(P.cp[yi], e0, pv);
-    PairIO<SP>::load_scaled(P.cx[yi], e0, xw);
     float2 rr = bc(0.f);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
-      const float2 na = pmul(a, bc(-1.f));
       rv[k] = {pfma(na, acc[k].re, rv[k].re), pfma(na, acc[k].im, rv[k].im)};
-      xw[k] = {pfma(a, pv[k].re, xw[k].re), pfma(a, pv[k].im, xw[k].im)};
       rr = pfma(rv[k].re, rv[k].re, rr);
       rr = pfma(rv[k].im, rv[k].im, rr);
     }
     PairIO<SP>::store(P.cr[yi], e0, rv);
-    PairIO<SP>::store(P.cx[yi], e0, xw);
     red[0] += rr.x;
     red[3] += rr.y;
     return;
@@ -492,7 +486,7 @@ __global__ void __launch_bounds__(256) __maxnreg__(PairCap<VAR>::regs) hop_pair_
     hop_dir_pair<1, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
     hop_dir_pair<2, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
     hop_dir_pair<3, DAG, SP>(P.gauge, P.in[yi], p, hs, nb, nrhs, r0, acc);
-    pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, acc, red);
+    pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, r0, acc, red);
   }
   if (P.red_mask || P.cg)
     block_reduce_finish<3, 2>(P.red, red, nrhs, blockIdx.y * gridDim.x + blockIdx.x,

@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(256, (VAR & 1) ? 2 : 1) hop_stage_kernel(HopPa
       stage_step<SP, 5, DAG>(P, yi, p, hs, nb, nhs, has_next, r0, base, sm, acc);
       stage_step<SP, 6, DAG>(P, yi, p, hs, nb, nhs, has_next, r0, base, sm, acc);
       stage_step<SP, 7, DAG>(P, yi, p, hs, nb, nhs, has_next, r0, base, sm, acc);
-      pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, acc, red);
+      pair_epilogue<SP, EPI>(P, yi, hs, int64_t(hs) * nrhs + r0, r0, acc, red);
       if (!has_next) break;
       tid = ntid;
       hs = nhs;

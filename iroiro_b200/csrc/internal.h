@@ -57,16 +57,14 @@ struct HopLaunch {
   int block_cap;  // largest block size (128 or 256), chosen by the autotuner
   // fused CG update on the output (see HopParams::cg)
   int cg = 0;
-  SpinorPtr cx[2], cr[2], cp[2];
+  SpinorPtr cr[2];
   const CGState* cst = nullptr;
 };
 cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st);
 
-// the fields of the CG update fused into the last launch of D^dag D
+// the residual updated by the CG step fused into the last launch of D^dag D
 struct CGFuse {
-  const DevField* x;
   const DevField* r;
-  const DevField* p;
   const CGState* st;
 };
 
@@ -91,7 +89,7 @@ cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr 
                          SpinorPtr s, const CGState* state, const Reduce& red, int max_blocks,
                          cudaStream_t st);
 // CG: p = beta p + r
-cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r,
+cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r, SpinorPtr x,
                         const CGState* state, const int* done, cudaStream_t st);
 
 // Multishift (FP64): x0 -= beta p0; r += beta (s + sigma0 p0); reduce |r|^2

@@ -61,6 +61,16 @@ cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st) {
 }
 
 // ---- linear algebra ------------------------------------------------------------
+// Streaming kernels without per-thread scalars launch one thread per element,
+// so that each thread issues all its loads at once and the whole grid keeps
+// HBM busy; those that first read per-right-hand-side scalars from memory use
+// a grid-stride loop over kScalarStreamGrid blocks instead.
+constexpr int kScalarStreamGrid = 148 * 16;
+static int stream_grid(int64_t n, int blk) {
+  const int64_t g = (n + blk - 1) / blk;
+  return int(g < 1 ? 1 : g);
+}
+
 template <typename RA, typename RB>
 __device__ __forceinline__ void cvt12(const Cx<RA> a[12], Cx<RB> b[12]) {
 #pragma unroll
@@ -138,8 +148,7 @@ cudaError_t launch_axpby(int prec, int64_t Vh, int nrhs, double a, SpinorPtr x, 
                          SpinorPtr y, SpinorPtr v, cudaStream_t st) {
   const int64_t n = Vh * nrhs;
   const int blk = 256;
-  int grid = int((n + blk - 1) / blk);
-  if (grid > 148 * 16) grid = 148 * 16;
+  const int grid = stream_grid(n, blk);
   switch (prec) {
     case PREC_DOUBLE: axpby_kernel<PREC_DOUBLE><<<grid, blk, 0, st>>>(n, a, x, b, y, v); break;
     case PREC_SINGLE: axpby_kernel<PREC_SINGLE><<<grid, blk, 0, st>>>(n, a, x, b, y, v); break;
@@ -166,8 +175,7 @@ cudaError_t launch_convert(int pin, SpinorPtr in, int pout, SpinorPtr out, int64
                            cudaStream_t st) {
   const int64_t n = Vh * nrhs;
   const int blk = 256;
-  int grid = int((n + blk - 1) / blk);
-  if (grid > 148 * 16) grid = 148 * 16;
+  const int grid = stream_grid(n, blk);
 #define IRO_CVT(A, B) \
   if (pin == A && pout == B) { convert_kernel<A, B><<<grid, blk, 0, st>>>(n, in, out); return cudaGetLastError(); }
   IRO_CVT(PREC_DOUBLE, PREC_DOUBLE)
@@ -296,36 +304,63 @@ cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr 
   return cudaGetLastError();
 }
 
-// p = p*(rr/rrp) + r (solver_CG.cpp:150-153)
+// x += alpha p (solver_CG.cpp:131-136, deferred from the fused r update)
+// and p = p*(rr/rrp) + r (solver_CG.cpp:150-153).  The x update runs for
+// every right-hand side whose iteration just completed (CGState::xpend), also
+// when it has just converged or paused; the p update only for those still
+// iterating.  The block is a multiple of nrhs, so a thread keeps one
+// right-hand side across the grid-stride loop, and loads its right-hand
+// side's scalars once (a grid of a few blocks per SM: with one element per
+// thread, the scalar loads ahead of the data would halve the bytes in
+// flight).  Each element in two phases -- p and x, then r -- so that at most
+// two spinors are live: 4 resident blocks per SM for FP32/FP16 storage, 2 for
+// FP64.
 template <int SP>
-__global__ void cg_p_kernel(int64_t vh, int nrhs, SpinorPtr p, SpinorPtr r, const CGState* state,
-                            const int* done) {
+struct CgpBounds {
+  static constexpr int blocks = SP == PREC_DOUBLE ? 2 : 4;
+};
+
+template <int SP>
+__global__ void __launch_bounds__(256, CgpBounds<SP>::blocks) cg_p_kernel(int64_t n, int nrhs, SpinorPtr p, SpinorPtr r,
+                                                   SpinorPtr x, const CGState* state,
+                                                   const int* done) {
   using R = typename SpinorIO<SP>::Real;
-  const int64_t n = vh * nrhs;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    const int rhs = int(i % nrhs);
-    if (done[rhs]) continue;
-    const double b = state[rhs].beta;
-    Cx<R> pv[12], rv[12];
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = i0 % nrhs;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  const bool upd_x = state[rhs].xpend != 0;
+  const bool upd_p = done[rhs] == RUNNING;
+  if (!upd_x && !upd_p) return;
+  const R a = R(state[rhs].alpha);
+  const R b = R(state[rhs].beta);
+  for (int64_t i = i0; i < n; i += stride) {
+    Cx<R> pv[12];
     SpinorIO<SP>::load(p, i, pv);
-    SpinorIO<SP>::load(r, i, rv);
+    if (upd_x) {
+      Cx<R> xv[12];
+      SpinorIO<SP>::load(x, i, xv);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) pv[k] = R(b) * pv[k] + rv[k];
-    SpinorIO<SP>::store(p, i, pv);
+      for (int k = 0; k < 12; ++k) xv[k] = xv[k] + a * pv[k];
+      SpinorIO<SP>::store(x, i, xv);
+    }
+    if (upd_p) {
+      Cx<R> rv[12];
+      SpinorIO<SP>::load(r, i, rv);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) pv[k] = b * pv[k] + rv[k];
+      SpinorIO<SP>::store(p, i, pv);
+    }
   }
 }
 
-cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r,
+cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r, SpinorPtr x,
                         const CGState* state, const int* done, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, nrhs, kScalarStreamGrid);
   const int64_t n = Vh * nrhs;
-  const int blk = 256;
-  int grid = int((n + blk - 1) / blk);
-  if (grid > 148 * 16) grid = 148 * 16;
   switch (prec) {
-    case PREC_DOUBLE: cg_p_kernel<PREC_DOUBLE><<<grid, blk, 0, st>>>(Vh, nrhs, p, r, state, done); break;
-    case PREC_SINGLE: cg_p_kernel<PREC_SINGLE><<<grid, blk, 0, st>>>(Vh, nrhs, p, r, state, done); break;
-    default: cg_p_kernel<PREC_HALF><<<grid, blk, 0, st>>>(Vh, nrhs, p, r, state, done); break;
+    case PREC_DOUBLE: cg_p_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(n, nrhs, p, r, x, state, done); break;
+    case PREC_SINGLE: cg_p_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(n, nrhs, p, r, x, state, done); break;
+    default: cg_p_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(n, nrhs, p, r, x, state, done); break;
   }
   return cudaGetLastError();
 }
@@ -839,13 +874,15 @@ void clover_init_tables() {
 namespace iro {
 
 // ---- mixed-precision reliable updates -------------------------------------------------
+// The blocks are multiples of nrhs (launch_cfg), so a thread keeps one
+// right-hand side across its grid-stride loop.
 // x64 += xlo; xlo = 0   for right-hand sides with mask[r] != 0
 template <int PL>
 __global__ void mx_merge_kernel(int64_t n, int nrhs, SpinorPtr x64, SpinorPtr xlo, const int* mask) {
   using RL = typename SpinorIO<PL>::Real;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    if (!mask[i % nrhs]) continue;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!mask[i0 % nrhs]) return;
+  for (int64_t i = i0; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     Cx<double> a[12];
     Cx<RL> l[12];
     SpinorIO<PREC_DOUBLE>::load(x64, i, a);
@@ -866,9 +903,9 @@ __global__ void __launch_bounds__(256) mx_residual_kernel(int64_t n, int nrhs, S
                                    SpinorPtr rlo, const int* mask, Reduce red) {
   using RL = typename SpinorIO<PL>::Real;
   double acc = 0.0;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    if (!mask[i % nrhs]) continue;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool on = mask[i0 % nrhs] != 0;
+  for (int64_t i = i0; on && i < n; i += int64_t(gridDim.x) * blockDim.x) {
     Cx<double> bv[12], sv[12];
     Cx<RL> l[12];
     SpinorIO<PREC_DOUBLE>::load(b, i, bv);
@@ -890,11 +927,11 @@ template <int PL>
 __global__ void mx_p_kernel(int64_t n, int nrhs, SpinorPtr p, SpinorPtr r, const CGState* state,
                             const int* mask) {
   using RL = typename SpinorIO<PL>::Real;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    const int rhs = int(i % nrhs);
-    if (!mask[rhs]) continue;
-    const RL beta = RL(state[rhs].beta);
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = i0 % nrhs;
+  if (!mask[rhs]) return;
+  const RL beta = RL(state[rhs].beta);
+  for (int64_t i = i0; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     Cx<RL> pv[12], rv[12];
     SpinorIO<PL>::load(p, i, pv);
     SpinorIO<PL>::load(r, i, rv);
@@ -907,10 +944,10 @@ __global__ void mx_p_kernel(int64_t n, int nrhs, SpinorPtr p, SpinorPtr r, const
 cudaError_t launch_mx_merge(int plo, int64_t sites, int nrhs, SpinorPtr x64, SpinorPtr xlo,
                             const int* mask, cudaStream_t st) {
   const int64_t n = sites * nrhs;
-  const int grid = grid_for(n, 256);
-  if (plo == PREC_SINGLE) mx_merge_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(n, nrhs, x64, xlo, mask);
-  else if (plo == PREC_HALF) mx_merge_kernel<PREC_HALF><<<grid, 256, 0, st>>>(n, nrhs, x64, xlo, mask);
-  else mx_merge_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(n, nrhs, x64, xlo, mask);
+  LaunchCfg c = launch_cfg(sites, nrhs, kScalarStreamGrid);
+  if (plo == PREC_SINGLE) mx_merge_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(n, nrhs, x64, xlo, mask);
+  else if (plo == PREC_HALF) mx_merge_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(n, nrhs, x64, xlo, mask);
+  else mx_merge_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(n, nrhs, x64, xlo, mask);
   return cudaGetLastError();
 }
 
@@ -928,10 +965,10 @@ cudaError_t launch_mx_residual(int plo, int64_t sites, int nrhs, SpinorPtr b, Sp
 cudaError_t launch_mx_p(int plo, int64_t sites, int nrhs, SpinorPtr p, SpinorPtr r,
                         const CGState* state, const int* mask, cudaStream_t st) {
   const int64_t n = sites * nrhs;
-  const int grid = grid_for(n, 256);
-  if (plo == PREC_SINGLE) mx_p_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(n, nrhs, p, r, state, mask);
-  else if (plo == PREC_HALF) mx_p_kernel<PREC_HALF><<<grid, 256, 0, st>>>(n, nrhs, p, r, state, mask);
-  else mx_p_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(n, nrhs, p, r, state, mask);
+  LaunchCfg c = launch_cfg(sites, nrhs, kScalarStreamGrid);
+  if (plo == PREC_SINGLE) mx_p_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(n, nrhs, p, r, state, mask);
+  else if (plo == PREC_HALF) mx_p_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(n, nrhs, p, r, state, mask);
+  else mx_p_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(n, nrhs, p, r, state, mask);
   return cudaGetLastError();
 }
 

@@ -3,10 +3,12 @@
 //
 // A kernel that reduces hands its per-thread partial sums to
 // block_reduce_finish(): a fixed-order tree inside the block, one partial per
-// block in global scratch, and the last block to arrive (ticket counter)
-// sums the partials in block order -- deterministic run to run -- and then
-// applies the solver stage's scalar update (alpha, beta, convergence flags,
-// multishift zeta recurrences).
+// block in global scratch; the last block to arrive in each group of 32
+// consecutive blocks sums that group's partials in block order, and the last
+// group to finish sums the group partials in group order (ticket counters,
+// so the result is deterministic run to run) and then applies the solver
+// stage's scalar update (alpha, beta, convergence flags, multishift zeta
+// recurrences).
 #pragma once
 
 #include "common.cuh"
@@ -25,6 +27,7 @@ struct CGState {
   double delta2;   // reliable-update trigger delta^2; 0 for plain CG
   int iter;        // iterations completed
   int conv_iter;   // 0-based index of the converging iteration, -1 before
+  int xpend;       // x += alpha p of the iteration just completed is still due
 };
 
 // done[] flag values
@@ -50,9 +53,13 @@ enum Stage {
   ST_CG_INIT = 6    // totals[0] = (r,r), [1] = |b|^2 -> rr, target
 };
 
+// blocks per first-level group of a reduction (see block_reduce_finish)
+constexpr int kReduceGroup = 32;
+
 struct Reduce {
   double* partials;   // [blocks][nred*nrhs] scratch
-  unsigned* counter;  // ticket, returned to zero by the last block
+  double* gpartials;  // [groups][nred*nrhs] scratch
+  unsigned* counter;  // [0]: group ticket; [1 + g]: block ticket of group g; all return to zero
   double* out;        // [nred*nrhs] totals
   int stage;
   void* state;   // CGState[nrhs] or MSState
@@ -65,6 +72,7 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
     case ST_CG_ALPHA: {
       CGState* s = static_cast<CGState*>(R.state);
       for (int r = 0; r < nrhs; ++r) {
+        s[r].xpend = 0;  // the previous iteration's p update has run
         if (R.done[r]) continue;
         s[r].pap = tot[r];
         s[r].alpha = s[r].rr / s[r].pap;
@@ -76,6 +84,7 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
         if (R.done[r]) continue;
         s[r].rr_prev = s[r].rr;
         s[r].rr = tot[r];
+        s[r].xpend = 1;
         const int it = s[r].iter;
         s[r].iter = it + 1;
         if (!isfinite(s[r].rr)) {  // breakdown: stop rather than iterate to max_iter
@@ -202,27 +211,41 @@ __device__ void block_reduce_finish(const Reduce& R, const double* v, int nrhs, 
 #pragma unroll
     for (int k = 0; k < NRED; ++k) R.partials[int64_t(bid) * nv + k * nrhs + u] = sm[k][u];
   }
+  // level 1: the last block of each group of kReduceGroup consecutive blocks
+  // sums the group's partials in block order
+  const int grp = bid / kReduceGroup;
+  const int first = grp * kReduceGroup;
+  const int gsize = min(kReduceGroup, nblk - first);
   __threadfence();
   __syncthreads();
-  if (t == 0) last = (atomicAdd(R.counter, 1u) == unsigned(nblk - 1));
+  if (t == 0) last = (atomicAdd(R.counter + 1 + grp, 1u) == unsigned(gsize - 1));
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int q = t; q < nv; q += n) {
+    const double* src = R.partials + int64_t(first) * nv + q;
+    double s = 0.0;
+#pragma unroll 8
+    for (int j = 0; j < gsize; ++j) s += __ldcg(src + int64_t(j) * nv);
+    R.gpartials[int64_t(grp) * nv + q] = s;
+  }
+  if (t == 0) R.counter[1 + grp] = 0u;
+  // level 2: the last group to finish sums the group partials in group order
+  const int ngrp = (nblk + kReduceGroup - 1) / kReduceGroup;
+  __threadfence();
+  __syncthreads();
+  if (t == 0) last = (atomicAdd(R.counter, 1u) == unsigned(ngrp - 1));
   __syncthreads();
   if (!last) return;
   __threadfence();
   __shared__ double tot[NRED * 16];
-  int p2 = 1;
-  while (p2 < n) p2 <<= 1;
-  for (int q = 0; q < nv; ++q) {
+  for (int q = t; q < nv; q += n) {
     double s = 0.0;
-    for (int b = t; b < nblk; b += n) s += __ldcg(R.partials + int64_t(b) * nv + q);
-    sm[0][t] = s;
-    __syncthreads();
-    for (int h = p2 / 2; h > 0; h >>= 1) {
-      if (t < h && t + h < n) sm[0][t] += sm[0][t + h];
-      __syncthreads();
-    }
-    if (t == 0) tot[q] = sm[0][0];
-    __syncthreads();
+#pragma unroll 8
+    for (int g = 0; g < ngrp; ++g) s += __ldcg(R.gpartials + int64_t(g) * nv + q);
+    tot[q] = s;
   }
+  __syncthreads();
   if (t == 0) {
     for (int q = 0; q < nv; ++q) R.out[q] = tot[q];
     *R.counter = 0u;

@@ -151,12 +151,12 @@ int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* 
   Reduce rbeta = reduce(c, ST_CG_BETA, prm->max_iter);
   auto body = [&](int n) -> int {
     for (int i = 0; i < n; ++i) {
-      // (p, A p) = |D p|^2; then D^dag (D p) with x += alpha p, r -= alpha A p
-      // and (r, r) fused into its last launch
+      // (p, A p) = |D p|^2; then D^dag (D p) with r -= alpha A p and (r, r)
+      // fused into its last launch; x += alpha p with the p update
       RC(apply(c, op, mass, csw, false, *P, *Q, &ralpha, RED_OUT2, skip));
       RC(apply_cg(c, op, mass, csw, true, *Q, *S, rbeta, skip,
-                  CGFuse{X, R, P, static_cast<const CGState*>(state(c))}));
-      CK(launch_cg_p(PREC_DOUBLE, P->sites(), nrhs, P->all(), R->all(),
+                  CGFuse{R, static_cast<const CGState*>(state(c))}));
+      CK(launch_cg_p(PREC_DOUBLE, P->sites(), nrhs, P->all(), R->all(), X->all(),
                      static_cast<const CGState*>(state(c)), done(c), st));
     }
     return IRO_OK;
@@ -451,8 +451,8 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
     for (int i = 0; i < n; ++i) {
       RC(apply(c, op, mass, csw, false, *Pl, *Ql, &ralpha, RED_OUT2, skip));
       RC(apply_cg(c, op, mass, csw, true, *Ql, *Sl, rbeta, skip,
-                  CGFuse{Xl, Rl, Pl, static_cast<const CGState*>(state(c))}));
-      CK(launch_cg_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(),
+                  CGFuse{Rl, static_cast<const CGState*>(state(c))}));
+      CK(launch_cg_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(), Xl->all(),
                      static_cast<const CGState*>(state(c)), done(c), st));
     }
     return IRO_OK;

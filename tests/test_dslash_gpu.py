@@ -150,7 +150,9 @@ def test_multi_rhs_equals_single(prec):
     for r in range(12):
         one = c.apply(ib.OP_CLOVER_SCHUR_EE, m, 1.0, 0, fs[r], prec)
         if prec == "double":
-            assert np.array_equal(blk[r], one)
+            # the autotuner may run one shape on reconstructed third link rows
+            # and the other on the stored ones: equal to FP64 rounding
+            assert rel(blk[r], one) < 1e-13
         else:
             # FP32/FP16 blocks may run two right-hand sides per thread in
             # packed FP32x2 arithmetic: equal to FP32 rounding, not bitwise
