@@ -42,7 +42,12 @@ enum {
   IRO_TIMEOUT = 4,       /* a device-side wait hit its iteration limit */
   IRO_NO_GAUGE = 5,      /* operator applied before iro_gauge_upload */
   IRO_NO_CLOVER = 6,     /* clover operator applied before iro_clover_setup */
-  IRO_OUT_OF_MEMORY = 7
+  IRO_OUT_OF_MEMORY = 7,
+  IRO_IO_ERROR = 8,      /* a file that cannot be opened, read or written; the
+                            reference stops in Errors::IOErr (lib/IO/fields_io.hpp:283) */
+  IRO_FORMAT_ERROR = 9,  /* a file whose header or size does not match the lattice
+                            (the NERSC header checks, lib/IO/NERSC_reader.cpp:47-175) */
+  IRO_UNSUPPORTED = 10   /* a format whose library is absent here (ILDG needs lime) */
 };
 
 /* ---- operators ----------------------------------------------------------- */
@@ -320,6 +325,56 @@ int iro_synth_gaussian(int64_t nsites, uint64_t seed, double* f);
    (lib/Measurements/FermionicM/source_types.hpp:40-60): 12 consecutive
    Format_F fields of nsites sites. */
 int iro_synth_point_sources(int64_t nsites, int64_t site, double* f12);
+
+/* ---- gauge-configuration files ------------------------------------------------
+   The readers behind GaugeConf_*::init_conf (lib/Main/gaugeConf.cpp:23-228) and
+   CCIO::ReadFromDisk / SaveOnDisk (lib/IO/fields_io.hpp:48-360), host-only (no
+   context, no GPU): a file <-> a Format_G array u[18 * (site + V * mu)] with
+   site = x + Lx (y + Ly (z + Lz t)), ready for iro_gauge_upload.  Readers
+   return IRO_IO_ERROR / IRO_FORMAT_ERROR / IRO_UNSUPPORTED with a message in
+   iro_io_last_error() (per thread). */
+enum {
+  IRO_GAUGE_BINARY = 0,       /* GaugeConf_bin: BinaryReader (lib/IO/binary_reader.cpp:21-35),
+                                 [site][mu][18] big-endian doubles; BinaryWriter
+                                 (binary_writer.cpp:18-24) writes host byte order */
+  IRO_GAUGE_JLQCD_LEGACY = 1, /* GaugeConf_JLQCDLegacy (gaugeConf.cpp:28-33): a 4-byte
+                                 Fortran record word, then [mu][site][18] host-order doubles */
+  IRO_GAUGE_NERSC = 2,        /* GaugeConf_NERSC: NERSCReader (lib/IO/NERSC_reader.cpp), text
+                                 header, [site][mu][12 or 18] big-endian 32/64-bit; NERSCWriter
+                                 (NERSC_writer.cpp) writes 3x3 IEEE64BIG */
+  IRO_GAUGE_ILDG = 3,         /* GaugeConf_ILDG: needs lime, absent -> IRO_UNSUPPORTED */
+  IRO_GAUGE_ILDG_FORTRAN = 4, /* GaugeConf_ILDG_FORTRAN: likewise */
+  IRO_GAUGE_CSDT = 5,         /* GaugeConf_csdt (gaugeConf.cpp:66-140): 4-byte record word,
+                                 then [t][mu][z][y][x][a][b] big-endian complex doubles */
+  IRO_GAUGE_TEXT = 6,         /* GaugeConf_txt (gaugeConf.cpp:142-209): text,
+                                 [t][z][y][x][mu][a][b] "re im" */
+  IRO_GAUGE_UNIT = 7          /* GaugeConf_unit (gaugeConf.cpp:211-228): unit links, no file */
+};
+
+typedef struct iro_gauge_info {
+  double plaquette;         /* Staples::plaquette of the field read or written */
+  double link_trace;        /* Staples::link_trace */
+  double stored_plaquette;  /* NERSC header PLAQUETTE / LINK_TRACE / CHECKSUM */
+  double stored_link_trace;
+  uint32_t checksum;        /* NERSC: sum of the data's 32-bit words as in the file */
+  uint32_t stored_checksum;
+  int is3x2;                /* NERSC: DATATYPE 4D_SU3_GAUGE (two rows stored) */
+  int bits;                 /* NERSC: 32 or 64 */
+} iro_gauge_info;
+
+/* Reads format `format` at byte `offset` (0 for the reference's own offsets)
+   into u.  info (may be null) gets the plaquette and link trace of u and, for
+   NERSC, the header's values and both checksums.  Like the reference, a read
+   does not fail on a plaquette or checksum mismatch (ReadFromDisk's check is
+   commented out, fields_io.hpp:346-352): compare info's fields to check. */
+int iro_gauge_read(const char* path, int format, const int L[4], int64_t offset, double* u,
+                   iro_gauge_info* info);
+/* SaveOnDisk<Format_G>(u, path, append, "Binary" | "NERSC"). */
+int iro_gauge_write(const char* path, int format, const int L[4], const double* u, int append);
+/* Staples::plaquette and Staples::link_trace (lib/Measurements/GaugeM/staples.cpp:24-38):
+   sum of Re tr over the 6 planes / (3 * 6 * V) and of Re tr U / (3 * 4 * V). */
+int iro_gauge_plaquette(const int L[4], const double* u, double* plaquette, double* link_trace);
+const char* iro_io_last_error(void);
 
 #ifdef __cplusplus
 }

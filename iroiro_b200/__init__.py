@@ -39,12 +39,16 @@ __all__ = [
     "synth_gauge", "synth_gaussian", "synth_point_sources",
     "OP_WILSON_FULL", "OP_WILSON_HOP_EO", "OP_WILSON_HOP_OE", "OP_WILSON_SCHUR_EE",
     "OP_CLOVER_FULL", "OP_CLOVER_SCHUR_EE", "OP_CLOVER_HOP_OE_INV", "PREC_DOUBLE", "PREC_SINGLE", "PREC_HALF",
+    "GaugeConf", "GaugeConf_bin", "GaugeConf_JLQCDLegacy", "GaugeConf_NERSC", "GaugeConf_ILDG",
+    "GaugeConf_ILDG_FORTRAN", "GaugeConf_csdt", "GaugeConf_txt", "GaugeConf_unit", "GaugeInfo",
+    "read_gauge", "save_on_disk", "plaquette", "link_trace",
 ]
 
 _HERE = Path(__file__).resolve().parent
 _LIBPATH = _HERE / "libiroiro_b200.so"
 
-OK, NOT_CONVERGED, BAD_ARG, CUDA_ERROR, TIMEOUT, NO_GAUGE, NO_CLOVER, OUT_OF_MEMORY = range(8)
+(OK, NOT_CONVERGED, BAD_ARG, CUDA_ERROR, TIMEOUT, NO_GAUGE, NO_CLOVER, OUT_OF_MEMORY, IO_ERROR,
+ FORMAT_ERROR, UNSUPPORTED) = range(11)
 (OP_WILSON_FULL, OP_WILSON_HOP_EO, OP_WILSON_HOP_OE, OP_WILSON_SCHUR_EE,
  OP_CLOVER_FULL, OP_CLOVER_SCHUR_EE, OP_CLOVER_HOP_OE_INV) = range(7)
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = range(3)
@@ -121,6 +125,10 @@ def _declare(L):
         "iro_synth_gauge": (I, [L4, D, ctypes.c_uint64, I, _D]),
         "iro_synth_gaussian": (I, [ctypes.c_int64, ctypes.c_uint64, _D]),
         "iro_synth_point_sources": (I, [ctypes.c_int64, ctypes.c_int64, _D]),
+        "iro_gauge_read": (I, [ctypes.c_char_p, I, L4, ctypes.c_int64, _D, _VP]),
+        "iro_gauge_write": (I, [ctypes.c_char_p, I, L4, _D, I]),
+        "iro_gauge_plaquette": (I, [L4, _D, _D, _D]),
+        "iro_io_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -808,3 +816,10 @@ class Qprop:
         if rc != OK:
             raise ConvergenceError(rc, "Qprop: CG not converged")
         return list(x.reshape(len(srcs), -1))
+
+
+# gauge-configuration files (GaugeConf_*, CCIO::SaveOnDisk, Staples::plaquette)
+from .gaugeconf import (GaugeConf, GaugeConf_bin, GaugeConf_csdt, GaugeConf_ILDG,  # noqa: E402
+                        GaugeConf_ILDG_FORTRAN, GaugeConf_JLQCDLegacy, GaugeConf_NERSC,
+                        GaugeConf_txt, GaugeConf_unit, GaugeInfo, link_trace, plaquette,
+                        read_gauge, save_on_disk)

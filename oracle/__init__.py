@@ -204,6 +204,9 @@ class Ref:
         lib.ref_eo_mult_throughput.argtypes = [_D, D, _D, _D, _I, _I, _D]
         lib.ref_eo_invert.argtypes = [_D, D, _D, _D, _I, D, _I]
         lib.ref_md_force.argtypes = [_D, _I, D, _D, _D, _D]
+        lib.ref_gauge_save.argtypes = [_D, ctypes.c_char_p, _I]
+        lib.ref_gauge_load.argtypes = [ctypes.c_char_p, _I, _D]
+        lib.ref_plaquette.argtypes = [_D, _D, _D]
         lib.ref_rational_solve.argtypes = [_D, _I, D, D, _D, _I, _D, _D, D, _D, D, _I, _D,
                                            ctypes.POINTER(_I)]
         self.L = None
@@ -287,6 +290,22 @@ class Ref:
         F = np.empty(72 * int(np.prod(self.L)))
         self._chk(self.lib.ref_md_force(_p(u), op, mass, _p(eta), _p(zeta), _p(F)), "ref_md_force")
         return F
+
+    def gauge_save(self, u, path, writer):
+        """CCIO::SaveOnDisk<Format_G>(u, path, false, "Binary" (0) | "NERSC" (2))."""
+        self._chk(self.lib.ref_gauge_save(_p(u), str(path).encode(), writer), "ref_gauge_save")
+
+    def gauge_load(self, path, kind):
+        """GaugeConf_{bin (0), NERSC (2), csdt (5), txt (6), unit (7)}::init_conf."""
+        u = np.zeros(72 * int(np.prod(self.L)))
+        self._chk(self.lib.ref_gauge_load(str(path).encode(), kind, _p(u)), "ref_gauge_load")
+        return u
+
+    def plaquette(self, u):
+        """(Staples::plaquette, Staples::link_trace)."""
+        p, t = ctypes.c_double(), ctypes.c_double()
+        self._chk(self.lib.ref_plaquette(_p(u), ctypes.byref(p), ctypes.byref(t)), "ref_plaquette")
+        return p.value, t.value
 
     def eo_mult_throughput(self, u, mass, f, nthreads, reps):
         out = np.empty_like(f)

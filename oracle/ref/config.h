@@ -7,6 +7,12 @@
 #define IROIRO_ORACLE_REF_CONFIG_H
 #define IMPROVED_WILSON 1
 #define VERBOSITY 1
+#define HAVE_SQRT 1
+#define STDC_HEADERS 1
+#endif
+/* The package macros sit outside the include guard: include/iroiro_config.h
+   undefines them and includes this file again to define them afresh. */
+#ifndef PACKAGE
 #define PACKAGE "iroiro"
 #define PACKAGE_BUGREPORT ""
 #define PACKAGE_NAME "IroIro"
@@ -15,6 +21,4 @@
 #define PACKAGE_URL ""
 #define PACKAGE_VERSION "1.0.9"
 #define VERSION "1.0.9"
-#define HAVE_SQRT 1
-#define STDC_HEADERS 1
 #endif

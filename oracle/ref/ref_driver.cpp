@@ -124,6 +124,9 @@ Dirac* make_dirac(int op, double mass, double csw, const Field* u) {
 
 extern "C" {
 
+// whether ref_init() has set up the lattice singletons
+int ref_ready(void) { return g_init ? 1 : 0; }
+
 // CommonPrms::instance(Lattice) with a 1x1x1x1 process grid.
 int ref_init(int Lx, int Ly, int Lz, int Lt) {
   if (g_init) {
