@@ -93,9 +93,10 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
         }
         if (s[r].delta2 > 0.0) {
           // mixed precision: pause for an FP64 residual recomputation when
-          // |r| fell by delta since the last one, or looks converged;
-          // convergence is declared on the true residual only
-          if (s[r].rr < s[r].delta2 * s[r].maxrr || s[r].rr < s[r].target) {
+          // |r| fell by delta since the last one (looking converged is
+          // handled for the group below); convergence is declared on the
+          // true residual only
+          if (s[r].rr < s[r].delta2 * s[r].maxrr) {
             R.done[r] = PAUSED;
             continue;
           }
@@ -111,10 +112,19 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
       // mixed precision: when one right-hand side pauses, the others pause
       // with it, so all share one FP64 residual recomputation (which treats
       // every right-hand side in one launch anyway) instead of idling in
-      // lockstep until each reaches its own trigger
-      bool any_pause = false;
-      for (int r = 0; r < nrhs; ++r) any_pause = any_pause || R.done[r] == PAUSED;
-      if (any_pause)
+      // lockstep until each reaches its own trigger.  A right-hand side whose
+      // iterated residual looks converged keeps iterating until every one
+      // still running does: then one recomputation confirms them together,
+      // instead of one per right-hand side as each crosses the target.
+      bool any_pause = false, any_mixed = false, all_conv = true;
+      for (int r = 0; r < nrhs; ++r) {
+        any_pause = any_pause || R.done[r] == PAUSED;
+        if (R.done[r] == RUNNING && s[r].delta2 > 0.0) {
+          any_mixed = true;
+          all_conv = all_conv && s[r].rr < s[r].target;
+        }
+      }
+      if (any_pause || (any_mixed && all_conv))
         for (int r = 0; r < nrhs; ++r)
           if (R.done[r] == RUNNING && s[r].delta2 > 0.0) R.done[r] = PAUSED;
     } break;
