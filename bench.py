@@ -767,7 +767,7 @@ def kernel_only(args):
     import torch
     import iroiro_b200 as ib
     Lk = [int(v) for v in args.lattice.split(",")]
-    if args.kernel.startswith("ptc,") or args.kernel == "md_force_eo":
+    if args.kernel.startswith(("ptc,", "batched,")) or args.kernel == "md_force_eo":
         return kernel_only_other(args, Lk)
     opn, prec, nrhs = args.kernel.split(",")
     nrhs = int(nrhs)
@@ -796,12 +796,39 @@ def kernel_only(args):
 def kernel_only_other(args, Lk):
     """Profiling driver for the other kernels: --kernel ptc,4-16-16-16-4 applies
     that network `steps` times to an FP32 field; --kernel md_force_eo computes
-    one even/odd Wilson MD force; both inside cudaProfilerStart/Stop."""
+    one even/odd Wilson MD force; --kernel batched,INNER,DELTA runs the batched
+    configuration's solve (the 12 point sources on the seeded field of
+    batched_solves, on the lattice given) once untimed and once profiled; all
+    inside cudaProfilerStart/Stop."""
     import torch
     import iroiro_b200 as ib
     from iroiro_b200 import learned
     V = int(np.prod(Lk))
     ctx = ib.Context(Lk, 0)
+    if args.kernel.startswith("batched,"):
+        _, inner, delta = args.kernel.split(",")
+        st = torch.cuda.Stream()
+        torch.cuda.set_stream(st)
+        ctx.set_stream(st.cuda_stream)  # a capturable stream: the solver's CUDA graphs
+        u = ib.synth_gauge(Lk, EPS, SEED + 7, gauge_transform=False)
+        ctx.upload_gauge(u, force=True)
+        D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+        site = int(np.random.default_rng(SEED).integers(V // 2))
+        B = ib.DeviceField(ctx, 0, "double", 12).upload(ib.synth_point_sources(V // 2, site).ravel())
+        X = ib.DeviceField(ctx, 0, "double", 12)
+        slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner, delta=float(delta))
+        slv.solve_field(B, X)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        t0 = time.perf_counter()
+        outs, rc = slv.solve_field(B, X)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        torch.cuda.profiler.stop()
+        print(json.dumps({"kernel": args.kernel, "lattice": Lk, "ms": round(ms, 2),
+                          "iterations": max(o.Iterations for o in outs),
+                          "reliable_updates": max(o.reliable_updates for o in outs), "rc": rc}))
+        return 0
     u = ib.synth_gauge(Lk, EPS, SEED, gauge_transform=True)
     ctx.upload_gauge(u, force=True)
     if args.kernel.startswith("ptc,"):
