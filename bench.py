@@ -508,6 +508,16 @@ def callers(torch, device):
         D.md_force(e, z)
     torch.cuda.synchronize()
     out["md_force_evenodd_24x24x24x48_ms"] = round((time.perf_counter() - t) * 1e3 / 5, 2)
+    # Dirac_Clover::md_force: the Wilson force plus the clover term's leaf derivatives
+    Dc = ib.Dirac_Clover(ib.Dirac_Wilson(MASS, u, ctx=ctx), CSW, u, ctx=ctx)
+    ef, zf = ib.synth_gaussian(2 * Vh, SEED + 14), ib.synth_gaussian(2 * Vh, SEED + 15)
+    Dc.md_force(ef, zf)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(5):
+        Dc.md_force(ef, zf)
+    torch.cuda.synchronize()
+    out["md_force_clover_24x24x24x48_ms"] = round((time.perf_counter() - t) * 1e3 / 5, 2)
     out["md_force_note"] = "host arrays: 2 spinors in, the 72*V-double Format_G force out (382 MB)"
     ctx.close()
     return out
@@ -767,7 +777,7 @@ def kernel_only(args):
     import torch
     import iroiro_b200 as ib
     Lk = [int(v) for v in args.lattice.split(",")]
-    if args.kernel.startswith(("ptc,", "batched,")) or args.kernel == "md_force_eo":
+    if args.kernel.startswith(("ptc,", "batched,")) or args.kernel in ("md_force_eo", "md_force_clover"):
         return kernel_only_other(args, Lk)
     opn, prec, nrhs = args.kernel.split(",")
     nrhs = int(nrhs)
@@ -796,7 +806,8 @@ def kernel_only(args):
 def kernel_only_other(args, Lk):
     """Profiling driver for the other kernels: --kernel ptc,4-16-16-16-4 applies
     that network `steps` times to an FP32 field; --kernel md_force_eo computes
-    one even/odd Wilson MD force; --kernel batched,INNER,DELTA runs the batched
+    one even/odd Wilson MD force, --kernel md_force_clover one full-lattice
+    Wilson-clover MD force; --kernel batched,INNER,DELTA runs the batched
     configuration's solve (the 12 point sources on the seeded field of
     batched_solves, on the lattice given) once untimed and once profiled; all
     inside cudaProfilerStart/Stop."""
@@ -838,6 +849,11 @@ def kernel_only_other(args, Lk):
         b = ib.DeviceField(ctx, 2, "single")
         run = lambda: ctx.check(net.L.iro_ptc_apply_field(ctx.h, net.h, a.h, b.h), "apply")
         reps = args.steps
+    elif args.kernel == "md_force_clover":
+        D = ib.Dirac_Clover(ib.Dirac_Wilson(MASS, u, ctx=ctx), CSW, u, ctx=ctx)
+        e, z = ib.synth_gaussian(V, SEED + 1), ib.synth_gaussian(V, SEED + 2)
+        run = lambda: D.md_force(e, z)
+        reps = 1
     else:
         D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
         e, z = ib.synth_gaussian(V // 2, SEED + 1), ib.synth_gaussian(V // 2, SEED + 2)

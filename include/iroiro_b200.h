@@ -247,16 +247,21 @@ int iro_rational_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const d
 int iro_eo_invert(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
                   const double* src, double* sol, int nrhs, iro_solver_out* out);
 
-/* Molecular-dynamics force of the Wilson operator, FP64:
+/* Molecular-dynamics force, FP64: the F with
+   Re Tr(X F_mu(x)) = d/de Re(zeta^dag D(U_mu(x) -> (1 + e X) U_mu(x)) eta).
    op = IRO_OP_WILSON_FULL: Dirac_Wilson::md_force(eta, zeta)
         (lib/Dirac_ops/dirac_wilson.cpp:41-91), eta and zeta full-lattice
         Format_F arrays;
    op = IRO_OP_WILSON_SCHUR_EE: Dirac_Wilson_EvenOdd::md_force(eta, zeta)
         (lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:95-117), eta and zeta even
-        halves (24*V/2 doubles).
-   force receives the Format_G field (72*V doubles), overwritten. */
-int iro_md_force(iro_ctx* ctx, int op, double mass, const double* eta, const double* zeta,
-                 double* force);
+        halves (24*V/2 doubles);
+   op = IRO_OP_CLOVER_FULL: Dirac_Clover::md_force(eta, zeta)
+        (lib/Dirac_ops/dirac_clover.cpp:356-532): the Wilson force plus the
+        derivative of the clover term, full-lattice arrays.
+   csw is used by the clover operator only.  force receives the Format_G
+   field (72*V doubles), overwritten. */
+int iro_md_force(iro_ctx* ctx, int op, double mass, double csw, const double* eta,
+                 const double* zeta, double* force);
 
 /* ---- learned preconditioner and flexible GCR --------------------------------
    No counterpart in the reference (its solvers are CG, BiCGStab and

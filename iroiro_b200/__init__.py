@@ -121,7 +121,7 @@ def _declare(L):
                                       ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
         "iro_eo_invert": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
                               ctypes.POINTER(SolverOut)]),
-        "iro_md_force": (I, [_VP, I, D, _D, _D, _D]),
+        "iro_md_force": (I, [_VP, I, D, D, _D, _D, _D]),
         "iro_synth_gauge": (I, [L4, D, ctypes.c_uint64, I, _D]),
         "iro_synth_gaussian": (I, [ctypes.c_int64, ctypes.c_uint64, _D]),
         "iro_synth_point_sources": (I, [ctypes.c_int64, ctypes.c_int64, _D]),
@@ -404,18 +404,20 @@ class _Dirac:
         return self.u
 
     def md_force(self, eta: np.ndarray, zeta: np.ndarray) -> np.ndarray:
-        """The MD force zeta^dag dD/dU eta as a Format_G field (gsize doubles):
+        """The MD force zeta^dag dD/dU eta as a Format_G field (gsize doubles),
+        Re Tr(X F_mu(x)) = d/de Re(zeta^dag D(U_mu(x) -> (1 + e X) U_mu(x)) eta):
         Dirac_Wilson::md_force (lib/Dirac_ops/dirac_wilson.cpp:41-58) for the
         full operator, Dirac_Wilson_EvenOdd::md_force
-        (dirac_wilson_EvenOdd.hpp:95-117) for the e/o one."""
-        if self.op not in (OP_WILSON_FULL, OP_WILSON_SCHUR_EE):
-            raise IroError(BAD_ARG, "md_force: Wilson full or even/odd operator only")
+        (dirac_wilson_EvenOdd.hpp:95-117) for the e/o one, Dirac_Clover::md_force
+        (dirac_clover.cpp:356-532) for the full clover operator."""
+        if self.op not in (OP_WILSON_FULL, OP_WILSON_SCHUR_EE, OP_CLOVER_FULL):
+            raise IroError(BAD_ARG, "md_force: Wilson full or even/odd, or full clover operator")
         self.ctx.upload_gauge(self.u)
         n = self.fsize()
         eta, zeta = _f64(eta, n, "eta"), _f64(zeta, n, "zeta")
         F = np.empty(self.gsize())
-        self.ctx.check(self.ctx._lib.iro_md_force(self.ctx.h, self.op, self.mass, _ptr(eta),
-                                                  _ptr(zeta), _ptr(F)), "iro_md_force")
+        self.ctx.check(self.ctx._lib.iro_md_force(self.ctx.h, self.op, self.mass, self.csw,
+                                                  _ptr(eta), _ptr(zeta), _ptr(F)), "iro_md_force")
         return F
 
 

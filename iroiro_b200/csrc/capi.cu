@@ -821,6 +821,7 @@ bool op_ok(int op) { return op_valid(op); }
 int clover_ready(iro_ctx* c, double mass, double csw) { return ensure_clover(c, mass, csw); }
 GaugePtr gauge_double(iro_ctx* c) { return gauge_ptr(c, PREC_DOUBLE); }
 int gauge_recon(iro_ctx* c) { return c->recon; }
+const double* gauge_format_g(iro_ctx* c) { return c->raw; }
 bool gauge_loaded(iro_ctx* c) { return c->has_gauge; }
 CloverPtr clover(iro_ctx* c, int prec, int p, bool inverse) { return clover_ptr(c, prec, p, inverse); }
 }  // namespace host

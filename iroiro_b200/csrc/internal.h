@@ -164,6 +164,11 @@ cudaError_t launch_clover_mult(int64_t Vh, int nrhs, CloverPtr cl, SpinorPtr in,
 // ---- molecular-dynamics force (forces.cu) ------------------------------------------
 // F[mu][lex site][18] += w (1 - g_mu) U_mu(x) psi(x+mu) (x) chi(x)^dag over the
 // sites x of parity p (gamma5 on both fields when g5)
+// the clover block of Dirac_Clover::md_force, added to F (Format_G) with weight
+// w = -kappa csw / 4; lam: scratch of 6 * 9 * V double2
+cudaError_t launch_clover_force(const Geom& g, const double* u_format_g, SpinorPtr e0, SpinorPtr e1,
+                                SpinorPtr z0, SpinorPtr z1, double w, double2* lam, double* F,
+                                cudaStream_t st);
 cudaError_t launch_force(const Geom& g, const GaugePtr& gauge, int recon, int p, SpinorPtr psi,
                          SpinorPtr chi, int g5, double w, double* F, cudaStream_t st);
 

@@ -43,6 +43,7 @@ int clover_ready(iro_ctx* c, double mass, double csw);
 CloverPtr clover(iro_ctx* c, int prec, int p, bool inverse);
 GaugePtr gauge_double(iro_ctx* c);
 int gauge_recon(iro_ctx* c);
+const double* gauge_format_g(iro_ctx* c);
 bool gauge_loaded(iro_ctx* c);
 const Geom& geom(iro_ctx* c);
 int64_t volume(iro_ctx* c);
@@ -652,13 +653,14 @@ extern "C" int iro_eo_invert(iro_ctx* c, int op, double mass, double csw,
 //   F = kappa [Deo.p(A, zeta) + Doe.m(A, zeta) + Doe.p(eta, B) + Deo.m(eta, B)]
 // with X.p(e, z) = mkfrc(e, z) and X.m(e, z) = mkfrc(g5 z, g5 e) on the
 // output sites of X (even for Deo, odd for Doe), in that order.
-extern "C" int iro_md_force(iro_ctx* c, int op, double mass, const double* eta,
+extern "C" int iro_md_force(iro_ctx* c, int op, double mass, double csw, const double* eta,
                             const double* zeta, double* force) {
-  if (!c || !eta || !zeta || !force || (op != IRO_OP_WILSON_FULL && op != IRO_OP_WILSON_SCHUR_EE))
+  if (!c || !eta || !zeta || !force ||
+      (op != IRO_OP_WILSON_FULL && op != IRO_OP_WILSON_SCHUR_EE && op != IRO_OP_CLOVER_FULL))
     return set_error(c, IRO_BAD_ARG, "bad md_force arguments");
   if (!gauge_loaded(c)) return set_error(c, IRO_NO_GAUGE, "no gauge field uploaded");
   CK(cudaSetDevice(device(c)));
-  const bool full = op == IRO_OP_WILSON_FULL;
+  const bool full = op != IRO_OP_WILSON_SCHUR_EE;
   const double k = 0.5 / (4.0 + mass);
   int rc = IRO_OK;
   const int sub = full ? 2 : 0;
@@ -683,6 +685,23 @@ extern "C" int iro_md_force(iro_ctx* c, int op, double mass, const double* eta,
     for (int p = 0; p < 2; ++p) {
       CK(launch_force(g, U, recon, p, E->half(1 - p), Z->half(p), 0, -k, F, st));
       CK(launch_force(g, U, recon, p, Z->half(1 - p), E->half(p), 1, -k, F, st));
+    }
+    if (op == IRO_OP_CLOVER_FULL && csw != 0.0) {
+      // the clover block of Dirac_Clover::md_force: Lambda_k for the 6 planes
+      // (6 * 9 complex per site), then the leaf derivatives; its site offsets
+      // reach two sites out, which one periodic wrap covers for extents >= 2
+      for (int d = 0; d < 4; ++d)
+        if (g.L[d] < 2) return set_error(c, IRO_BAD_ARG, "clover force needs every extent >= 2");
+      const size_t nL = size_t(6) * 9 * size_t(volume(c));
+      double2* lam = nullptr;
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&lam), nL * sizeof(double2), st));
+      struct FreeL {
+        double2* p;
+        cudaStream_t s;
+        ~FreeL() { if (p) cudaFreeAsync(p, s); }
+      } lguard{lam, st};
+      CK(launch_clover_force(g, gauge_format_g(c), E->half(0), E->half(1), Z->half(0), Z->half(1),
+                             -k * csw / 4.0, lam, F, st));
     }
   } else {
     DevField* A = workspace(c, 1, PREC_DOUBLE, 1, 62, &rc); if (!A) return rc;

@@ -1,6 +1,8 @@
-"""Wilson MD forces on the GPU against the reference's md_force (golden
-fixtures, including the 6x2x4x4 lattice whose two y-neighbours coincide) and
-against the oracle on a larger lattice."""
+"""MD forces on the GPU: the Wilson ones against the reference's md_force
+(golden fixtures, including the 6x2x4x4 lattice whose two y-neighbours
+coincide) and the oracle on a larger lattice; the clover one
+(Dirac_Clover::md_force) against derivatives of the reference's clover operator
+and the oracle's restatement."""
 import numpy as np
 import pytest
 
@@ -65,3 +67,38 @@ def test_md_force_is_the_derivative_of_the_operator():
         fd = (f(h) - f(-h)) / (2 * h)
         an = float(np.trace(X @ (F[mu, x, ..., 0] + 1j * F[mu, x, ..., 1])).real)
         assert abs(fd - an) < 1e-6 * max(1.0, abs(an)), (fd, an)
+
+
+@pytest.mark.parametrize("name", ["4x4x4x4", "6x2x4x4"])
+def test_clover_md_force_vs_reference_operator(name, port):
+    """Dirac_Clover::md_force: the derivative of the reference's own clover
+    operator (golden central differences, ~1e-10), and the oracle's
+    restatement to FP64 round-off."""
+    from oracle.clover_force import clover_md_force
+    g = load_golden(name)
+    L, u, m, csw = [int(v) for v in g["L"]], g["u"], float(g["mass"]), float(g["csw"])
+    V = int(np.prod(L))
+    ctx = ib.Context(L, 0)
+    Dw = ib.Dirac_Wilson(m, u, ctx=ctx)
+    D = ib.Dirac_Clover(Dw, csw, u, ctx=ctx)
+    F = D.md_force(g["cforce_eta"], g["cforce_zeta"])
+    ref = clover_md_force(L, u, m, csw, g["cforce_eta"], g["cforce_zeta"], port)
+    assert rel(F, ref) < TOL_FP64
+    Fc = F.reshape(4, V, 3, 3, 2)
+    Fc = Fc[..., 0] + 1j * Fc[..., 1]
+    X = g["cforce_X"][..., 0] + 1j * g["cforce_X"][..., 1]
+    for k, fd in enumerate(g["cforce_fd"]):
+        an = float(np.trace(X[k] @ Fc[g["cforce_dirs"][k], g["cforce_sites"][k]]).real)
+        assert abs(an - fd) < 1e-8 * max(1.0, abs(fd)), (k, an, fd)
+
+
+def test_clover_md_force_vs_oracle_8x8x8x16(port):
+    from oracle.clover_force import clover_md_force
+    L = [8, 8, 8, 16]
+    V = int(np.prod(L))
+    u = ib.synth_gauge(L, 0.2, 95, gauge_transform=True)
+    m, csw = 0.5 / 0.124 - 4, 1.7
+    ctx = ib.Context(L, 0)
+    D = ib.Dirac_Clover(ib.Dirac_Wilson(m, u, ctx=ctx), csw, u, ctx=ctx)
+    e, z = ib.synth_gaussian(V, 96), ib.synth_gaussian(V, 97)
+    assert rel(D.md_force(e, z), clover_md_force(L, u, m, csw, e, z, port)) < TOL_FP64

@@ -94,3 +94,20 @@ def test_md_force(port, golden):
     assert rel(port.md_force(L, u, m, False, g["force_eta"], g["force_zeta"]), g["force_full"]) < TOL_FP64
     assert rel(port.md_force(L, u, m, True, g["force_eta_half"], g["force_zeta_half"]),
                g["force_eo"]) < TOL_FP64
+
+
+def test_clover_force_restatement_is_the_operator_derivative(golden, port):
+    """The oracle's Dirac_Clover::md_force meets the central differences of the
+    reference's own clover operator (the reference's force block returns zero in
+    the build here, so its operator is the pin)."""
+    from oracle.clover_force import clover_md_force
+    g = golden
+    L = [int(v) for v in g["L"]]
+    V = int(np.prod(L))
+    F = clover_md_force(L, g["u"], float(g["mass"]), float(g["csw"]), g["cforce_eta"],
+                        g["cforce_zeta"], port).reshape(4, V, 3, 3, 2)
+    F = F[..., 0] + 1j * F[..., 1]
+    X = g["cforce_X"][..., 0] + 1j * g["cforce_X"][..., 1]
+    for k, fd in enumerate(g["cforce_fd"]):
+        an = float(np.trace(X[k] @ F[g["cforce_dirs"][k], g["cforce_sites"][k]]).real)
+        assert abs(an - fd) < 1e-8 * max(1.0, abs(fd)), (k, an, fd)
