@@ -235,14 +235,31 @@ HopLaunch base_launch(iro_ctx* c, int prec, bool dag, int nrhs) {
 // launch is idempotent) before the real launch; during stream capture the
 // default configuration is used.  IRO_HOP_VARIANT="<variant>,<block>" fixes
 // the choice.
-// FP64 variants 6..11 are variants 0..5 on the stored 18-real links of an
-// SU(3) gauge field (no third-row reconstruction: fewer FP64 operations,
-// more link bytes).
+// Candidates (see hop_var): all precisions 0..3; FP64 4, 5 and, on an SU(3)
+// field, 6..11 = 0..5 on the stored 18-real links (no third-row
+// reconstruction: fewer FP64 operations, more link bytes); FP32/FP16 with an
+// even nrhs 4..9 (two right-hand sides per thread); FP16 10..12 (the
+// mixed-precision kernel on the FP16 links with three stored rows at 3, 4 or
+// 2 blocks per SM, any nrhs).
+constexpr int kHopVariants = 13;
+
+static bool variant_ok(const HopLaunch& L, int v) {
+  if (v < 0 || v >= kHopVariants) return false;
+  if (v < 4) return true;
+  if (L.prec == PREC_DOUBLE) return v < 12 && (v < 6 || L.recon == 12);
+  if (v < 10) return L.recon == 12 && L.nrhs % 2 == 0;
+  return L.prec == PREC_HALF && L.recon == 12;
+}
+
 static cudaError_t launch_variant(iro_ctx* c, HopLaunch L, cudaStream_t st) {
   if (L.prec == PREC_DOUBLE && L.variant >= 6) {
     L.variant -= 6;
     L.recon = 18;
     L.gauge.a = c->ga.d18;
+  } else if (L.prec == PREC_HALF && L.variant >= 10) {
+    L.recon = 18;
+    L.gauge.a = c->ga.h18a;
+    L.gauge.b = c->ga.h18b;
   }
   return launch_hop(L, st);
 }
@@ -252,16 +269,16 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
   cudaStream_t st = c->stream;
   static const char* forced = std::getenv("IRO_HOP_VARIANT");
   auto it = c->tuned.find(key);
-  // two right-hand sides per thread (variant bit 2) needs FP32/FP16 storage,
-  // reconstruct-12 links and an even number of right-hand sides
-  const bool pair_ok = L.prec != PREC_DOUBLE && L.recon == 12 && L.nrhs % 2 == 0;
-  // FP64: variants 4, 5 (168-register hop kernel), 6..11 on 18-real links of
-  // an SU(3) field; FP32/FP16: 4..9 when pairs apply
-  const int nvar = L.prec == PREC_DOUBLE ? (L.recon == 12 ? 12 : 6) : (pair_ok ? 10 : 4);
   if (forced) {
+    // the forced variant, modulo the candidates of the shape: FP64 6 (12 on
+    // an SU(3) field); otherwise 13, a variant the shape lacks falling back
+    // to its number modulo 4
     int v = 0, b = 256;
     std::sscanf(forced, "%d,%d", &v, &b);
-    c->tuned[key] = {v % nvar, b};
+    if (L.prec == PREC_DOUBLE) v %= (L.recon == 12 ? 12 : 6);
+    else if (!variant_ok(L, v % kHopVariants)) v %= 4;
+    else v %= kHopVariants;
+    c->tuned[key] = {v, b};
     it = c->tuned.find(key);
   }
   if (it == c->tuned.end()) {
@@ -281,8 +298,9 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
     std::pair<int, int> pick{0, 256};
-    for (int v = 0; v < nvar; ++v)
+    for (int v = 0; v < kHopVariants; ++v)
       for (int b : {256, 128}) {
+        if (!variant_ok(L, v)) continue;
         T.variant = v;
         T.block_cap = b;
         CK(launch_variant(c, T, st));  // warm-up
@@ -571,7 +589,8 @@ int iro_ctx_destroy(iro_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& kv : c->ws) free_field(kv.second);
-  void* ptrs[] = {c->raw, c->ga.d12, c->ga.d18, c->ga.s12, c->ga.h12a, c->ga.h12b, c->d_maxdev,
+  void* ptrs[] = {c->raw, c->ga.d12, c->ga.d18, c->ga.s12, c->ga.h12a, c->ga.h12b, c->ga.h18a,
+                  c->ga.h18b, c->d_maxdev,
                   c->d_singular, c->stage, c->partials, c->counter, c->redout, c->state, c->done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -631,6 +650,8 @@ int iro_gauge_upload(iro_ctx* c, const double* u) {
     CK(cudaMalloc(&c->ga.s12, size_t(2) * 4 * 3 * c->Vh * sizeof(float4)));
     CK(cudaMalloc(&c->ga.h12a, size_t(2) * 4 * c->Vh * sizeof(uint4)));
     CK(cudaMalloc(&c->ga.h12b, size_t(2) * 4 * c->Vh * sizeof(uint2)));
+    CK(cudaMalloc(&c->ga.h18a, size_t(2) * 4 * 2 * c->Vh * sizeof(uint4)));
+    CK(cudaMalloc(&c->ga.h18b, size_t(2) * 4 * c->Vh * sizeof(uint32_t)));
   }
   CK(cudaMemcpyAsync(c->raw, u, raw_bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_maxdev, 0, sizeof(unsigned long long), c->stream));

@@ -20,6 +20,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "dslash_mix.cuh"
 #include "solver_scalars.cuh"
 
 namespace iro {
@@ -166,11 +167,16 @@ struct HopParams {
 // VAR bit 1: the four directions as a rolled loop (no hoisting of one
 // direction's loads over another's, fewer live registers);
 // VAR bit 2 (FP64 only): 128-thread blocks, at least three per SM (register
-// cap 168: between the uncapped 254 and the spilling 128).
+// cap 168: between the uncapped 254 and the spilling 128);
+// VAR bit 3 (FP16 on links with three stored rows only): the mixed-precision
+// direction code of dslash_mix.cuh, at least three 256-thread blocks per SM
+// (four with bit 0, two with bit 1).
 template <int VAR>
 struct HopBounds {
   static constexpr int threads = (VAR & 4) ? 128 : 256;
-  static constexpr int blocks = (VAR & 4) ? 3 : ((VAR & 1) ? 2 : 1);
+  static constexpr int blocks =
+      (VAR & 8) ? ((VAR & 1) ? 4 : ((VAR & 2) ? 2 : 3))
+                : ((VAR & 4) ? 3 : ((VAR & 1) ? 2 : 1));
 };
 
 template <int SP, int GP, int RECON, bool DAG, int EPI, int CP, int VAR>
@@ -194,7 +200,13 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
     Cx<R> acc[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = {R(0), R(0)};
-    if (VAR & 2) {
+    if constexpr ((VAR & 8) != 0) {
+      static_assert(SP == PREC_HALF && RECON == 18, "mixed path: FP16 with three-row links");
+      hop_dir_mix<0, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      hop_dir_mix<1, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      hop_dir_mix<2, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      hop_dir_mix<3, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+    } else if (VAR & 2) {
 #pragma unroll 1
       for (int mu = 0; mu < 4; ++mu) {
         switch (mu) {

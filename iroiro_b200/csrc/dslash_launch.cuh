@@ -119,15 +119,34 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
 // 4-7 two right-hand sides per thread with the register cap none / 128 /
 // 152 / 168, 8-9 the same with the neighbours staged through shared memory.
 // FP64: 4/5 the 168-register 128-thread hop_kernel (5 with the rolled loop).
+// FP16 on links with three stored rows (RECON 18): only 10/11/12, the
+// mixed-precision hop_kernel (VAR 8 / 9 / 10: 3 / 4 / 2 blocks per SM).
+template <int SP, int GP, int RECON, bool DAG, int EPI>
+static cudaError_t hop_var_more(const HopLaunch& L, cudaStream_t st);
+
 template <int SP, int GP, int RECON, bool DAG, int EPI>
 static cudaError_t hop_var(const HopLaunch& L, cudaStream_t st) {
-  switch (L.variant) {
-    case 0: return hop_go<SP, GP, RECON, DAG, EPI, 0>(L, st);
-    case 1: return hop_go<SP, GP, RECON, DAG, EPI, 1>(L, st);
-    case 2: return hop_go<SP, GP, RECON, DAG, EPI, 2>(L, st);
-    case 3: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
-    default: break;
+  if constexpr (SP == PREC_HALF && RECON == 18) {
+    switch (L.variant) {
+      case 10: return hop_go<SP, GP, RECON, DAG, EPI, 8>(L, st);
+      case 11: return hop_go<SP, GP, RECON, DAG, EPI, 9>(L, st);
+      case 12: return hop_go<SP, GP, RECON, DAG, EPI, 10>(L, st);
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    switch (L.variant) {
+      case 0: return hop_go<SP, GP, RECON, DAG, EPI, 0>(L, st);
+      case 1: return hop_go<SP, GP, RECON, DAG, EPI, 1>(L, st);
+      case 2: return hop_go<SP, GP, RECON, DAG, EPI, 2>(L, st);
+      case 3: return hop_go<SP, GP, RECON, DAG, EPI, 3>(L, st);
+      default: break;
+    }
+    return hop_var_more<SP, GP, RECON, DAG, EPI>(L, st);
   }
+}
+
+template <int SP, int GP, int RECON, bool DAG, int EPI>
+static cudaError_t hop_var_more(const HopLaunch& L, cudaStream_t st) {
   if constexpr (SP == PREC_DOUBLE) {
     switch (L.variant) {
       case 4: return hop_go<SP, GP, RECON, DAG, EPI, 4>(L, st);

@@ -133,6 +133,8 @@ struct GaugeArrays {
   float4* s12;   // [2][4][3][Vh]
   uint4* h12a;   // [2][4][Vh]
   uint2* h12b;   // [2][4][Vh]
+  uint4* h18a;   // [2][4][Vh][2]: FP16 U00..U21 (all three rows stored)
+  uint32_t* h18b;  // [2][4][Vh]: FP16 U22
 };
 cudaError_t launch_import_gauge(const Geom& g, const double* raw, GaugeArrays ga,
                                 unsigned long long* maxdev_bits, cudaStream_t st);

@@ -578,6 +578,13 @@ __global__ void import_gauge_kernel(Geom g, const double* raw, GaugeArrays ga,
     hb.y = pack_h2(float(U.e[1][2].re), float(U.e[1][2].im));
     ga.h12a[base * Vh + hs] = ha;
     ga.h12b[base * Vh + hs] = hb;
+    uint32_t hw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      hw[k] = pack_h2(float(U.e[k / 3][k % 3].re), float(U.e[k / 3][k % 3].im));
+    ga.h18a[2 * (base * Vh + hs)] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    ga.h18a[2 * (base * Vh + hs) + 1] = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+    ga.h18b[base * Vh + hs] = pack_h2(float(U.e[2][2].re), float(U.e[2][2].im));
     // SU(3) check: rows 0,1 orthonormal and row 2 = conj(row0 x row1)
     Su3<double> W = U;
     reconstruct_row2(W);

@@ -4,7 +4,8 @@ subprocess): 12-RHS FP32/FP16 operators against the FP64 single-RHS operator,
 and a 12-RHS mixed-precision CG whose fused reductions drive the solve.
 Variants 4-7 are the two-right-hand-sides-per-thread kernel with four
 register caps, 8-9 the same with its neighbours staged through shared memory;
-FP64 variants 6-11 are 0-5 on the 18-real links."""
+FP64 variants 6-11 are 0-5 on the 18-real links; FP16 10-12 the
+mixed-precision kernel (FP16 x FP16 -> FP32 FMAs) on three-row FP16 links."""
 import json
 import os
 import subprocess
@@ -61,7 +62,7 @@ print("RESULT " + json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("variant", ["0,256", "4,256", "5,128", "6,128", "7,256", "8,128", "9,256", "10,128", "11,256"])
+@pytest.mark.parametrize("variant", ["0,256", "4,256", "5,128", "6,128", "7,256", "8,128", "9,256", "10,128", "11,256", "12,256"])
 def test_forced_variant(variant):
     env = dict(os.environ, IRO_HOP_VARIANT=variant)
     r = subprocess.run([sys.executable, "-c", SCRIPT, str(ROOT)], env=env, capture_output=True,
@@ -70,15 +71,17 @@ def test_forced_variant(variant):
     line = [l for l in r.stdout.splitlines() if l.startswith("RESULT ")][-1]
     res = json.loads(line[len("RESULT "):])
     v = int(variant.split(",")[0])
-    # the forced variant ran, modulo the variants each shape has: FP64 6 (12 on
-    # an SU(3) field, whose 18-real links are variants 6-11), FP32/FP16 10 with
-    # an even number of right-hand sides, else 4
+    # the forced variant ran: FP64 modulo 6 (12 on an SU(3) field, whose
+    # 18-real links are variants 6-11); otherwise modulo 13, a variant the
+    # shape lacks (4-9 need an even nrhs, 10-12 FP16) falling back modulo 4
     for t in res["autotune"]:
         if t["prec"] == 0:
-            nvar = 12 if t["recon"] == 12 else 6
+            exp = v % (12 if t["recon"] == 12 else 6)
         else:
-            nvar = 10 if t["nrhs"] % 2 == 0 else 4
-        assert t["variant"] == v % nvar, t
+            w = v % 13
+            ok = w < 4 or (w < 10 and t["nrhs"] % 2 == 0) or (w >= 10 and t["prec"] == 2)
+            exp = w if ok else w % 4
+        assert t["variant"] == exp, t
     for key, err in res["ops"].items():
         tol = TOL_FP32 if key.endswith("single") else TOL_FP16
         assert err < tol, (key, err)
