@@ -431,18 +431,21 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
     s.conv_iter = -1;
   }
   CK(cudaMemcpyAsync(state(c), hs.data(), sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
-  // FP64 r = b - A x; low-precision r, p; x_lo = 0
-  RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
-  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  // r = b - A x for x = b: only the inner iteration starts from this residual,
+  // and the first reliable update recomputes it in FP64 from the FP64 x (which
+  // is b exactly), so A x is applied in the inner precision; these launches
+  // also autotune the inner operator outside the graph capture.  Then the
+  // low-precision r and p, and x_lo = 0.
+  RC(convert(c, *B, *Pl));
+  RC(apply(c, op, mass, csw, false, *Pl, *Ql, nullptr, 0, nullptr));
+  RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, nullptr));
+  RC(convert(c, *Sl, *S));
   Reduce rinit = reduce(c, ST_CG_INIT, prm->max_iter);
   CK(launch_cg_init(PREC_DOUBLE, B->sites(), nrhs, B->all(), S->all(), R->all(), Q->all(), rinit,
                     max_blocks(c), st));
   RC(convert(c, *R, *Rl));
   RC(convert(c, *R, *Pl));
   RC(axpby(c, 0.0, *Rl, 0.0, *Rl, *Xl));
-  // autotune the low-precision operator launches outside the graph capture
-  RC(apply(c, op, mass, csw, false, *Pl, *Ql, nullptr, 0, nullptr));
-  RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, nullptr));
 
   const int* skip = done(c);
   Reduce ralpha = reduce(c, ST_CG_ALPHA, prm->max_iter);
