@@ -249,32 +249,34 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
       const R a = R(P.cst[r].alpha);
       Cx<R> rv[12];
       SpinorIO<SP>::load(P.cr[yi], tid, rv);
-      double rr = 0.0;
+      R rr = R(0);
 #pragma unroll
       for (int k = 0; k < 12; ++k) {
         rv[k] = rv[k] - a * acc[k];
-        rr += double(rv[k].re) * rv[k].re + double(rv[k].im) * rv[k].im;
+        rr += rv[k].re * rv[k].re + rv[k].im * rv[k].im;
       }
       SpinorIO<SP>::store(P.cr[yi], tid, rv);
-      red[0] += rr;
+      red[0] += double(rr);
       continue;
     }
     SpinorIO<SP>::store(P.out[yi], tid, acc);
+    // per-site sums in the arithmetic precision, accumulated in FP64 across
+    // sites (one conversion per sum instead of one per term)
     if (P.red_mask) {
-      double o2 = 0.0, x2 = 0.0, xo = 0.0;
+      R o2 = R(0);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) o2 += acc[k].re * acc[k].re + acc[k].im * acc[k].im;
+      red[0] += double(o2);
+    }
+    if ((EPI == EPI_XPAY || EPI == EPI_XPAY_CLOV) && (P.red_mask & (RED_X2 | RED_XOUT))) {
+      R x2 = R(0), xo = R(0);
 #pragma unroll
       for (int k = 0; k < 12; ++k) {
-        const double ar = acc[k].re, ai = acc[k].im;
-        o2 += ar * ar + ai * ai;
-        if (EPI == EPI_XPAY || EPI == EPI_XPAY_CLOV) {
-          const double xr = xv[k].re, xi = xv[k].im;
-          x2 += xr * xr + xi * xi;
-          xo += xr * ar + xi * ai;
-        }
+        x2 += xv[k].re * xv[k].re + xv[k].im * xv[k].im;
+        xo += xv[k].re * acc[k].re + xv[k].im * acc[k].im;
       }
-      red[0] += o2;
-      red[1] += x2;
-      red[2] += xo;
+      red[1] += double(x2);
+      red[2] += double(xo);
     }
   }
   if (P.red_mask || P.cg)
