@@ -257,14 +257,21 @@ struct SpinorIO<PREC_HALF> {
     for (int k = 0; k < 12; ++k) v[k] = n * v[k];
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i, const Cx<float> v[12]) {
+    store_scaled(s, i, v, 1.f);
+  }
+  // stores sc * v: the words are v / max|v| with the sign of sc, the norm
+  // |sc| max|v|
+  __device__ __forceinline__ static void store_scaled(const SpinorPtr& s, int64_t i, const Cx<float> v[12],
+                                                      float sc) {
     float m = 0.f;
 #pragma unroll
     for (int k = 0; k < 12; ++k) m = fmaxf(m, fmaxf(fabsf(v[k].re), fabsf(v[k].im)));
+    float n = m * fabsf(sc);
     // elements whose largest component is below the normal FP32 range are
     // stored as zero: 1/m would overflow (0 * inf = NaN), and such values are
     // far below FP16 resolution relative to any field they belong to
-    if (!(m >= 1e-37f)) m = 0.f;
-    const float inv = (m > 0.f) ? 1.0f / m : 0.f;
+    if (!(n >= 1e-37f) || !(m >= 1e-37f)) m = n = 0.f;
+    const float inv = (m > 0.f) ? copysignf(1.0f / m, sc) : 0.f;
     uint4* p = static_cast<uint4*>(s.data) + blk0<3>(i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -275,7 +282,7 @@ struct SpinorIO<PREC_HALF> {
       d.w = pack_h2(v[4 * k + 3].re * inv, v[4 * k + 3].im * inv);
       p[32 * k] = d;
     }
-    s.norm[i] = m;
+    s.norm[i] = n;
   }
 };
 

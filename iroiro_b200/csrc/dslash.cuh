@@ -202,10 +202,12 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
     for (int k = 0; k < 12; ++k) acc[k] = {R(0), R(0)};
     if constexpr ((VAR & 8) != 0) {
       static_assert(SP == PREC_HALF && RECON == 18, "mixed path: FP16 with three-row links");
-      hop_dir_mix<0, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
-      hop_dir_mix<1, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
-      hop_dir_mix<2, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
-      hop_dir_mix<3, DAG>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
+      const uint32_t vh = uint32_t(P.g.Vh);
+      const uint32_t lown = uint32_t(p * 4) * vh, lnb = uint32_t((1 - p) * 4) * vh;
+      hop_dir_mix<0, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<1, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<2, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<3, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
     } else if (VAR & 2) {
 #pragma unroll 1
       for (int mu = 0; mu < 4; ++mu) {
@@ -223,8 +225,13 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
       hop_dir<3, DAG, SP, GP, RECON>(P.gauge, P.in[yi], p, hs, nb, nrhs, r, acc);
     }
     const R sc = R(P.scale);
+    // the FP16 output of a plain hop takes the scale into the store's
+    // normalisation instead of multiplying every component
+    const bool fold = SP == PREC_HALF && EPI == EPI_SCALE && !P.cg;
+    if (!fold) {
 #pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
+      for (int k = 0; k < 12; ++k) acc[k] = sc * acc[k];
+    }
     if (EPI == EPI_SCALE_CLOV) {
       CloverBlock<R> B[2];
       CloverIO<CP>::load(P.clov[yi], hs, B);
@@ -259,14 +266,21 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
       red[0] += double(rr);
       continue;
     }
-    SpinorIO<SP>::store(P.out[yi], tid, acc);
+    if constexpr (SP == PREC_HALF && EPI == EPI_SCALE) {
+      if (fold)
+        SpinorIO<SP>::store_scaled(P.out[yi], tid, acc, sc);
+      else
+        SpinorIO<SP>::store(P.out[yi], tid, acc);
+    } else {
+      SpinorIO<SP>::store(P.out[yi], tid, acc);
+    }
     // per-site sums in the arithmetic precision, accumulated in FP64 across
     // sites (one conversion per sum instead of one per term)
     if (P.red_mask) {
       R o2 = R(0);
 #pragma unroll
       for (int k = 0; k < 12; ++k) o2 += acc[k].re * acc[k].re + acc[k].im * acc[k].im;
-      red[0] += double(o2);
+      red[0] += double(fold ? o2 * sc * sc : o2);
     }
     if ((EPI == EPI_XPAY || EPI == EPI_XPAY_CLOV) && (P.red_mask & (RED_X2 | RED_XOUT))) {
       R x2 = R(0), xo = R(0);

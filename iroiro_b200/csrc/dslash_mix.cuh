@@ -144,19 +144,28 @@ __device__ __forceinline__ void reconstruct_w(Cx<float> acc[12], const Cx<float>
   }
 }
 
-// FP16 links with the three rows stored (GaugeIO<PREC_HALF, 18>), as words
-__device__ __forceinline__ void load_link_w(const GaugePtr& g, int p, int mu, int64_t i, uint32_t u[9]) {
-  const int64_t j = int64_t(p * 4 + mu) * g.Vh + i;
-  const uint4 a = __ldg(static_cast<const uint4*>(g.a) + 2 * j);
-  const uint4 b = __ldg(static_cast<const uint4*>(g.a) + 2 * j + 1);
+// Addresses.  A context holds fewer than 2^31 elements (half-sites times
+// right-hand sides) and fewer than 2^30 links, so element and link indices
+// are formed in 32-bit arithmetic and widened only in the multiply that
+// scales them to bytes.
+
+// FP16 links with the three rows stored (GaugeIO<PREC_HALF, 18>), as words;
+// j = (parity * 4 + mu) * Vh + half-site
+__device__ __forceinline__ void load_link_w(const GaugePtr& g, uint32_t j, uint32_t u[9]) {
+  const uint4* pa = static_cast<const uint4*>(g.a) + 2 * size_t(j);
+  const uint4 a = __ldg(pa);
+  const uint4 b = __ldg(pa + 1);
   u[0] = a.x; u[1] = a.y; u[2] = a.z; u[3] = a.w;
   u[4] = b.x; u[5] = b.y; u[6] = b.z; u[7] = b.w;
   u[8] = __ldg(static_cast<const uint32_t*>(g.b) + j);
 }
 
-// the stored words and norm of an FP16 element
-__device__ __forceinline__ float load_raw_w(const SpinorPtr& s, int64_t i, uint32_t f[12]) {
-  const uint4* p = static_cast<const uint4*>(s.data) + blk0<3>(i);
+// the stored words and norm of FP16 element i: chunk 0 of a warp block of 32
+// elements sits at 16-byte unit (i / 32) * 96 + i % 32, i.e. at byte
+// 32 * (i & ~31) + 16 * i
+__device__ __forceinline__ float load_raw_w(const SpinorPtr& s, uint32_t i, uint32_t f[12]) {
+  const char* base = static_cast<const char*>(s.data);
+  const uint4* p = reinterpret_cast<const uint4*>(base + size_t(i & ~31u) * 32u + size_t(i) * 16u);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const uint4 d = __ldg(p + 32 * k);
@@ -168,24 +177,27 @@ __device__ __forceinline__ float load_raw_w(const SpinorPtr& s, int64_t i, uint3
   return __ldg(s.norm + i);
 }
 
-// forward and backward contributions of direction MU (as hop_dir)
+// forward and backward contributions of direction MU (as hop_dir); lown and
+// lnb are the link indices of direction 0 at parity p and 1 - p
+// ((p * 4) * Vh and ((1 - p) * 4) * Vh)
 template <int MU, bool DAG>
-__device__ __forceinline__ void hop_dir_mix(const GaugePtr& gauge, const SpinorPtr& in, int p, int hs,
-                                            const int nb[8], int nrhs, int r, Cx<float> acc[12]) {
+__device__ __forceinline__ void hop_dir_mix(const GaugePtr& gauge, const SpinorPtr& in, uint32_t lown,
+                                            uint32_t lnb, uint32_t vh, int hs, const int nb[8],
+                                            int nrhs, int r, Cx<float> acc[12]) {
   uint32_t u[9], f[12], h[6];
   Cx<float> g[6];
   {
     constexpr int S = DAG ? -1 : 1;
-    load_link_w(gauge, p, MU, hs, u);
-    const float n = load_raw_w(in, int64_t(nb[2 * MU]) * nrhs + r, f);
+    load_link_w(gauge, lown + MU * vh + uint32_t(hs), u);
+    const float n = load_raw_w(in, uint32_t(nb[2 * MU]) * uint32_t(nrhs) + uint32_t(r), f);
     project_w<MU, S>(f, h);
     su3_w<false>(u, h, g);
     reconstruct_w<MU, S>(acc, g, MU == 3 ? 2.f * n : n);
   }
   {
     constexpr int S = DAG ? 1 : -1;
-    load_link_w(gauge, 1 - p, MU, nb[2 * MU + 1], u);
-    const float n = load_raw_w(in, int64_t(nb[2 * MU + 1]) * nrhs + r, f);
+    load_link_w(gauge, lnb + MU * vh + uint32_t(nb[2 * MU + 1]), u);
+    const float n = load_raw_w(in, uint32_t(nb[2 * MU + 1]) * uint32_t(nrhs) + uint32_t(r), f);
     project_w<MU, S>(f, h);
     su3_w<true>(u, h, g);
     reconstruct_w<MU, S>(acc, g, MU == 3 ? 2.f * n : n);
