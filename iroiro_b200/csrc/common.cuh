@@ -170,6 +170,19 @@ __host__ __device__ __forceinline__ int64_t blk0(int64_t i) {
   return (i >> 5) * (NCHUNK * 32) + (i & 31);
 }
 
+// Device address of chunk 0 of element i of a blocked array of 16-byte
+// chunks, NCHUNK per element: unit (i & ~31) * NCHUNK + (i & 31) =
+// (i & ~31) * (NCHUNK - 1) + i, as blk0.  Element indices on the device stay
+// below 2^32 (a context holds fewer than 2^31 elements per parity), so the
+// index arithmetic is 32-bit and only the byte offset is widened.
+template <int NCHUNK, typename T>
+__device__ __forceinline__ T* chunk0(T* base, int64_t i) {
+  static_assert(sizeof(T) == 16, "16-byte chunks");
+  const uint32_t e = uint32_t(i);
+  const size_t off = size_t(e & ~31u) * (16u * (NCHUNK - 1)) + size_t(e) * 16u;
+  return reinterpret_cast<T*>(reinterpret_cast<uintptr_t>(base) + off);
+}
+
 // ---- spinor storage ------------------------------------------------------------
 enum Prec { PREC_DOUBLE = 0, PREC_SINGLE = 1, PREC_HALF = 2 };
 
@@ -187,7 +200,7 @@ struct SpinorIO<PREC_DOUBLE> {
   static constexpr int NCHUNK = 12;
   static constexpr int BYTES = 192;
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<double> v[12]) {
-    const double2* p = static_cast<const double2*>(s.data) + blk0<12>(i);
+    const double2* p = chunk0<12>(static_cast<const double2*>(s.data), i);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
       double2 d = __ldg(p + 32 * k);
@@ -195,7 +208,7 @@ struct SpinorIO<PREC_DOUBLE> {
     }
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i, const Cx<double> v[12]) {
-    double2* p = static_cast<double2*>(s.data) + blk0<12>(i);
+    double2* p = chunk0<12>(static_cast<double2*>(s.data), i);
 #pragma unroll
     for (int k = 0; k < 12; ++k) p[32 * k] = make_double2(v[k].re, v[k].im);
   }
@@ -207,7 +220,7 @@ struct SpinorIO<PREC_SINGLE> {
   static constexpr int NCHUNK = 6;
   static constexpr int BYTES = 96;
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
-    const float4* p = static_cast<const float4*>(s.data) + blk0<6>(i);
+    const float4* p = chunk0<6>(static_cast<const float4*>(s.data), i);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       float4 d = __ldg(p + 32 * k);
@@ -216,7 +229,7 @@ struct SpinorIO<PREC_SINGLE> {
     }
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i, const Cx<float> v[12]) {
-    float4* p = static_cast<float4*>(s.data) + blk0<6>(i);
+    float4* p = chunk0<6>(static_cast<float4*>(s.data), i);
 #pragma unroll
     for (int k = 0; k < 6; ++k)
       p[32 * k] = make_float4(v[2 * k].re, v[2 * k].im, v[2 * k + 1].re, v[2 * k + 1].im);
@@ -239,7 +252,7 @@ struct SpinorIO<PREC_HALF> {
   static constexpr int BYTES = 52;  // 48 bytes of FP16 + 4-byte norm
   // the stored (normalised) values and the element's norm
   __device__ __forceinline__ static float load_raw(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
-    const uint4* p = static_cast<const uint4*>(s.data) + blk0<3>(i);
+    const uint4* p = chunk0<3>(static_cast<const uint4*>(s.data), i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       uint4 d = __ldg(p + 32 * k);
@@ -249,7 +262,7 @@ struct SpinorIO<PREC_HALF> {
       v[4 * k + 2] = {c.x, c.y};
       v[4 * k + 3] = {e.x, e.y};
     }
-    return __ldg(s.norm + i);
+    return __ldg(s.norm + uint32_t(i));
   }
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i, Cx<float> v[12]) {
     const float n = load_raw(s, i, v);
@@ -272,7 +285,7 @@ struct SpinorIO<PREC_HALF> {
     // far below FP16 resolution relative to any field they belong to
     if (!(n >= 1e-37f) || !(m >= 1e-37f)) m = n = 0.f;
     const float inv = (m > 0.f) ? copysignf(1.0f / m, sc) : 0.f;
-    uint4* p = static_cast<uint4*>(s.data) + blk0<3>(i);
+    uint4* p = chunk0<3>(static_cast<uint4*>(s.data), i);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       uint4 d;
@@ -282,7 +295,7 @@ struct SpinorIO<PREC_HALF> {
       d.w = pack_h2(v[4 * k + 3].re * inv, v[4 * k + 3].im * inv);
       p[32 * k] = d;
     }
-    s.norm[i] = n;
+    s.norm[uint32_t(i)] = n;
   }
 };
 
@@ -311,6 +324,14 @@ __host__ __device__ __forceinline__ int64_t link0(int64_t Vh, int p, int mu, int
   return int64_t(p * 4 + mu) * Vh * NCHUNK + blk0<NCHUNK>(i);
 }
 
+// device address of chunk 0 of the link of half-site i, direction mu, parity
+// p (as link0; the parity/direction offset is uniform across a block)
+template <int NCHUNK, typename T>
+__device__ __forceinline__ T* link_chunk0(T* base, int64_t Vh, int p, int mu, int64_t i) {
+  const size_t pm = size_t(p * 4 + mu) * size_t(Vh) * (16u * NCHUNK);
+  return chunk0<NCHUNK>(reinterpret_cast<T*>(reinterpret_cast<uintptr_t>(base) + pm), i);
+}
+
 template <int P, int RECON>
 struct GaugeIO;
 
@@ -320,7 +341,7 @@ struct GaugeIO<PREC_DOUBLE, RECON> {
   static constexpr int NCHUNK = RECON / 2;
   static constexpr int BYTES = RECON * 8;
   __device__ __forceinline__ static void load(const GaugePtr& g, int p, int mu, int64_t i, Su3<double>& U) {
-    const double2* q = static_cast<const double2*>(g.a) + link0<NCHUNK>(g.Vh, p, mu, i);
+    const double2* q = link_chunk0<NCHUNK>(static_cast<const double2*>(g.a), g.Vh, p, mu, i);
 #pragma unroll
     for (int k = 0; k < NCHUNK; ++k) {
       double2 d = __ldg(q + 32 * k);
@@ -336,7 +357,7 @@ struct GaugeIO<PREC_SINGLE, 12> {
   static constexpr int NCHUNK = 3;
   static constexpr int BYTES = 48;
   __device__ __forceinline__ static void load(const GaugePtr& g, int p, int mu, int64_t i, Su3<float>& U) {
-    const float4* q = static_cast<const float4*>(g.a) + link0<3>(g.Vh, p, mu, i);
+    const float4* q = link_chunk0<3>(static_cast<const float4*>(g.a), g.Vh, p, mu, i);
     float4 a = __ldg(q), b = __ldg(q + 32), c = __ldg(q + 64);
     U.e[0][0] = {a.x, a.y};
     U.e[0][1] = {a.z, a.w};
@@ -354,7 +375,7 @@ struct GaugeIO<PREC_HALF, 12> {
   static constexpr int NCHUNK = 1;
   static constexpr int BYTES = 24;
   __device__ __forceinline__ static void load(const GaugePtr& g, int p, int mu, int64_t i, Su3<float>& U) {
-    const int64_t j = int64_t(p * 4 + mu) * g.Vh + i;
+    const uint32_t j = uint32_t(p * 4 + mu) * uint32_t(g.Vh) + uint32_t(i);
     uint4 a = __ldg(static_cast<const uint4*>(g.a) + j);
     uint2 b = __ldg(static_cast<const uint2*>(g.b) + j);
     float2 t;
@@ -389,7 +410,7 @@ struct CloverIO<PREC_DOUBLE> {
   using Real = double;
   static constexpr int BYTES = 576;
   __device__ __forceinline__ static void load(const CloverPtr& c, int64_t i, CloverBlock<double> B[2]) {
-    const double2* q = static_cast<const double2*>(c.data) + blk0<36>(i);
+    const double2* q = chunk0<36>(static_cast<const double2*>(c.data), i);
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
 #pragma unroll
@@ -412,7 +433,7 @@ struct CloverIO<PREC_SINGLE> {
   using Real = float;
   static constexpr int BYTES = 288;
   __device__ __forceinline__ static void load(const CloverPtr& c, int64_t i, CloverBlock<float> B[2]) {
-    const float4* q = static_cast<const float4*>(c.data) + blk0<18>(i);
+    const float4* q = chunk0<18>(static_cast<const float4*>(c.data), i);
     float v[72];
 #pragma unroll
     for (int k = 0; k < 18; ++k) {
@@ -437,7 +458,7 @@ struct CloverIO<PREC_HALF> {
   using Real = float;
   static constexpr int BYTES = 144;
   __device__ __forceinline__ static void load(const CloverPtr& c, int64_t i, CloverBlock<float> B[2]) {
-    const uint4* q = static_cast<const uint4*>(c.data) + blk0<9>(i);
+    const uint4* q = chunk0<9>(static_cast<const uint4*>(c.data), i);
     float v[72];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {

@@ -47,7 +47,7 @@ template <>
 struct PairIO<PREC_SINGLE> {
   // elements i0, i0+1 (i0 even); w = (1, 1)
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i0, Cp f[12], float2& w) {
-    const float4* p = static_cast<const float4*>(s.data) + blk0<6>(i0);
+    const float4* p = chunk0<6>(static_cast<const float4*>(s.data), i0);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       const float4 a = __ldg(p + 32 * k), b = __ldg(p + 32 * k + 1);
@@ -61,7 +61,7 @@ struct PairIO<PREC_SINGLE> {
     load(s, i0, f, w);
   }
   __device__ __forceinline__ static void store(const SpinorPtr& s, int64_t i0, const Cp v[12]) {
-    float4* p = static_cast<float4*>(s.data) + blk0<6>(i0);
+    float4* p = chunk0<6>(static_cast<float4*>(s.data), i0);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       const Cp a = v[2 * k], b = v[2 * k + 1];
@@ -75,7 +75,7 @@ template <>
 struct PairIO<PREC_HALF> {
   // the stored (normalised) values of elements i0, i0+1 and their norms w
   __device__ __forceinline__ static void load(const SpinorPtr& s, int64_t i0, Cp f[12], float2& w) {
-    const uint4* p = static_cast<const uint4*>(s.data) + blk0<3>(i0);
+    const uint4* p = chunk0<3>(static_cast<const uint4*>(s.data), i0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const uint4 a = __ldg(p + 32 * k), b = __ldg(p + 32 * k + 1);
@@ -86,7 +86,7 @@ struct PairIO<PREC_HALF> {
         f[4 * k + m] = {make_float2(x.x, y.x), make_float2(x.y, y.y)};
       }
     }
-    w = __ldg(reinterpret_cast<const float2*>(s.norm + i0));
+    w = __ldg(reinterpret_cast<const float2*>(s.norm + uint32_t(i0)));
   }
   __device__ __forceinline__ static void load_scaled(const SpinorPtr& s, int64_t i0, Cp f[12]) {
     float2 w;
@@ -105,7 +105,7 @@ struct PairIO<PREC_HALF> {
     if (!(m0 >= 1e-37f)) m0 = 0.f;
     if (!(m1 >= 1e-37f)) m1 = 0.f;
     const float2 inv = make_float2(m0 > 0.f ? 1.0f / m0 : 0.f, m1 > 0.f ? 1.0f / m1 : 0.f);
-    uint4* p = static_cast<uint4*>(s.data) + blk0<3>(i0);
+    uint4* p = chunk0<3>(static_cast<uint4*>(s.data), i0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       uint32_t a[4], b[4];
@@ -118,7 +118,7 @@ struct PairIO<PREC_HALF> {
       p[32 * k] = make_uint4(a[0], a[1], a[2], a[3]);
       p[32 * k + 1] = make_uint4(b[0], b[1], b[2], b[3]);
     }
-    *reinterpret_cast<float2*>(s.norm + i0) = make_float2(m0, m1);
+    *reinterpret_cast<float2*>(s.norm + uint32_t(i0)) = make_float2(m0, m1);
   }
 };
 
@@ -330,14 +330,14 @@ template <int SP>
 __device__ __forceinline__ void load_raw_pair(const SpinorPtr& s, int64_t i0, RawPair<SP>& r,
                                               float2& w) {
   constexpr int NC = SP == PREC_HALF ? 3 : 6;
-  const uint4* p = static_cast<const uint4*>(s.data) + blk0<NC>(i0);
+  const uint4* p = chunk0<NC>(static_cast<const uint4*>(s.data), i0);
 #pragma unroll
   for (int k = 0; k < NC; ++k) {
     r.v[2 * k] = __ldg(p + 32 * k);
     r.v[2 * k + 1] = __ldg(p + 32 * k + 1);
   }
   if constexpr (SP == PREC_HALF)
-    w = __ldg(reinterpret_cast<const float2*>(s.norm + i0));
+    w = __ldg(reinterpret_cast<const float2*>(s.norm + uint32_t(i0)));
   else
     w = bc(1.f);
 }

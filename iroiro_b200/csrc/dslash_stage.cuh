@@ -82,7 +82,7 @@ __device__ __forceinline__ void stage_issue(const GaugePtr& gauge, const SpinorP
   const int ls = BWD ? n : hs;
   const int64_t e0 = int64_t(n) * nrhs + r0;
   if constexpr (SP == PREC_HALF) {
-    const uint4* sp = static_cast<const uint4*>(in.data) + blk0<3>(e0);
+    const uint4* sp = chunk0<3>(static_cast<const uint4*>(in.data), e0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       cp_async16(slot_addr(base, S, 2 * k, NS), sp + 32 * k);
@@ -90,16 +90,16 @@ __device__ __forceinline__ void stage_issue(const GaugePtr& gauge, const SpinorP
     }
     const int64_t j = int64_t(lp * 4 + MU) * gauge.Vh + ls;
     cp_async16(slot_addr(base, S, 6, NS), static_cast<const uint4*>(gauge.a) + j);
-    cp_async8(slot_addr(base, S, 7, NS), in.norm + e0);
+    cp_async8(slot_addr(base, S, 7, NS), in.norm + uint32_t(e0));
     cp_async8(slot_addr(base, S, 7, NS) + 8, static_cast<const uint2*>(gauge.b) + j);
   } else {
-    const float4* sp = static_cast<const float4*>(in.data) + blk0<6>(e0);
+    const float4* sp = chunk0<6>(static_cast<const float4*>(in.data), e0);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       cp_async16(slot_addr(base, S, 2 * k, NS), sp + 32 * k);
       cp_async16(slot_addr(base, S, 2 * k + 1, NS), sp + 32 * k + 1);
     }
-    const float4* q = static_cast<const float4*>(gauge.a) + link0<3>(gauge.Vh, lp, MU, ls);
+    const float4* q = link_chunk0<3>(static_cast<const float4*>(gauge.a), gauge.Vh, lp, MU, ls);
 #pragma unroll
     for (int k = 0; k < 3; ++k) cp_async16(slot_addr(base, S, 12 + k, NS), q + 32 * k);
   }
