@@ -183,6 +183,13 @@ template <int SP, int GP, int RECON, bool DAG, int EPI, int CP, int VAR>
 __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::blocks)
     hop_kernel(HopParams P) {
   using R = typename SpinorIO<SP>::Real;
+  // Launched as a programmatic dependent launch (hop_go): wait until the
+  // previous kernel of the stream has completed and its writes are visible
+  // (its output is this launch's input; nothing global is read before), then
+  // allow the next launch to be scheduled as this grid's blocks retire.  In
+  // an ordinary launch both are no-ops.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;
   const int nrhs = P.nrhs;

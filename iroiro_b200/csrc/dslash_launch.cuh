@@ -34,9 +34,21 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks,
                            L.block_cap < HopBounds<VAR>::threads ? L.block_cap
                                                                  : HopBounds<VAR>::threads);
-  dim3 grid(c.grid, L.nparity);
-  hop_kernel<SP, GP, RECON, DAG, EPI, SP, VAR><<<grid, c.block, 0, st>>>(P);
-  return cudaGetLastError();
+  // programmatic dependent launch: the blocks of this grid may be scheduled
+  // while the previous kernel's last blocks retire (hop_kernel waits for
+  // that kernel's completion before it reads anything), hiding the launch
+  // gap between the dependent stencil launches of an operator
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(c.grid, L.nparity);
+  cfg.blockDim = dim3(c.block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, hop_kernel<SP, GP, RECON, DAG, EPI, SP, VAR>, P);
 }
 
 // two right-hand sides per thread (FP32/FP16, reconstruct-12, even nrhs)
