@@ -341,8 +341,11 @@ def batched_solves(torch, device):
     out["fp64_cg_12_sequential_ms"] = round(12 * seq["double"]["ms"], 2)
     out["fp64_cg_iterations"] = seq["double"]["iterations"]
     # reliable updates when |r| fell by 0.02 (6 FP64 residual recomputations to
-    # 1e-10, against 8 at 0.05, for 2-3 more iterations)
-    blk = timed_solves(ctx, D, src.ravel(), 12, torch, inners=("double", "single", "half"),
+    # 1e-10, against 8 at 0.05, for 2-3 more iterations).  The FP16 block solve
+    # is timed first, right after the FP64 baseline above, so that the two
+    # numbers compared both follow one warm-up solve; timed after the FP64 and
+    # FP32 block solves (seconds at the 1000 W cap) it ran at reduced clocks.
+    blk = timed_solves(ctx, D, src.ravel(), 12, torch, inners=("half", "single", "double"),
                        delta=0.02)
     out["reliable_update_delta"] = 0.02
     for k, v in blk.items():
