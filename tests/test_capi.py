@@ -38,6 +38,30 @@ def test_bad_lattice_rejected_without_device():
         assert lib.iro_ctx_create((ctypes.c_int * 4)(*L), 0, ctypes.byref(h)) == ib.BAD_ARG
 
 
+def test_element_count_bound_rejected_without_device():
+    # the device index arithmetic is 32-bit: a context holds fewer than 2^31
+    # elements per parity at 16 right-hand sides (Vh * 16 < 2^31)
+    import iroiro_b200 as ib
+    lib = ib.lib()
+    h = ctypes.c_void_p()
+    L = [128, 128, 128, 128]  # Vh * 16 = 2^31
+    assert lib.iro_ctx_create((ctypes.c_int * 4)(*L), 0, ctypes.byref(h)) == ib.BAD_ARG
+
+
+def test_chunk_address_formula():
+    # chunk 0 of element i of a blocked array with N 16-byte chunks per element
+    # (warp blocks of 32 elements) is at unit (i >> 5) * 32 N + (i & 31); the
+    # device computes it as (i & ~31) (N - 1) + i from a 32-bit i (at most
+    # 2 * Vh * 16 - 1 < 2^32 for a full-lattice field) with a 64-bit product
+    edge = [0, 1, 31, 32, 33, 2**31 - 1, 2**31, 2**31 + 31, 2**32 - 33, 2**32 - 1]
+    rng = np.random.default_rng(3)
+    idx = np.concatenate([np.array(edge, np.uint64), rng.integers(0, 2**32, 4096, dtype=np.uint64)])
+    for n in (3, 6, 9, 12, 18, 36):
+        blocked = (idx >> np.uint64(5)) * np.uint64(32 * n) + (idx & np.uint64(31))
+        device = (idx & np.uint64(0xFFFFFFE0)) * np.uint64(n - 1) + idx
+        assert np.array_equal(blocked, device), n
+
+
 def test_null_arguments_rejected():
     import iroiro_b200 as ib
     lib = ib.lib()
