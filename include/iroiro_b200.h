@@ -247,6 +247,16 @@ int iro_rational_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const d
 int iro_eo_invert(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
                   const double* src, double* sol, int nrhs, iro_solver_out* out);
 
+/* Qprop_EvenOdd::calc (lib/Measurements/FermionicM/qprop_EvenOdd.cpp:10-28)
+   on a Source_local (lib/Measurements/FermionicM/source_types.hpp:23-60):
+   the spin-colour point sources r = first .. first + nrhs - 1 (r = 3 s + c,
+   1 at the real part of spin s, colour c of lattice site `site`, SiteIndex
+   order x + Lx (y + Ly (z + Lz t))) are built on the device and inverted as
+   one block as iro_eo_invert does; sol receives the nrhs full-lattice
+   Format_F solutions in that order.  first + nrhs <= 12. */
+int iro_qprop_point(iro_ctx* ctx, int op, double mass, double csw, const iro_cg_params* prm,
+                    int64_t site, int first, int nrhs, double* sol, iro_solver_out* out);
+
 /* Molecular-dynamics force, FP64: the F with
    Re Tr(X F_mu(x)) = d/de Re(zeta^dag D(U_mu(x) -> (1 + e X) U_mu(x)) eta).
    op = IRO_OP_WILSON_FULL: Dirac_Wilson::md_force(eta, zeta)

@@ -121,6 +121,8 @@ def _declare(L):
                                       ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
         "iro_eo_invert": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
                               ctypes.POINTER(SolverOut)]),
+        "iro_qprop_point": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), ctypes.c_int64, I, I, _D,
+                                ctypes.POINTER(SolverOut)]),
         "iro_md_force": (I, [_VP, I, D, D, _D, _D, _D]),
         "iro_synth_gauge": (I, [L4, D, ctypes.c_uint64, I, _D]),
         "iro_synth_gaussian": (I, [ctypes.c_int64, ctypes.c_uint64, _D]),
@@ -784,16 +786,48 @@ class Qprop_EvenOdd:
         self.inv = Inverter_WilsonLike(D, solver)
         self.last_outputs = []
 
-    def calc(self, src) -> list:
-        if isinstance(src, (list, tuple)):
-            srcs = np.stack([_f64(f) for f in src])
+    def calc(self, src, s=None, c=None, out=None) -> list:
+        """The 12 solutions (s-major), or with s and c the one solution of
+        source (s, c) as the reference's calc(xq, src, s, c)
+        (qprop_EvenOdd.cpp:24-28).  The point sources of a Source_local are
+        built on the device (iro_qprop_point) instead of as host fields.
+        `out`, an array of (number of sources) * 24 * V doubles that the
+        caller keeps across calls (the reference's prop_t xq), receives the
+        solutions; the returned arrays are views of it."""
+        one = s is not None
+        nsrc = 1 if one else (len(src) if isinstance(src, (list, tuple)) else 12)
+        D, slv = self.inv.D, self.inv.slv
+        n = 24 * D.ctx.V
+        if out is not None:
+            o = _f64(out, n * nsrc, "out")
+            if not np.shares_memory(o, out):
+                raise IroError(BAD_ARG, "out must be a contiguous float64 array")
+        if isinstance(src, Source_local):
+            D.ctx.upload_gauge(D.u)
+            x = np.empty(n * nsrc) if out is None else o
+            outs = (SolverOut * nsrc)()
+            first = 3 * s + c if one else 0
+            rc = D.ctx._lib.iro_qprop_point(D.ctx.h, D.op, D.mass, D.csw, ctypes.byref(slv.params),
+                                            src.site, first, nsrc, _ptr(x), outs)
+            if rc not in (OK, NOT_CONVERGED):
+                D.ctx.check(rc, "iro_qprop_point")
+            res = [SolverOutput(o.diff, o.iterations, o.timing_ms, "CG solver", o.reliable_updates,
+                                o.operator_applies) for o in outs]
         else:
-            srcs = np.stack([src.mksrc(s, c) for s in range(4) for c in range(3)])
-        x, res, rc = self.inv.invert_many(srcs.ravel(), srcs.shape[0])
+            if isinstance(src, (list, tuple)):
+                srcs = np.stack([_f64(f) for f in src])
+            elif one:
+                srcs = src.mksrc(s, c)[None, :]
+            else:
+                srcs = np.stack([src.mksrc(sp, cp) for sp in range(4) for cp in range(3)])
+            x, res, rc = self.inv.invert_many(srcs.ravel(), nsrc)
+            if out is not None:
+                o.reshape(-1)[...] = x
+                x = o
         self.last_outputs = res
         if rc != OK:
             raise ConvergenceError(rc, "Qprop_EvenOdd: CG not converged")
-        return list(x.reshape(srcs.shape[0], -1))
+        return list(x.reshape(nsrc, -1))
 
 
 class Qprop:

@@ -121,6 +121,10 @@ cudaError_t launch_import_spinor(const Geom& g, const double* stage, int layout,
 cudaError_t launch_export_spinor(const Geom& g, double* stage, int layout, int p,
                                  int64_t host_sites, int nrhs, int prec, SpinorPtr in,
                                  cudaStream_t st);
+// F (a full-lattice FP64 field of F.nrhs right-hand sides) = the spin-colour
+// point sources r = first .. first + F.nrhs - 1 at half-site hs of parity p:
+// right-hand side j is 1 at the real part of spin-colour component first + j
+cudaError_t launch_point_sources(const DevField& F, int p, int64_t hs, int first, cudaStream_t st);
 // gamma5 on a Format_F staging buffer in place
 cudaError_t launch_gamma5_aos(double* stage, int64_t nsites, cudaStream_t st);
 

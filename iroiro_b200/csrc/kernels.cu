@@ -494,6 +494,20 @@ static int grid_for(int64_t n, int blk) {
   return int(g > 148 * 32 ? 148 * 32 : (g < 1 ? 1 : g));
 }
 
+__global__ void point_source_kernel(SpinorPtr s, int64_t hs, int nrhs, int first) {
+  const int j = threadIdx.x;
+  if (j < nrhs) chunk0<12>(static_cast<double2*>(s.data), hs * nrhs + j)[32 * (first + j)] = make_double2(1.0, 0.0);
+}
+
+cudaError_t launch_point_sources(const DevField& F, int p, int64_t hs, int first, cudaStream_t st) {
+  if (F.prec != PREC_DOUBLE || F.subset != 2 || hs < 0 || hs >= F.Vh || first < 0 || first + F.nrhs > 12)
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(F.data, 0, F.bytes_data, st);
+  if (e != cudaSuccess) return e;
+  point_source_kernel<<<1, 32, 0, st>>>(F.half(p), hs, F.nrhs, first);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_import_spinor(const Geom& g, const double* stage, int layout, int p,
                                  int64_t host_sites, int nrhs, int prec, SpinorPtr out,
                                  cudaStream_t st) {

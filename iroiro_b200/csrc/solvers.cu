@@ -606,23 +606,18 @@ DevField half_view(const DevField& F, int p) {
 //   x_o = A_oo^-1 (b_o - D_oe y_e),
 // and sol = (y_e, x_o) in the full Format_F layout.  out[] holds the CG's
 // outputs, as the reference prints its SolverOutput.
-extern "C" int iro_eo_invert(iro_ctx* c, int op, double mass, double csw,
-                             const iro_cg_params* prm, const double* src, double* sol, int nrhs,
-                             iro_solver_out* out) {
-  if (!c || !src || !sol || !out || nrhs < 1 || nrhs > 16 || !cg_args_ok(prm, op) ||
-      (op != IRO_OP_WILSON_SCHUR_EE && op != IRO_OP_CLOVER_SCHUR_EE))
-    return set_error(c, IRO_BAD_ARG, "bad e/o inverter arguments");
-  CK(cudaSetDevice(device(c)));
+namespace {
+// The e/o inversion of the nrhs full-lattice FP64 sources in F, in place:
+// F holds the solutions on return.
+int eo_invert_dev(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
+                  DevField* F, int nrhs, iro_solver_out* out) {
   const bool cl = op == IRO_OP_CLOVER_SCHUR_EE;
-  if (cl) RC(clover_ready(c, mass, csw));
   int rc = IRO_OK;
-  DevField* F = workspace(c, 2, PREC_DOUBLE, nrhs, 50, &rc); if (!F) return rc;
   DevField* BE = workspace(c, 0, PREC_DOUBLE, nrhs, 51, &rc); if (!BE) return rc;
   DevField* RHS = workspace(c, 0, PREC_DOUBLE, nrhs, 52, &rc); if (!RHS) return rc;
   DevField* YE = workspace(c, 0, PREC_DOUBLE, nrhs, 53, &rc); if (!YE) return rc;
   DevField* TO = workspace(c, 1, PREC_DOUBLE, nrhs, 54, &rc); if (!TO) return rc;
   cudaStream_t st = stream(c);
-  RC(import_field(c, src, true, *F));
   DevField fe = half_view(*F, 0), fo = half_view(*F, 1);
   // t_o = A_oo^-1 b_o;  be = b_e - D_eo t_o
   const DevField* bo = &fo;
@@ -644,6 +639,50 @@ extern "C" int iro_eo_invert(iro_ctx* c, int op, double mass, double csw,
   else
     RC(axpby(c, 1.0, *TO, 0.0, *TO, fo));
   RC(axpby(c, 1.0, *YE, 0.0, *YE, fe));
+  return solve_rc;
+}
+}  // namespace
+
+extern "C" int iro_eo_invert(iro_ctx* c, int op, double mass, double csw,
+                             const iro_cg_params* prm, const double* src, double* sol, int nrhs,
+                             iro_solver_out* out) {
+  if (!c || !src || !sol || !out || nrhs < 1 || nrhs > 16 || !cg_args_ok(prm, op) ||
+      (op != IRO_OP_WILSON_SCHUR_EE && op != IRO_OP_CLOVER_SCHUR_EE))
+    return set_error(c, IRO_BAD_ARG, "bad e/o inverter arguments");
+  CK(cudaSetDevice(device(c)));
+  if (op == IRO_OP_CLOVER_SCHUR_EE) RC(clover_ready(c, mass, csw));
+  int rc = IRO_OK;
+  DevField* F = workspace(c, 2, PREC_DOUBLE, nrhs, 50, &rc); if (!F) return rc;
+  RC(import_field(c, src, true, *F));
+  const int solve_rc = eo_invert_dev(c, op, mass, csw, prm, F, nrhs, out);
+  if (solve_rc != IRO_OK && solve_rc != IRO_NOT_CONVERGED) return solve_rc;
+  RC(export_field(c, *F, true, sol));
+  return solve_rc;
+}
+
+// Qprop_EvenOdd::calc (lib/Measurements/FermionicM/qprop_EvenOdd.cpp:10-28)
+// on the point sources of Source_local (source_types.hpp:23-60): source
+// r = 3 s + c is 1 at the real part of spin s, colour c of the lattice site
+// `site` (SiteIndex::site order, x fastest).  The sources r = first ..
+// first + nrhs - 1 are built on the device (the reference builds each one as
+// a host field) and inverted as one block; sol receives them in that order.
+extern "C" int iro_qprop_point(iro_ctx* c, int op, double mass, double csw,
+                               const iro_cg_params* prm, int64_t site, int first, int nrhs,
+                               double* sol, iro_solver_out* out) {
+  if (!c || !sol || !out || nrhs < 1 || first < 0 || first + nrhs > 12 || !cg_args_ok(prm, op) ||
+      (op != IRO_OP_WILSON_SCHUR_EE && op != IRO_OP_CLOVER_SCHUR_EE) || site < 0 ||
+      site >= volume(c))
+    return set_error(c, IRO_BAD_ARG, "bad point-source inverter arguments");
+  CK(cudaSetDevice(device(c)));
+  if (op == IRO_OP_CLOVER_SCHUR_EE) RC(clover_ready(c, mass, csw));
+  int rc = IRO_OK;
+  DevField* F = workspace(c, 2, PREC_DOUBLE, nrhs, 50, &rc); if (!F) return rc;
+  const Geom& g = geom(c);
+  const int64_t x = site % g.L[0], y = site / g.L[0] % g.L[1], z = site / (int64_t(g.L[0]) * g.L[1]) % g.L[2],
+                t = site / (int64_t(g.L[0]) * g.L[1] * g.L[2]);
+  CK(launch_point_sources(*F, int((x + y + z + t) & 1), site >> 1, first, stream(c)));
+  const int solve_rc = eo_invert_dev(c, op, mass, csw, prm, F, nrhs, out);
+  if (solve_rc != IRO_OK && solve_rc != IRO_NOT_CONVERGED) return solve_rc;
   RC(export_field(c, *F, true, sol));
   return solve_rc;
 }
