@@ -21,6 +21,9 @@ int apply_cg(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFie
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
 int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
 int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
+// host <-> device copies (large pageable ones through the context's pinned ring)
+int host_to_device(iro_ctx* c, void* dev, const void* host, size_t bytes);
+int device_to_host(iro_ctx* c, void* host, const void* dev, size_t bytes);
 int norms(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
           std::vector<double>* nw);
 int axpby(iro_ctx* c, double a, const DevField& x, double b, const DevField& y, DevField& v);
@@ -755,7 +758,5 @@ extern "C" int iro_md_force(iro_ctx* c, int op, double mass, double csw, const d
     CK(launch_force(g, U, recon, 1, E->half(0), B->half(1), 0, k, F, st));
     CK(launch_force(g, U, recon, 0, B->half(1), E->half(0), 1, k, F, st));
   }
-  CK(cudaMemcpyAsync(force, F, nF * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  return IRO_OK;
+  return device_to_host(c, force, F, nF * sizeof(double));
 }
