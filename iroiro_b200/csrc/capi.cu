@@ -161,15 +161,22 @@ bool host_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// the stripes no thread took (thread creation can fail) are copied by the caller
 void parallel_copy(void* dst, const void* src, size_t bytes) {
   const int nt = int(std::min<unsigned>(kCopyThreads, std::max(1u, std::thread::hardware_concurrency())));
   const size_t stripe = ((bytes / nt) + 63) & ~size_t(63);
-  std::vector<std::thread> th;
-  for (int k = 0; k < nt; ++k) {
+  auto part = [=](int k) {
     const size_t a = std::min(bytes, k * stripe), b = std::min(bytes, a + stripe);
-    if (b > a)
-      th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
+    if (b > a) std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a);
+  };
+  std::vector<std::thread> th;
+  int k = 1;
+  try {
+    for (; k < nt; ++k) th.emplace_back(part, k);
+  } catch (...) {
   }
+  part(0);
+  for (int j = k; j < nt; ++j) part(j);
   for (auto& t : th) t.join();
 }
 
