@@ -144,7 +144,7 @@ DevField* ws(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc) {
 
 // ---- host copies -----------------------------------------------------------------
 // The driver copies pageable host memory through its own staging on one host
-// thread (~21 GB/s for 4.8 GB device to host, measured on the B200 box).
+// thread (~21 GB/s for 4.8 GB device to host, measured on a B200 host).
 // Large copies to or from pageable memory go through two pinned chunks
 // instead: the DMA of one chunk overlaps the copy of the other, which
 // kCopyThreads host threads split (~46 GB/s measured).  Pinned (registered)

@@ -1,8 +1,8 @@
 """CPU oracle for the fermion-solve hot path -- TEST INFRASTRUCTURE ONLY.
 
 Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may load this package, and only as the checker: the product
-(``iroiro_b200``) never imports it.
+``bench.py`` may load this package, and only to check results against: the
+product (``iroiro_b200``) never imports it.
 
 Two implementations live here:
 

@@ -1,7 +1,7 @@
 /* CPU oracle: plain-C restatement of the reference's fermion-solve hot path.
  *
  * TEST INFRASTRUCTURE ONLY -- loaded by the tests, the smoke check and the
- * benchmark's CPU-baseline leg as the checker; never by the product.
+ * benchmark's CPU-baseline leg, to check results against; never by the product.
  *
  * Written for clarity, not speed: every operator is applied literally from
  * its definition with explicit 4x4 spin matrices, so that it checks the

@@ -2,8 +2,8 @@
 //
 // This file is compiled together with the reference's sources (read in place,
 // never copied) into oracle/_ref/libiroiro_ref.so by oracle/Makefile.  It is
-// the checker: tests, the golden-fixture script and the CPU baseline of
-// bench.py call it; the product never does.
+// test infrastructure: the tests, the golden-fixture script and the CPU
+// baseline of bench.py call it to check results against; the product never does.
 //
 // Every entry point takes plain host arrays in the reference's own layouts
 // (Format_F spinors, include/format_F.h:32-42; Format_G links,
