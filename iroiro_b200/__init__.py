@@ -42,6 +42,8 @@ __all__ = [
     "GaugeConf", "GaugeConf_bin", "GaugeConf_JLQCDLegacy", "GaugeConf_NERSC", "GaugeConf_ILDG",
     "GaugeConf_ILDG_FORTRAN", "GaugeConf_csdt", "GaugeConf_txt", "GaugeConf_unit", "GaugeInfo",
     "read_gauge", "save_on_disk", "plaquette", "link_trace",
+    "Source_local", "Inverter_WilsonLike", "Qprop_EvenOdd", "Qprop", "Qprop_MultiShift",
+    "RationalApprox", "RationalSolver_CG", "DeviceField",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -852,6 +854,31 @@ class Qprop:
         if rc != OK:
             raise ConvergenceError(rc, "Qprop: CG not converged")
         return list(x.reshape(len(srcs), -1))
+
+
+class Qprop_MultiShift:
+    """Qprop_MultiShift(D, solver) (lib/Measurements/FermionicM/qprop_MultiShift.hpp:20-42):
+    calc(src, mass_shifts) solves, source by source (s-major, as
+    qprop_MultiShift.cpp:11-31), (D^dag D + sigma_m) x_m = src.mksrc(s, c) for
+    every shift with the multishift solver and returns D x_m, one propagator
+    per source and shift (shift fastest).  The reference sizes its solution
+    vector to Nc * Nd = 12 whatever the number of shifts, so it returns 12
+    fields per source (the trailing ones zero when fewer shifts are given);
+    this returns one per shift."""
+
+    def __init__(self, D, solver: "MultiShiftSolver_CG"):
+        self.D, self.slv = D, solver
+        self.last_outputs = []
+
+    def calc(self, src, mass_shifts) -> list:
+        srcs = list(src) if isinstance(src, (list, tuple)) else \
+            [src.mksrc(s, c) for s in range(4) for c in range(3)]
+        out, self.last_outputs = [], []
+        for b in srcs:
+            xs = []
+            self.last_outputs.append(self.slv.solve(xs, b, mass_shifts))
+            out.extend(self.D.mult(x) for x in xs)
+        return out
 
 
 # gauge-configuration files (GaugeConf_*, CCIO::SaveOnDisk, Staples::plaquette)

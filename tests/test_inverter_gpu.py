@@ -96,6 +96,28 @@ def test_qprop_full_matches_evenodd(g):
         assert rel(xs[k], g["qprop_x"][k]) < TOL_SOL
 
 
+def test_qprop_multishift(g):
+    """Qprop_MultiShift: per source (s-major) and shift (fastest), D x_m with
+    (D^dag D + sigma_m) x_m = src.mksrc(s, c)."""
+    m = float(g["mass"])
+    L = [int(v) for v in g["L"]]
+    ctx = g["ctx"]
+    D = ib.Dirac_Wilson(m, g["u"], ctx=ctx)
+    shifts = [0.01, 0.3]
+    src = ib.Source_local([1, 2, 0, 3], L)
+    qp = ib.Qprop_MultiShift(D, ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-24, 5000))
+    props = qp.calc(src, shifts)
+    assert len(props) == 12 * len(shifts) and len(qp.last_outputs) == 12
+    for k in (0, 7, 11):
+        b = src.mksrc(k // 3, k % 3)
+        xs = []
+        ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-24, 5000).solve(xs, b, shifts)
+        for i, sig in enumerate(shifts):
+            Ax = ctx.apply(ib.OP_WILSON_FULL, m, 0.0, 1, ctx.apply(ib.OP_WILSON_FULL, m, 0.0, 0, xs[i])) + sig * xs[i]
+            assert rel(Ax, b) < 1e-10
+            assert rel(props[k * len(shifts) + i], D.mult(xs[i])) < 1e-14
+
+
 def test_clover_eo_invert_solves_full_clover(g):
     """No e/o clover in the reference: the inverter's solution must solve the
     reference-validated full clover operator and equal the oracle's
