@@ -2,27 +2,32 @@
 
 Workload (one "step"): one application of the even-odd Schur operator
 Dirac_Wilson_EvenOdd<Dirac_Wilson>::mult, M f_e = f_e - kappa^2 H_eo H_oe f_e
-(lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:80-84), on a 24^3x48 lattice, kappa =
+(lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:80-84), on a 32^3x64 lattice, kappa =
 0.12, seeded synthetic SU(3) links exp(i*0.2*H) followed by a random gauge
 transformation, FP64 storage and arithmetic (the reference's own arithmetic),
 reconstruct-12 links.  One step = two launches of the hopping kernel.
 
-value     algorithmic GB/s of the step, fields resident in HBM, L2 flushed
-          (256 MiB written) before every step, CUDA events on the launching
-          stream around each step; summed over ranks (replicas) / max time.
+value     GB/s of the step on compulsory bytes, fields resident in HBM, L2
+          flushed (256 MiB written) before every step, CUDA events on the
+          launching stream around each step; summed over ranks (replicas) /
+          max time.  Compulsory bytes per even site: 2496 = hop 1152 (4 own
+          links 384 + 4 neighbours' links 384 + input spinor 192 + output
+          192, each byte once) + hop 1152 + the f_e read (192) of the fused
+          f - x epilogue.  The model that counts every neighbour spinor and
+          link once per reading site (5184 B per even site) is reported as
+          roofline.algorithmic_GBps.
 e2e       the same metric through the C ABI with host buffers:
           iro_dirac_apply() on pinned Format_F arrays, H2D + D2H inside the
           timed region.
-roofline  achieved = algorithmic bytes per hopping launch / its mean
-          duration; bytes per even output site 2496 (8 neighbour spinors,
-          8 two-row links, 1 output spinor) for the first hop and 2688
-          (+ the f_e read of the fused x + a*y epilogue) for the second.
-solve     time to a 1e-10 FP64 true relative residual on the e/o Wilson-
-          clover Schur operator (csw=1.0) of the same field, for the
-          reference's FP64 CG and the mixed-precision reliable-update CG.
+roofline  achieved = compulsory bytes per step / mean step time; traffic =
+          DRAM bytes (read + write) of one step from the committed ncu
+          capture of this lattice, scaled by the sites processed.
+summary   (last key) the headline numbers of every configuration.
 
 --impl reference runs the reference's own C++ (compiled from its sources
-into oracle/_ref) on the host cores for the same metric, config and step.
+into oracle/_ref) on the host cores for the same metric, config and step, on
+inputs made by the oracle's copy of the generator (the product library is
+not loaded).
 """
 from __future__ import annotations
 
@@ -41,17 +46,30 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-L = [24, 24, 24, 48]
+L = [32, 32, 32, 64]          # headline lattice
+L_C2 = [24, 24, 24, 48]       # the Wilson-clover configuration's lattice
 KAPPA = 0.12
 MASS = 0.5 / KAPPA - 4.0
 CSW = 1.0
 EPS = 0.2
 SEED = 20240601
-BYTES_HOP = 2496          # FP64, reconstruct-12, per even/odd output site
-BYTES_XPAY = 192          # extra f_e read of the fused epilogue
+BYTES_HOP = 1152          # FP64 recon-12, per output site, each byte once
+BYTES_XPAY = 192          # f_e read of the fused epilogue
+BYTES_STEP = 2 * BYTES_HOP + BYTES_XPAY           # 2496 per even site
+BYTES_STEP_ALG = 2 * 2496 + 192                   # every neighbour counted per reader
 FLOPS_SCHUR = 2 * 1320 + 48
-METRIC = "EO-Wilson Dslash GB/s (FP64 Schur operator, algorithmic bytes)"
-WORKLOAD = "Dirac_Wilson_EvenOdd::mult 24^3x48, kappa=0.12, FP64, recon-12"
+METRIC = "EO-Wilson Dslash GB/s (% of HBM peak)"
+WORKLOAD = "Dirac_Wilson_EvenOdd::mult 32^3x64, kappa=0.12, FP64, recon-12"
+PROFILE_32 = "profiles/hop_fp64_32x32x32x64_dram.txt"
+
+
+def config_for(world: int) -> dict:
+    """The config object of the JSON line, identical in both arms."""
+    return {"workload": WORKLOAD, "lattice": L, "kappa": KAPPA, "eps": EPS,
+            "gauge_transform": True, "seed": SEED,
+            "bytes_model": "compulsory, 2496 B per even site",
+            "l2": "GPU arm: 256 MiB written before every step (fields 1.0 GB > 126 MB L2)",
+            "parallelism": f"replicas x{world}"}
 
 
 def _env_int(name, default):
@@ -182,15 +200,17 @@ def barrier(world: int):
         dist.barrier()
 
 
-def traffic_per_launch(vh: int):
+def traffic_per_step(vh: int):
     """DRAM bytes (read + write) of one Schur application (both hop launches)
-    from the committed ncu summary, scaled from the captured lattice to this
-    one by the sites processed."""
-    p = ROOT / "profiles" / "hop_fp64_24x24x24x48.txt"
+    from the committed ncu capture of the 32^3x64 lattice, scaled to `vh`
+    even sites by the sites processed; (bytes, source) or (None, None)."""
+    p = ROOT / PROFILE_32
     if not p.exists():
-        return None
-    m = re.search(r"^dram_bytes_per_site_schur:\s*([0-9.]+)", p.read_text(), re.M)
-    return float(m.group(1)) * vh if m else None
+        return None, None
+    m = re.search(r"^dram_bytes_per_site_schur_32x32x32x64:\s*([0-9.]+)", p.read_text(), re.M)
+    if not m:
+        return None, None
+    return float(m.group(1)) * vh, f"{PROFILE_32} (ncu, DRAM read+write per even site x sites)"
 
 
 def measured_peak():
@@ -203,6 +223,18 @@ def measured_peak():
 
 # ---- reference arm ----------------------------------------------------------------------
 
+REF_MAX_STEPS = 40   # a step takes about 3 s on the host at 32^3x64
+
+
+def ref_inputs():
+    """The headline's gauge field and source, made by the oracle's copy of the
+    generator (bit-identical to the product's), without the product library."""
+    import oracle
+    P = oracle.port()
+    V = int(np.prod(L))
+    return P.synth_gauge(L, EPS, SEED, True), P.synth_gaussian(V // 2, SEED + 100)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -211,32 +243,31 @@ def run_reference(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libiroiro_ref.so was not built (needs the reference tree)"}))
         return 0
-    import iroiro_b200 as ib
     V = int(np.prod(L))
-    u = ib.synth_gauge(L, EPS, SEED, gauge_transform=True)
-    f = ib.synth_gaussian(V // 2, SEED + 1)
+    u, f = ref_inputs()
     ref = oracle.ref()
     ref.init(L)
     threads = cpu_cores()
-    for _ in range(min(args.warmup, 2)):
+    warm = max(args.warmup, 3)
+    nsteps = max(1, min(args.steps, REF_MAX_STEPS))
+    for _ in range(warm):
         ref.eo_mult_throughput(u, MASS, f, threads, 1)
     t = 0.0
-    nsteps = max(1, min(args.steps, 20))  # bounded sample: a step takes ~1 s on the host
     for _ in range(nsteps):
         _, s = ref.eo_mult_throughput(u, MASS, f, threads, 1)
         t += s
-    steps_bytes = (2 * BYTES_HOP + BYTES_XPAY) * (V // 2) * threads * nsteps
-    val = steps_bytes / t / 1e9
+    step_bytes = BYTES_STEP * (V // 2) * threads
+    val = step_bytes * nsteps / t / 1e9
+    sample = (f"{threads} host threads, each one Dirac_Wilson_EvenOdd::mult per step on its own "
+              f"copy of the source ({nsteps} steps, at most {REF_MAX_STEPS})")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GB/s",
-        "n_gpus": args.gpus, "steps": nsteps, "warmup": min(args.warmup, 2),
+        "n_gpus": args.gpus, "steps": nsteps, "warmup": warm,
         "ms_per_step": round(1e3 * t / nsteps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "lattice": L, "kappa": KAPPA,
-                   "sample": f"{threads} concurrent Dirac_Wilson_EvenOdd::mult per step"},
+        "config": config_for(args.gpus),
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": threads,
-                         "kind": "reference",
-                         "sample": f"{threads} threads x 1 mult per step, {nsteps} steps (at most 20: one step takes about a second)"},
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -244,47 +275,34 @@ def run_reference(args, world, rank):
     return 0
 
 
-def schur_fp64_32(torch, device, steps, peak):
-    """FP64 e/o Wilson Schur operator at 32^3x64, L2 flushed before every
-    application, CUDA events on the launching stream; DRAM bytes per site
-    from the ncu summary of this lattice."""
+def schur_timing(torch, ctx, st, prec, op, csw, vh, steps, flush, nrhs=1, source=None):
+    """Mean event-timed ms of one Schur application (op, precision) on device
+    fields, L2 flushed before every application."""
     import iroiro_b200 as ib
-    Lb = [32, 32, 32, 64]
-    Vh = int(np.prod(Lb)) // 2
-    ctx = ib.Context(Lb, device)
-    st = torch.cuda.current_stream()
-    ctx.set_stream(st.cuda_stream)
-    ctx.upload_gauge(ib.synth_gauge(Lb, EPS, SEED + 5, gauge_transform=True), force=True)
-    a = ib.DeviceField(ctx, 0, "double").upload(ib.synth_gaussian(Vh, SEED + 6))
-    b = ib.DeviceField(ctx, 0, "double")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=torch.device("cuda", device))
     lib = ctx._lib
+    a = ib.DeviceField(ctx, 0, prec, nrhs).upload(
+        source if source is not None else ib.synth_gaussian(vh * nrhs, SEED + 6))
+    b = ib.DeviceField(ctx, 0, prec, nrhs)
     for _ in range(3):
-        ctx.check(lib.iro_dirac_apply_field(ctx.h, ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, a.h, b.h), "apply")
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, csw, 0, a.h, b.h), "apply")
     torch.cuda.synchronize()
-    n = max(10, min(steps, 500))
     tot = 0.0
-    for _ in range(n):
+    for _ in range(steps):
         flush.zero_()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(st)
-        ctx.check(lib.iro_dirac_apply_field(ctx.h, ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, a.h, b.h), "apply")
+        ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, csw, 0, a.h, b.h), "apply")
         e.record(st)
         e.synchronize()
         tot += s.elapsed_time(e)
-    ms = tot / n
-    alg = (2 * BYTES_HOP + BYTES_XPAY) * Vh / (ms * 1e-3) / 1e9
-    traffic = None
-    p = ROOT / "profiles" / "hop_fp64_32x32x32x64_dram.txt"
-    if p.exists():
-        m = re.search(r"^dram_bytes_per_site_schur_32x32x32x64:\s*([0-9.]+)", p.read_text(), re.M)
-        traffic = float(m.group(1)) * Vh if m else None
-    out = {"ms_per_op": round(ms, 4), "GBps": round(alg, 1), "frac_of_measured_hbm": round(alg / peak, 3)}
-    if traffic:
-        dram = traffic / (ms * 1e-3) / 1e9
-        out.update({"dram_GBps": round(dram, 1), "dram_frac_of_measured_hbm": round(dram / peak, 3)})
-    ctx.close()
-    return out
+    a.close()
+    b.close()
+    return tot / steps
+
+
+def variant_line(ms, bytes_per_site, vh, peak):
+    gbs = bytes_per_site * vh / (ms * 1e-3) / 1e9
+    return {"ms": round(ms, 4), "GBps": round(gbs, 1), "frac": round(gbs / peak, 3)}
 
 
 def timed_solves(ctx, D, b, nrhs, torch, inners=("double", "single", "half"), prec=1e-20,
@@ -364,7 +382,6 @@ def batched_solves(torch, device):
     torch.cuda.synchronize()
     out["multishift12"] = {"ms": round((time.perf_counter() - t0) * 1e3, 2), "iterations": o.Nconv,
                            "max_true_residual": o.diff}
-    out["autotune"] = ctx.autotune_report()
     ctx.close()
     return out
 
@@ -554,21 +571,17 @@ def mixed48(torch, device):
     del src
     out = {"op": "e/o Wilson-clover Schur 48^3x96, kappa=0.124, csw=1.0, eps=0.25, 12 Gaussian sources"}
     X64 = ib.DeviceField(ctx, 0, "double", 12)
-    # outside the timed solves: the clover set-up and the autotuning of the
-    # 12-RHS operator shapes of both precisions (D and D^dag)
-    lib = ctx._lib
-    for dag in (0, 1):
-        ctx.check(lib.iro_dirac_apply_field(ctx.h, D.op, mass, CSW, dag, B.h, X64.h), "apply")
-    # (FP16 scratch fields: the tuning only times the launch shapes)
-    H = [ib.DeviceField(ctx, 0, "half", 12) for _ in range(2)]
-    for dag in (0, 1):
-        ctx.check(lib.iro_dirac_apply_field(ctx.h, D.op, mass, CSW, dag, H[0].h, H[1].h), "apply")
-    for h in H:
-        h.close()
-    torch.cuda.synchronize()
     res = {}
     # (FP32 storage is left out here: its 12-RHS workspaces would not fit
     # beside the FP64 and FP16 ones and the clover terms in 180 GB)
+    # Outside the timed solves: the clover set-up, the autotuning of every
+    # operator shape on the real sources, the solver workspaces and graphs --
+    # one 16-iteration solve per precision.
+    for inner in ("double", "half"):
+        Xw = ib.DeviceField(ctx, 0, "double", 12)
+        ib.Solver_CG(1e-20, 16, ib.Fopr_DdagD(D), inner=inner, delta=0.1).solve_field(B, Xw)
+        Xw.close()
+    torch.cuda.synchronize()
     for inner, X in (("double", X64), ("half", None)):
         X = X or ib.DeviceField(ctx, 0, "double", 12)
         slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner, delta=0.1)
@@ -584,35 +597,34 @@ def mixed48(torch, device):
         if inner != "double":
             x = X.download().reshape(12, -1)
             x64 = X64.download().reshape(12, -1)
-            res[inner]["error_vs_fp64_per_rhs"] = [
-                float(np.linalg.norm(x[r] - x64[r]) / np.linalg.norm(x64[r])) for r in range(12)]
+            res[inner]["error_vs_fp64_max"] = max(
+                float(np.linalg.norm(x[r] - x64[r]) / np.linalg.norm(x64[r])) for r in range(12))
             res[inner]["speedup_vs_fp64_block_cg"] = round(res["double"]["ms"] / ms, 2)
             X.close()
     out.update(res)
-    out["note"] = ("single timed solve each, after the clover set-up and the operator autotuning; "
-                   "the solver workspaces are allocated inside the first call of each precision")
+    out["note"] = ("one timed solve each, after an untimed 16-iteration solve per precision "
+                   "(clover set-up, autotuning, workspaces, graphs)")
     ctx.close()
     return out
 
 
 def cpu_baseline_leg():
-    """The reference's own e/o mult on the host cores, a bounded sample."""
+    """The reference's own e/o mult on the host cores, a bounded sample of
+    the headline workload (inputs from the oracle's generator)."""
     import oracle
-    import iroiro_b200 as ib
     if not oracle.ref_available():
         return None
     V = int(np.prod(L))
-    u = ib.synth_gauge(L, EPS, SEED, gauge_transform=True)
-    f = ib.synth_gaussian(V // 2, SEED + 1)
+    u, f = ref_inputs()
     ref = oracle.ref()
     ref.init(L)
     threads = cpu_cores()
     ref.eo_mult_throughput(u, MASS, f, threads, 1)
     reps = 3
     _, s = ref.eo_mult_throughput(u, MASS, f, threads, reps)
-    val = (2 * BYTES_HOP + BYTES_XPAY) * (V // 2) * threads * reps / s / 1e9
+    val = BYTES_STEP * (V // 2) * threads * reps / s / 1e9
     return {"value": round(val, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
-            "sample": f"{threads} threads x {reps} Dirac_Wilson_EvenOdd::mult at 24^3x48 "
+            "sample": f"{threads} threads x {reps} Dirac_Wilson_EvenOdd::mult at 32^3x64 "
                       f"({s:.1f} s)"}
 
 
@@ -669,7 +681,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ck = clocks.stop()
     t_ms = sum(s.elapsed_time(e) for s, e in ev)
-    step_bytes = (2 * BYTES_HOP + BYTES_XPAY) * Vh
+    step_bytes = BYTES_STEP * Vh
     t_max = reduce_max(t_ms, world)
     value = replica_value(step_bytes, args.steps, t_ms, world)
     achieved = step_bytes / ((t_ms / args.steps) * 1e-3) / 1e9
@@ -698,96 +710,141 @@ def run_ours(args, world, rank, local):
     e2e_ms = reduce_max(es.elapsed_time(ee), world)
     e2e_val = world * step_bytes * args.steps / (e2e_ms * 1e-3) / 1e9
 
-    # FP32 / FP16 Schur and clover variants, same protocol (reported, not the headline)
+    # other precisions and operators, same protocol (reported, not the headline)
+    nvar = max(10, min(args.steps, 200))
     variants = {}
     for name, op, csw, prec, bps in (
-            ("wilson_fp32", ib.OP_WILSON_SCHUR_EE, 0.0, ib.PREC_SINGLE, 2 * 1248 + 96),
-            ("wilson_fp16", ib.OP_WILSON_SCHUR_EE, 0.0, ib.PREC_HALF, 2 * 660 + 52),
-            ("clover_fp64", ib.OP_CLOVER_SCHUR_EE, CSW, ib.PREC_DOUBLE, 2 * (2496 + 576) + 192),
-            ("clover_fp32", ib.OP_CLOVER_SCHUR_EE, CSW, ib.PREC_SINGLE, 2 * (1248 + 288) + 96)):
-        a, b = ctypes.c_void_p(), ctypes.c_void_p()
-        ctx.check(lib.iro_field_create(ctx.h, 0, prec, 1, ctypes.byref(a)), "field")
-        ctx.check(lib.iro_field_create(ctx.h, 0, prec, 1, ctypes.byref(b)), "field")
-        ctx.check(lib.iro_field_upload(ctx.h, a, h.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "up")
-        for _ in range(3):
-            ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, csw, 0, a, b), "apply")
-        torch.cuda.synchronize()
-        tot = 0.0
-        for _ in range(args.steps):
-            flush.zero_()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            ctx.check(lib.iro_dirac_apply_field(ctx.h, op, MASS, csw, 0, a, b), "apply")
-            e.record(stream)
-            e.synchronize()
-            tot += s.elapsed_time(e)
-        ms = tot / args.steps
-        variants[name] = {"ms_per_op": round(ms, 4), "GBps": round(bps * Vh / (ms * 1e-3) / 1e9, 1),
-                          "frac_of_measured_hbm": round(bps * Vh / (ms * 1e-3) / 1e9 / peak, 3)}
-        lib.iro_field_destroy(a)
-        lib.iro_field_destroy(b)
-
-    # the FP64 Schur operator on the 32^3x64 lattice (same protocol)
-    variants["wilson_fp64_32x32x32x64"] = schur_fp64_32(torch, local, args.steps, peak)
+            ("wilson_fp32", ib.OP_WILSON_SCHUR_EE, 0.0, "single", 2 * 576 + 96),
+            ("wilson_fp16", ib.OP_WILSON_SCHUR_EE, 0.0, "half", 2 * 296 + 52)):
+        ms = schur_timing(torch, ctx, stream, prec, op, csw, Vh, nvar, flush, source=h)
+        variants[name + "_32x32x32x64"] = variant_line(ms, bps, Vh, peak)
+    lib.iro_field_destroy(fin)
+    lib.iro_field_destroy(fout)
+    ctx.close()
+    # the Wilson-clover configuration's lattice: 24^3x48, gauge-transformed field
+    ctx2 = ib.Context(L_C2, local)
+    ctx2.set_stream(stream.cuda_stream)
+    u2 = ib.synth_gauge(L_C2, EPS, SEED + 1, gauge_transform=True)
+    ctx2.upload_gauge(u2, force=True)
+    Vh2 = int(np.prod(L_C2)) // 2
+    h2 = ib.synth_gaussian(Vh2, SEED + 101)
+    for name, op, csw, prec, bps in (
+            ("wilson_fp64", ib.OP_WILSON_SCHUR_EE, 0.0, "double", BYTES_STEP),
+            ("wilson_fp32", ib.OP_WILSON_SCHUR_EE, 0.0, "single", 2 * 576 + 96),
+            ("wilson_fp16", ib.OP_WILSON_SCHUR_EE, 0.0, "half", 2 * 296 + 52),
+            # + the clover blocks A_oo^-1 and A_ee, 72 reals per site each
+            ("clover_fp64", ib.OP_CLOVER_SCHUR_EE, CSW, "double", BYTES_STEP + 2 * 576),
+            ("clover_fp32", ib.OP_CLOVER_SCHUR_EE, CSW, "single", 2 * 576 + 96 + 2 * 288)):
+        ms = schur_timing(torch, ctx2, stream, prec, op, csw, Vh2, nvar, flush, source=h2)
+        variants[name + "_24x24x24x48"] = variant_line(ms, bps, Vh2, peak)
 
     # time to a 1e-10 FP64 true residual, e/o Wilson-clover, FP64 CG vs mixed
     # precision; fields resident on the device (iro_cg_solve_field)
     solve = {}
     if not args.no_solve:
-        D = ib.Dirac_Clover_EvenOdd(MASS, CSW, u, ctx=ctx)
-        solve = timed_solves(ctx, D, h, 1, torch)
+        D = ib.Dirac_Clover_EvenOdd(MASS, CSW, u2, ctx=ctx2)
+        solve = timed_solves(ctx2, D, h2, 1, torch)
         solve["op"] = "e/o Wilson-clover Schur 24^3x48, kappa=0.12, csw=1.0, one Gaussian source"
+    ctx2.close()
     batched = {}
     if not args.no_solve and not args.no_batched:
         batched = batched_solves(torch, local)
     learned_res = {}
     if not args.no_solve and not args.no_learned:
         learned_res = learned_solves(torch, local)
-    mixed = {}
-    if args.mixed48:
-        mixed = mixed48(torch, local)
     caller_res = {}
     if not args.no_solve and not args.no_callers:
         caller_res = callers(torch, local)
+    mixed = {}
+    if not args.no_solve and not args.no_mixed48:
+        mixed = mixed48(torch, local)
 
-    lib.iro_field_destroy(fin)
-    lib.iro_field_destroy(fout)
     if rank != 0:
         return 0
     cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline_leg()
-    traffic = traffic_per_launch(Vh)
+    traffic, traffic_src = traffic_per_step(Vh)
+    t_step = (t_ms / args.steps) * 1e-3
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3),
         "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "lattice": L, "kappa": KAPPA, "eps": EPS,
-                   "gauge_transform": True, "l2": "flushed (256 MiB write) before every step",
-                   "parallelism": f"replicas x{world}"},
+        "config": config_for(world),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic,
-                     "peak_kind": peak_kind,
-                     "dram_GBps": None if traffic is None else
-                     round(traffic / ((t_ms / args.steps) * 1e-3) / 1e9, 1),
+                     "traffic_source": traffic_src, "peak_kind": peak_kind,
+                     "dram_GBps": None if traffic is None else round(traffic / t_step / 1e9, 1),
                      "dram_frac": None if traffic is None else
-                     round(traffic / ((t_ms / args.steps) * 1e-3) / 1e9 / peak, 3),
-                     "bytes_model": "per even site: hop 2496 + hop 2496 + f_e 192 (FP64, recon-12)",
-                     "gflops": round(FLOPS_SCHUR * Vh / ((t_ms / args.steps) * 1e-3) / 1e9, 1)},
+                     round(traffic / t_step / 1e9 / peak, 3),
+                     "bytes_model": "compulsory per even site: hop 1152 + hop 1152 + f_e 192 "
+                                    "(FP64, recon-12)",
+                     "algorithmic_GBps": round(BYTES_STEP_ALG * Vh / t_step / 1e9, 1),
+                     "algorithmic_bytes_model": "5184 B per even site: 2 hops x (8 neighbour "
+                                                "spinors + 8 links + output) + f_e",
+                     "gflops": round(FLOPS_SCHUR * Vh / t_step / 1e9, 1)},
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": 24 * 8 * Vh,
                 "d2h_bytes_per_step": 24 * 8 * Vh, "ms_per_step": round(e2e_ms / args.steps, 3)},
         "gpu_launches": 2 * args.steps,
-        "autotune": ctx.autotune_report(),
         "clocks": ck,
+        "cpu_baseline": cpu,
         "variants": variants,
         "solve": solve,
-        "batched": batched,
         "learned": learned_res,
-        "mixed48": mixed,
         "callers": caller_res,
-        "cpu_baseline": cpu,
+        "mixed48": mixed,
+        "batched": batched,
     }
+    line["summary"] = summarise(line, peak)
     print(json.dumps(line))
     return 0
+
+
+def summarise(line, peak):
+    """The headline numbers of every configuration, short enough to survive
+    any truncation of the printed line (the last key)."""
+    g = lambda d, *k: _dig(d, k)  # noqa: E731
+    out = {"headline_32x32x32x64_fp64": {"ms": line["ms_per_step"], "GBps": line["value"],
+                                         "frac_of_measured_hbm": line["roofline"]["frac"],
+                                         "dram_frac": line["roofline"]["dram_frac"]}}
+    v = line["variants"]
+    out["schur_fp64_24x24x24x48_frac"] = g(v, "wilson_fp64_24x24x24x48", "frac")
+    out["clover_fp64_24x24x24x48_ms"] = g(v, "clover_fp64_24x24x24x48", "ms")
+    out["clover_solve_24x24x24x48_ms"] = {k: g(line["solve"], k, "ms") for k in ("double", "single", "half")}
+    b = line["batched"]
+    if b:
+        out["batched_32x32x32x64"] = {
+            "fp64_cg_12_sequential_ms": b.get("fp64_cg_12_sequential_ms"),
+            "block12_ms": {k: g(b, "block12", k, "ms") for k in ("half", "single", "double")},
+            "block12_half_speedup_vs_12_fp64_cg": g(b, "block12", "half", "speedup_vs_12_fp64_cg"),
+            "block12_half_residual": g(b, "block12", "half", "true_residual_max"),
+            "multishift12_ms": {k: g(b, "multishift12", k, "ms") for k in ("double", "single", "half")},
+            "multishift12_max_error_vs_fp64": {k: g(b, "multishift12", k, "max_error_vs_fp64")
+                                               for k in ("single", "half")}}
+    lr = line["learned"]
+    if lr:
+        out["learned_32x32x32x64_ms"] = {k: g(lr, k, "ms") for k in
+                                         ("gcr_network", "gcr_plain", "cg_double", "cg_single", "cg_half")}
+        out["learned_iterations"] = {k: g(lr, k, "iterations") for k in ("gcr_network", "cg_half")}
+        out["learned_network_apply_ms"] = lr.get("network_apply_ms")
+        out["gcr_network_vs_best_mixed_cg"] = lr.get("gcr_network_vs_best_mixed_cg")
+    m = line["mixed48"]
+    if m:
+        out["mixed48_clover_12rhs"] = {"fp64_ms": g(m, "double", "ms"), "fp16_ms": g(m, "half", "ms"),
+                                       "speedup": g(m, "half", "speedup_vs_fp64_block_cg"),
+                                       "max_error_vs_fp64": g(m, "half", "error_vs_fp64_max")}
+    c = line["callers"]
+    if c:
+        out["qprop_block12_half_speedup"] = g(c, "qprop_evenodd_32x32x32x64",
+                                              "speedup_block12_half_vs_sequential_fp64")
+    return out
+
+
+def _dig(d, keys):
+    for k in keys:
+        if not isinstance(d, dict) or k not in d:
+            return None
+        d = d[k]
+    return d
 
 
 def kernel_only(args):
@@ -903,8 +960,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-callers", action="store_true")
-    ap.add_argument("--mixed48", action="store_true",
-                    help="also run the 48^3x96 mixed-precision 12-RHS configuration (~1 min)")
+    ap.add_argument("--no-mixed48", action="store_true",
+                    help="skip the 48^3x96 mixed-precision 12-RHS configuration (~1 min)")
     ap.add_argument("--kernel", default=None, help="profiling driver: OP,PREC,NRHS")
     ap.add_argument("--lattice", default="24,24,24,48")
     args = ap.parse_args()

@@ -171,7 +171,9 @@ int iro_field_dot(iro_ctx* ctx, const iro_field* a, const iro_field* b, double* 
    process exits and shared by every call: calls that overlap on the GPU
    (different streams or threads at the same time) race and give wrong
    results.  The first call on a device looks up the array's device address
-   (cudaGetSymbolAddress); make that first call before any stream capture. */
+   (cudaGetSymbolAddress), and so does the first call after the device's
+   context has changed (cudaDeviceReset makes a new one); make those calls
+   before any stream capture. */
 int iro_norm_noalloc(const double* d_in, int64_t n, double* d_out, void* stream);
 
 /* ---- solvers -------------------------------------------------------------- */

@@ -36,24 +36,66 @@ static __device__ __align__(256) double g_scratch[kScratchDoubles];
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 double* g_address[kMaxDevices] = {};
+unsigned long long g_context_id[kMaxDevices] = {};
 
 __host__ __device__ inline unsigned* counter_of(double* scratch) {
   return reinterpret_cast<unsigned*>(scratch + kMaxBlocks);
 }
 
-// Device address of g_scratch on the current device, looked up once per
-// device with that device current.
+// Driver API entry points, resolved through the runtime so that the library
+// needs no link against libcuda: the ID of the current context, which is
+// unique for the life of the process.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    resolved = true;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Device address of g_scratch on the current device, looked up with that
+// device current the first time, and again whenever the device's context is
+// not the one the address was taken in (after a cudaDeviceReset the runtime
+// makes a new context, in which the old address means nothing).
 cudaError_t scratch_address(double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_mutex);
+  // cudaGetSymbolAddress also makes the device's context current if needed
   if (!g_address[dev]) {
     double* p = nullptr;
     e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_scratch);
     if (e != cudaSuccess) return e;
     g_address[dev] = p;
+    g_context_id[dev] = current_context_id();
+  } else {
+    const unsigned long long id = current_context_id();
+    if (id == 0 || id != g_context_id[dev]) {
+      double* p = nullptr;
+      e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_scratch);
+      if (e != cudaSuccess) return e;
+      g_address[dev] = p;
+      g_context_id[dev] = current_context_id();
+    }
   }
   *out = g_address[dev];
   return cudaSuccess;

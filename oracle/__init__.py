@@ -89,6 +89,8 @@ class Port:
         lib.orc_md_force.argtypes = [L4, _D, D, _I, _D, _D, _D]
         lib.orc_rational.argtypes = [L4, _D, _I, D, D, _D, _I, _D, _D, D, _D, D, _I, _D,
                                      ctypes.POINTER(_I)]
+        lib.orc_synth_gauge.argtypes = [L4, D, ctypes.c_ulonglong, _I, _D]
+        lib.orc_synth_gaussian.argtypes = [ctypes.c_longlong, ctypes.c_ulonglong, _D]
 
     @staticmethod
     def _L(L):
@@ -181,6 +183,34 @@ def _port_md_force(self, L, u, mass, eo, eta, zeta):
     return F
 
 
+def _port_synth_gauge(self, L, eps, seed, gauge_transform=False):
+    """The seeded exp(i eps H) field of the product's synth_gauge, bit for bit
+    (Format_G, 18*4*V doubles), without loading the product library."""
+    u = np.empty(72 * int(np.prod(L)))
+    if self.lib.orc_synth_gauge(self._L(L), float(eps), int(seed), int(gauge_transform), _p(u)):
+        raise ValueError(f"bad lattice {L}")
+    return u
+
+
+def _port_synth_gaussian(self, nsites, seed):
+    """N(0,1) in every real component of nsites Format_F sites, as the
+    product's synth_gaussian."""
+    f = np.empty(24 * int(nsites))
+    self.lib.orc_synth_gaussian(int(nsites), int(seed), _p(f))
+    return f
+
+
+def synth_point_sources(nsites, site):
+    """The 12 Source_local point sources at `site` (1.0 at index_r(c,s,site),
+    source_types.hpp:40-60), shape (12, 24*nsites)."""
+    f = np.zeros((12, 24 * int(nsites)))
+    for k in range(12):
+        f[k, 24 * int(site) + 2 * k] = 1.0
+    return f
+
+
+Port.synth_gauge = _port_synth_gauge
+Port.synth_gaussian = _port_synth_gaussian
 Port.eo_invert = _port_eo_invert
 Port.md_force = _port_md_force
 Port.rational = _port_rational

@@ -33,15 +33,22 @@ typedef struct {
   long* eo_site; /* [2][Vh] lexicographic site of the hs-th even/odd site */
   long* half_of; /* [V] hs of a site within its parity */
   int* parity;   /* [V] */
+  long* nb;      /* [V][8] neighbour along +dir (2*dir) and -dir (2*dir+1), periodic */
 } Geom;
 
-static void geom_init(Geom* g, const int L[4]) {
+/* The tables of the last lattice used stay cached: every operator call of a
+   solve would otherwise rebuild them. */
+static Geom g_cache;
+static int g_cache_valid = 0;
+
+static void geom_build(Geom* g, const int L[4]) {
   for (int d = 0; d < 4; ++d) g->L[d] = L[d];
   g->V = (long)L[0] * L[1] * L[2] * L[3];
   g->Vh = g->V / 2;
   g->eo_site = malloc(sizeof(long) * g->V);
   g->half_of = malloc(sizeof(long) * g->V);
   g->parity = malloc(sizeof(int) * g->V);
+  g->nb = malloc(sizeof(long) * 8 * g->V);
   long n[2] = {0, 0};
   for (long s = 0; s < g->V; ++s) {
     long r = s;
@@ -56,24 +63,44 @@ static void geom_init(Geom* g, const int L[4]) {
     g->eo_site[p * g->Vh + n[p]] = s;
     ++n[p];
   }
+#pragma omp parallel for schedule(static)
+  for (long s = 0; s < g->V; ++s) {
+    long c[4];
+    long r = s;
+    for (int d = 0; d < 4; ++d) {
+      c[d] = r % L[d];
+      r /= L[d];
+    }
+    for (int dir = 0; dir < 4; ++dir)
+      for (int k = 0; k < 2; ++k) {
+        long e[4] = {c[0], c[1], c[2], c[3]};
+        e[dir] = (e[dir] + (k ? -1 : 1) + L[dir]) % L[dir];
+        g->nb[8 * s + 2 * dir + k] = e[0] + L[0] * (e[1] + L[1] * (e[2] + L[2] * e[3]));
+      }
+  }
 }
 
-static void geom_free(Geom* g) {
-  free(g->eo_site);
-  free(g->half_of);
-  free(g->parity);
+static void geom_init(Geom* g, const int L[4]) {
+  int same = g_cache_valid;
+  for (int d = 0; d < 4 && same; ++d) same = g_cache.L[d] == L[d];
+  if (!same) {
+    if (g_cache_valid) {
+      free(g_cache.eo_site);
+      free(g_cache.half_of);
+      free(g_cache.parity);
+      free(g_cache.nb);
+    }
+    geom_build(&g_cache, L);
+    g_cache_valid = 1;
+  }
+  *g = g_cache;
 }
+
+static void geom_free(Geom* g) { (void)g; /* the cache owns the tables */ }
 
 /* neighbour of `site` one step along +dir (sgn=+1) or -dir (sgn=-1), periodic */
 static long neighbour(const Geom* g, long site, int dir, int sgn) {
-  long c[4];
-  long r = site;
-  for (int d = 0; d < 4; ++d) {
-    c[d] = r % g->L[d];
-    r /= g->L[d];
-  }
-  c[dir] = (c[dir] + sgn + g->L[dir]) % g->L[dir];
-  return c[0] + g->L[0] * (c[1] + g->L[1] * (c[2] + g->L[2] * c[3]));
+  return g->nb[8 * site + 2 * dir + (sgn < 0)];
 }
 
 /* ---- spin algebra ---------------------------------------------------------- */
@@ -153,6 +180,8 @@ static void hop_accumulate(const Geom* g, const double* u, int pout, const doubl
                            double* w) {
   spin_init();
   const long nout = pout < 0 ? g->V : g->Vh;
+  /* output sites are independent: threads change nothing in the result */
+#pragma omp parallel for schedule(static)
   for (long o = 0; o < nout; ++o) {
     const long x = pout < 0 ? o : g->eo_site[pout * g->Vh + o];
     for (int mu = 0; mu < 4; ++mu) {
@@ -296,6 +325,7 @@ int orc_field_strength(const int L[4], const double* u, int mu, int nu, double* 
   Geom g;
   geom_init(&g, L);
   M3* v = malloc(sizeof(M3) * g.V);
+#pragma omp parallel for schedule(static)
   for (long x = 0; x < g.V; ++x) {
     long xn = neighbour(&g, x, nu, 1), xm = neighbour(&g, x, mu, 1);
     M3 up = m3_mul(m3_mul(m3_load(u, g.V, x, nu), m3_load(u, g.V, xn, mu)),
@@ -307,6 +337,7 @@ int orc_field_strength(const int L[4], const double* u, int mu, int nu, double* 
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) v[x].a[a][b] = d1.a[a][b] - d2.a[a][b];
   }
+#pragma omp parallel for schedule(static)
   for (long x = 0; x < g.V; ++x) {
     long xm = neighbour(&g, x, mu, -1);
     M3 f1 = m3_ah(m3_mul(m3_load(u, g.V, x, mu), v[x]));
@@ -332,15 +363,21 @@ int orc_field_strength(const int L[4], const double* u, int mu, int nu, double* 
    w = Dw f - kappa*csw * sum_k F_k (S_k f), F = (Bx,By,Bz,Ex,Ey,Ez) =
    F(1,2),F(2,0),F(0,1),F(3,0),F(3,1),F(3,2) (set_csw, :139-162);
    mult_dag = gamma5 mult gamma5 (:351-353). */
-int orc_clover_full(const int L[4], const double* u, double mass, double csw, int dag,
-                    const double* in, double* out) {
-  spin_init();
+static double* clover_fields(const int L[4], const double* u) {
   static const int PAIRS[6][2] = {{1, 2}, {2, 0}, {0, 1}, {3, 0}, {3, 1}, {3, 2}};
+  const long V = (long)L[0] * L[1] * L[2] * L[3];
+  double* F = malloc(sizeof(double) * 18 * V * 6);
+  for (int k = 0; k < 6; ++k) orc_field_strength(L, u, PAIRS[k][0], PAIRS[k][1], F + 18 * V * k);
+  return F;
+}
+
+/* the clover operator with the six field strengths F already formed */
+static int clover_apply(const int L[4], const double* u, const double* F, double mass, double csw,
+                        int dag, const double* in, double* out) {
+  spin_init();
   Geom g;
   geom_init(&g, L);
   const long n = 24 * g.V;
-  double* F = malloc(sizeof(double) * 18 * g.V * 6);
-  for (int k = 0; k < 6; ++k) orc_field_strength(L, u, PAIRS[k][0], PAIRS[k][1], F + 18 * g.V * k);
   double* f = malloc(sizeof(double) * n);
   double* w = malloc(sizeof(double) * n);
   double* sw = calloc(n, sizeof(double));
@@ -349,6 +386,7 @@ int orc_clover_full(const int L[4], const double* u, double mass, double csw, in
   else
     memcpy(f, in, sizeof(double) * n);
   orc_wilson_full(L, u, mass, 0, f, w);
+#pragma omp parallel for schedule(static)
   for (long x = 0; x < g.V; ++x)
     for (int k = 0; k < 6; ++k)
       for (int s = 0; s < 4; ++s)
@@ -369,12 +407,19 @@ int orc_clover_full(const int L[4], const double* u, double mass, double csw, in
     orc_gamma5(g.V, w, out);
   else
     memcpy(out, w, sizeof(double) * n);
-  free(F);
   free(f);
   free(w);
   free(sw);
   geom_free(&g);
   return 0;
+}
+
+int orc_clover_full(const int L[4], const double* u, double mass, double csw, int dag,
+                    const double* in, double* out) {
+  double* F = clover_fields(L, u);
+  int rc = clover_apply(L, u, F, mass, csw, dag, in, out);
+  free(F);
+  return rc;
 }
 
 /* ---- solvers ----------------------------------------------------------------- */
@@ -386,6 +431,7 @@ typedef struct {
   double mass, csw;
   long n;
   double* tmp;
+  double* F; /* clover: the six field strengths, formed once per solve */
 } Opr;
 
 /* Fopr_DdagD::mult = D^dag (D f) (lib/Fopr/fopr.h:146-153) */
@@ -400,8 +446,8 @@ static void opr_apply(Opr* A, const double* in, double* out) {
       orc_wilson_eo(A->L, A->u, A->mass, 1, A->tmp, out);
       break;
     default:
-      orc_clover_full(A->L, A->u, A->mass, A->csw, 0, in, A->tmp);
-      orc_clover_full(A->L, A->u, A->mass, A->csw, 1, A->tmp, out);
+      clover_apply(A->L, A->u, A->F, A->mass, A->csw, 0, in, A->tmp);
+      clover_apply(A->L, A->u, A->F, A->mass, A->csw, 1, A->tmp, out);
       break;
   }
 }
@@ -421,6 +467,7 @@ static int opr_init(Opr* A, const int L[4], const double* u, int op, double mass
   A->csw = csw;
   A->n = (op == ORC_WILSON_EO) ? 12 * V : 24 * V;
   A->tmp = malloc(sizeof(double) * A->n);
+  A->F = (op == ORC_CLOVER_FULL) ? clover_fields(L, u) : NULL;
   return 0;
 }
 
@@ -466,6 +513,7 @@ int orc_cg(const int L[4], const double* u, int op, double mass, double csw, con
   free(p);
   free(s);
   free(A.tmp);
+  free(A.F);
   return *iters < 0 ? 1 : 0;
 }
 
@@ -555,6 +603,7 @@ int orc_multishift(const int L[4], const double* u, int op, double mass, double 
   free(csh2);
   free(pp);
   free(A.tmp);
+  free(A.F);
   return *nconv < 0 ? 1 : 0;
 }
 

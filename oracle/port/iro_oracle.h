@@ -41,6 +41,12 @@ int orc_rational(const int L[4], const double* u, int op, double mass, double cs
 int orc_md_force(const int L[4], const double* u, double mass, int eo, const double* eta,
                  const double* zeta, double* F);
 
+/* Seeded synthetic inputs, bit-identical to the product's iro_synth_gauge and
+   iro_synth_gaussian (port/synth.c), for code that must not load the product. */
+int orc_synth_gauge(const int L[4], double eps, unsigned long long seed, int gauge_transform,
+                    double* u);
+int orc_synth_gaussian(long long nsites, unsigned long long seed, double* f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,3 +58,15 @@ def test_point_sources():
     for k in range(12):
         nz = np.flatnonzero(s[k])
         assert list(nz) == [24 * 5 + 2 * k] and s[k, nz[0]] == 1.0
+
+
+def test_oracle_generator_is_bit_identical():
+    """The oracle's C generator (oracle/port/synth.c), which the reference arm
+    of the benchmark and the reference-side tests use so as not to load the
+    product library, gives the same bits as the product's."""
+    import oracle
+    P = oracle.port()
+    for L, gt in (([4, 4, 4, 8], False), ([6, 2, 4, 4], True), ([8, 8, 8, 16], True)):
+        assert np.array_equal(P.synth_gauge(L, 0.2, 123, gt), ib.synth_gauge(L, 0.2, 123, gt))
+    assert np.array_equal(P.synth_gaussian(1000, 5), ib.synth_gaussian(1000, 5))
+    assert np.array_equal(oracle.synth_point_sources(16, 5), ib.synth_point_sources(16, 5))
