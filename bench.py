@@ -373,15 +373,31 @@ def batched_solves(torch, device):
     # multishift, 12 shifts geometrically spaced 1e-4..10, one Gaussian source
     shifts = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
     g = ib.synth_gaussian(Vb // 2, SEED + 9)
-    ms = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 20000)
-    xs = []
-    ms.solve(xs, g, shifts)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    o = ms.solve(xs, g, shifts)
-    torch.cuda.synchronize()
-    out["multishift12"] = {"ms": round((time.perf_counter() - t0) * 1e3, 2), "iterations": o.Nconv,
-                           "max_true_residual": o.diff}
+    # FP64 (the reference's solver) against the mixed-precision one, on
+    # device-resident fields (source in, the 12 solutions out)
+    msr = {}
+    G = ib.DeviceField(ctx, 0, "double").upload(g)
+    XS = ib.DeviceField(ctx, 0, "double", 12)
+    x64 = None
+    for inner in ("double", "single", "half"):
+        ms = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 20000, inner=inner)
+        ms.solve_field(G, XS, shifts)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        o = ms.solve_field(G, XS, shifts)
+        torch.cuda.synchronize()
+        msr[inner] = {"ms": round((time.perf_counter() - t0) * 1e3, 2), "iterations": o.Nconv,
+                      "max_true_residual": o.diff, "reliable_updates": o.reliable_updates}
+        xs = XS.download().reshape(12, -1)
+        if inner == "double":
+            x64 = xs
+        else:
+            msr[inner]["max_error_vs_fp64"] = max(
+                float(np.linalg.norm(xs[k] - x64[k]) / np.linalg.norm(x64[k])) for k in range(12))
+            msr[inner]["speedup_vs_fp64"] = round(msr["double"]["ms"] / msr[inner]["ms"], 2)
+    G.close()
+    XS.close()
+    out["multishift12"] = msr
     ctx.close()
     return out
 
@@ -508,12 +524,12 @@ def callers(torch, device):
     out["qprop_evenodd_32x32x32x64"] = res
     ctx.close()
     # RationalSolver_CG and md_force at 24^3x48
-    ctx = ib.Context(L, device)
+    ctx = ib.Context(L_C2, device)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
-    u = ib.synth_gauge(L, EPS, SEED, gauge_transform=True)
+    u = ib.synth_gauge(L_C2, EPS, SEED, gauge_transform=True)
     ctx.upload_gauge(u, force=True)
     D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
-    Vh = int(np.prod(L)) // 2
+    Vh = int(np.prod(L_C2)) // 2
     b = ib.synth_gaussian(Vh, SEED + 11)
     poles = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
     ra = ib.RationalApprox(0.5, [0.1 / (k + 1) for k in range(12)], poles)
@@ -856,7 +872,8 @@ def kernel_only(args):
     import torch
     import iroiro_b200 as ib
     Lk = [int(v) for v in args.lattice.split(",")]
-    if args.kernel.startswith(("ptc,", "batched,")) or args.kernel in ("md_force_eo", "md_force_clover"):
+    if args.kernel.startswith(("ptc,", "batched,", "multishift,")) or \
+            args.kernel in ("md_force_eo", "md_force_clover"):
         return kernel_only_other(args, Lk)
     opn, prec, nrhs = args.kernel.split(",")
     nrhs = int(nrhs)
@@ -895,6 +912,31 @@ def kernel_only_other(args, Lk):
     from iroiro_b200 import learned
     V = int(np.prod(Lk))
     ctx = ib.Context(Lk, 0)
+    if args.kernel.startswith("multishift,"):
+        inner = args.kernel.split(",")[1]
+        st = torch.cuda.Stream()
+        torch.cuda.set_stream(st)
+        ctx.set_stream(st.cuda_stream)
+        u = ib.synth_gauge(Lk, EPS, SEED + 7, gauge_transform=False)
+        ctx.upload_gauge(u, force=True)
+        D = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+        g = ib.synth_gaussian(V // 2, SEED + 9)
+        shifts = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
+        ms = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 20000, inner=inner)
+        G = ib.DeviceField(ctx, 0, "double").upload(g)
+        XS = ib.DeviceField(ctx, 0, "double", 12)
+        ms.solve_field(G, XS, shifts)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        t0 = time.perf_counter()
+        o = ms.solve_field(G, XS, shifts)
+        torch.cuda.synchronize()
+        ms_t = (time.perf_counter() - t0) * 1e3
+        torch.cuda.profiler.stop()
+        print(json.dumps({"kernel": args.kernel, "lattice": Lk, "ms": round(ms_t, 2),
+                          "iterations": o.Nconv, "residual": o.diff,
+                          "reliable_updates": o.reliable_updates}))
+        return 0
     if args.kernel.startswith("batched,"):
         _, inner, delta = args.kernel.split(",")
         st = torch.cuda.Stream()

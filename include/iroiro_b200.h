@@ -226,6 +226,28 @@ int iro_multishift_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const
                             int nshift, const double* shifts, double* x, double precision,
                             int max_iter, iro_solver_out* out, int* nconv);
 
+/* MultiShiftSolver_CG::solve (lib/Solver/multiShiftSolver_CG.cpp:95-185) in
+   mixed precision: the same result contract as iro_multishift_cg_solve (every
+   shift to |b - (A + sigma_i) x_i|^2 / |b|^2 < precision in FP64), computed
+   as (1) the reference's multishift iteration on FP32 vectors with its FP64
+   zeta/alpha/beta recurrences and pruning, to a relative residual of 1e-6,
+   then (2) one block of reliable-update CG solves, one right-hand side per
+   shift, with inner_prec storage (IRO_PREC_SINGLE or IRO_PREC_HALF) and FP64
+   residual recomputations, refining every x_i from there.  inner_prec =
+   IRO_PREC_DOUBLE is iro_multishift_cg_solve.  Shifts ascending.  *nconv is
+   the phase-1 iterations plus the refinement's (-1 if not converged). */
+int iro_multishift_cg_solve_mixed(iro_ctx* ctx, int op, double mass, double csw, const double* b,
+                                  int nshift, const double* shifts, double* x, double precision,
+                                  int max_iter, int inner_prec, iro_solver_out* out, int* nconv);
+/* The same on device-resident fields: b an FP64 field of the operator's
+   subset with one right-hand side, x an FP64 field of that subset with
+   nshift right-hand sides (right-hand side i = the solution of shift i);
+   no host traffic.  inner_prec as above (IRO_PREC_DOUBLE: the FP64 solver). */
+int iro_multishift_cg_solve_field(iro_ctx* ctx, int op, double mass, double csw,
+                                  const iro_field* b, int nshift, const double* shifts,
+                                  iro_field* x, double precision, int max_iter, int inner_prec,
+                                  iro_solver_out* out, int* nconv);
+
 /* RationalSolver_CG::solve (lib/Solver/rationalSolver_CG.cpp:12-39):
    sol = c0 b + sum_i residues[i] (D^dagger D + poles[i])^-1 b, the shifted
    systems solved by iro_multishift_cg_solve's algorithm (poles ascending, at

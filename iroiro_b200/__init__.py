@@ -119,6 +119,10 @@ def _declare(L):
                                    ctypes.POINTER(SolverOut)]),
         "iro_multishift_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, I,
                                         ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
+        "iro_multishift_cg_solve_mixed": (I, [_VP, I, D, D, _D, I, _D, _D, D, I, I,
+                                              ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
+        "iro_multishift_cg_solve_field": (I, [_VP, I, D, D, _VP, I, _D, _VP, D, I, I,
+                                              ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
         "iro_rational_cg_solve": (I, [_VP, I, D, D, _D, I, _D, _D, D, _D, D, I,
                                       ctypes.POINTER(SolverOut), ctypes.POINTER(I)]),
         "iro_eo_invert": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
@@ -608,14 +612,19 @@ class Solver_CG:
 
 class MultiShiftSolver_CG:
     """MultiShiftSolver_CG(Fopr_DdagD(D), stop_cond, Niter)
-    (lib/Solver/multiShiftSolver_CG.hpp:61-65), FP64."""
+    (lib/Solver/multiShiftSolver_CG.hpp:61-65).  inner="double" is the
+    reference's FP64 solver; "single" or "half" the mixed-precision one
+    (FP32 multishift with FP64 recurrences, then a reliable-update CG
+    refinement of all shifts as one block in that storage), with the same
+    FP64 true-residual contract."""
 
-    def __init__(self, fopr: Fopr_DdagD, stop_cond: float, Niter: int):
+    def __init__(self, fopr: Fopr_DdagD, stop_cond: float, Niter: int, inner: str = "double"):
         if not isinstance(fopr, Fopr_DdagD) or fopr.D.op not in _SOLVER_OPS:
             raise IroError(BAD_ARG, "MultiShiftSolver_CG needs Fopr_DdagD of a full or Schur operator")
         self.fopr = fopr
         self.prec = float(stop_cond)
         self.niter = int(Niter)
+        self.inner = _PREC[inner]
 
     def solve(self, xq: list, b: np.ndarray, shifts) -> SolverOutput:
         """solve(vector_Field& x, const Field& b, const vector_double& shifts,
@@ -629,9 +638,10 @@ class MultiShiftSolver_CG:
         x = np.empty(n * sh.size)
         o = SolverOut()
         nconv = ctypes.c_int(-1)
-        rc = D.ctx._lib.iro_multishift_cg_solve(D.ctx.h, D.op, D.mass, D.csw, _ptr(b), sh.size,
-                                                _ptr(sh), _ptr(x), self.prec, self.niter,
-                                                ctypes.byref(o), ctypes.byref(nconv))
+        rc = D.ctx._lib.iro_multishift_cg_solve_mixed(D.ctx.h, D.op, D.mass, D.csw, _ptr(b),
+                                                      sh.size, _ptr(sh), _ptr(x), self.prec,
+                                                      self.niter, self.inner, ctypes.byref(o),
+                                                      ctypes.byref(nconv))
         D.ctx.check(rc, "iro_multishift_cg_solve")
         x = x.reshape(sh.size, n)
         for i in range(sh.size):
@@ -639,8 +649,26 @@ class MultiShiftSolver_CG:
                 xq[i][...] = x[i]
             else:
                 xq.append(x[i].copy())
-        out = SolverOutput(o.diff, o.iterations, o.timing_ms, "Multishift CG solver", 0,
-                           o.operator_applies)
+        out = SolverOutput(o.diff, o.iterations, o.timing_ms, "Multishift CG solver",
+                           o.reliable_updates, o.operator_applies)
+        out.Nconv = nconv.value
+        return out
+
+    def solve_field(self, b: "DeviceField", x: "DeviceField", shifts) -> SolverOutput:
+        """The solve on device-resident FP64 fields, without host traffic: b
+        one right-hand side, x one right-hand side per shift."""
+        D = self.fopr.D
+        D.ctx.upload_gauge(D.u)
+        sh = _f64(shifts)
+        o = SolverOut()
+        nconv = ctypes.c_int(-1)
+        rc = D.ctx._lib.iro_multishift_cg_solve_field(D.ctx.h, D.op, D.mass, D.csw, b.h, sh.size,
+                                                      _ptr(sh), x.h, self.prec, self.niter,
+                                                      self.inner, ctypes.byref(o),
+                                                      ctypes.byref(nconv))
+        D.ctx.check(rc, "iro_multishift_cg_solve_field")
+        out = SolverOutput(o.diff, o.iterations, o.timing_ms, "Multishift CG solver",
+                           o.reliable_updates, o.operator_applies)
         out.Nconv = nconv.value
         return out
 

@@ -112,7 +112,12 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
     for (int i = 0; i < 2; ++i) {
       P.cr[i] = L.cr[i];
     }
-    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
+    // the staging buffers of a block must fit the 227 KiB a block can opt in
+    // to (FP32: 976 B per thread, so at most 232 threads)
+    int cap = L.block_cap;
+    while (cap > 32 && stage_bytes<SP>() * cap > 232448) cap /= 2;
+    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, cap);
+    if (stage_bytes<SP>() * c.block > 232448) return cudaErrorInvalidValue;
     const int smem = stage_bytes<SP>() * c.block;
     static int opted = 0;  // largest dynamic shared memory already allowed
     if (smem > opted) {

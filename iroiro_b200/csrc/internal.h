@@ -92,15 +92,36 @@ cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr 
 cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r, SpinorPtr x,
                         const CGState* state, const int* done, cudaStream_t st);
 
-// Multishift (FP64): x0 -= beta p0; r += beta (s + sigma0 p0); reduce |r|^2
-cudaError_t launch_ms_xr(int64_t Vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
+// Multishift, vectors in FP64 or FP32 (prec), FP64 scalars:
+// x0 -= beta p0; r += beta (s + sigma0 p0); reduce |r|^2
+cudaError_t launch_ms_xr(int prec, int64_t Vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
                          const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st);
 // p0 = alpha p0 + r; x_k -= betas_k p_k; p_k = alphas_k p_k + zeta_k r; reduce |p_k|^2
 struct MSFields {
   SpinorPtr x[MAXSHIFT], p[MAXSHIFT];
 };
-cudaError_t launch_ms_p(int64_t Vh, int nshift, const MSFields& f, SpinorPtr r, const MSState* m,
-                        const Reduce& red, int max_blocks, cudaStream_t st);
+cudaError_t launch_ms_p(int prec, int64_t Vh, int nshift, const MSFields& f, SpinorPtr r,
+                        const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st);
+// x64_k += xlo_k (FP32), xlo_k = 0 for k < n
+cudaError_t launch_ms_merge(int64_t Vh, int n, const MSFields& x64, const MSFields& xlo,
+                            cudaStream_t st);
+// shifted CG: r -= alpha (s + sigma p) per rhs (CGState::alpha, ::sigma);
+// reduce |r|^2 (stage ST_CG_BETA)
+cudaError_t launch_cg_shift_r(int prec, int64_t Vh, int nrhs, SpinorPtr r, SpinorPtr s, SpinorPtr p,
+                              const CGState* state, const Reduce& red, int max_blocks,
+                              cudaStream_t st);
+// s += sigma_rhs x (FP64)
+cudaError_t launch_shift_add(int64_t sites, int nrhs, SpinorPtr s, SpinorPtr x, const CGState* state,
+                             cudaStream_t st);
+// FP64 block of ns right-hand sides from the single fields f.x[k] (prec)
+cudaError_t launch_ms_pack(int prec, int64_t sites, int ns, const MSFields& f, SpinorPtr out,
+                           cudaStream_t st);
+struct ShiftList {
+  double s[MAXSHIFT];
+};
+// r_k = b - s_k - sigma_k x_k (FP64 block, b a single field)
+cudaError_t launch_ms_block_residual(int64_t sites, int ns, SpinorPtr b, SpinorPtr s, SpinorPtr x,
+                                     const ShiftList& sg, SpinorPtr r, cudaStream_t st);
 
 // ---- mixed precision (reliable updates), masked by mask[rhs] != 0 ----------------
 cudaError_t launch_mx_merge(int plo, int64_t sites, int nrhs, SpinorPtr x64, SpinorPtr xlo,

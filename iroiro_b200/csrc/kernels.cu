@@ -365,83 +365,263 @@ cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r
   return cudaGetLastError();
 }
 
-// ---- multishift (FP64) -------------------------------------------------------------
+// ---- multishift ---------------------------------------------------------------------
+// The vectors in SP: FP64 for the reference's solver, FP32 in the first phase
+// of the mixed-precision solve; the scalars (MSState) are FP64 in both.
+// Per-site sums are formed in the arithmetic precision and accumulated in
+// FP64 (FP64 vectors: term by term, as before the FP32 phase existed).
+template <int SP>
+__device__ __forceinline__ void acc_norm(double& acc, const Cx<typename SpinorIO<SP>::Real> v[12]) {
+  using R = typename SpinorIO<SP>::Real;
+  if constexpr (SP == PREC_DOUBLE) {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc += v[k].re * v[k].re + v[k].im * v[k].im;
+  } else {
+    R a = R(0);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) a += v[k].re * v[k].re + v[k].im * v[k].im;
+    acc += double(a);
+  }
+}
+
 // multiShiftSolver_CG.cpp:49-59: x0 -= beta p0; r += beta s, s = A p0 + sigma0 p0
+template <int SP>
 __global__ void __launch_bounds__(256) ms_xr_kernel(int64_t vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
                              const MSState* m, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
   double acc = 0.0;
   if (!red.done[0]) {
-    const double beta = m->beta, s0 = m->sigma0;
+    const R beta = R(m->beta), s0 = R(m->sigma0);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
          i += int64_t(gridDim.x) * blockDim.x) {
-      Cx<double> xv[12], rv[12], pv[12], sv[12];
-      SpinorIO<PREC_DOUBLE>::load(x0, i, xv);
-      SpinorIO<PREC_DOUBLE>::load(r, i, rv);
-      SpinorIO<PREC_DOUBLE>::load(p0, i, pv);
-      SpinorIO<PREC_DOUBLE>::load(s, i, sv);
+      Cx<R> xv[12], rv[12], pv[12], sv[12];
+      SpinorIO<SP>::load(x0, i, xv);
+      SpinorIO<SP>::load(r, i, rv);
+      SpinorIO<SP>::load(p0, i, pv);
+      SpinorIO<SP>::load(s, i, sv);
 #pragma unroll
       for (int k = 0; k < 12; ++k) {
         sv[k] = sv[k] + s0 * pv[k];
         xv[k] = xv[k] - beta * pv[k];
         rv[k] = rv[k] + beta * sv[k];
-        acc += rv[k].re * rv[k].re + rv[k].im * rv[k].im;
       }
-      SpinorIO<PREC_DOUBLE>::store(x0, i, xv);
-      SpinorIO<PREC_DOUBLE>::store(r, i, rv);
+      acc_norm<SP>(acc, rv);
+      SpinorIO<SP>::store(x0, i, xv);
+      SpinorIO<SP>::store(r, i, rv);
     }
   }
   block_reduce_finish<1>(red, &acc, 1, blockIdx.x, gridDim.x);
 }
 
-cudaError_t launch_ms_xr(int64_t Vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
+cudaError_t launch_ms_xr(int prec, int64_t Vh, SpinorPtr x0, SpinorPtr r, SpinorPtr p0, SpinorPtr s,
                          const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st) {
   LaunchCfg c = launch_cfg(Vh, 1, max_blocks);
-  ms_xr_kernel<<<c.grid, c.block, 0, st>>>(Vh, x0, r, p0, s, m, red);
+  if (prec == PREC_DOUBLE)
+    ms_xr_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(Vh, x0, r, p0, s, m, red);
+  else if (prec == PREC_SINGLE)
+    ms_xr_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(Vh, x0, r, p0, s, m, red);
+  else
+    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
 // multiShiftSolver_CG.cpp:61-83: all shifts' x and p updated in one pass
+template <int SP>
 __global__ void __launch_bounds__(256) ms_p_kernel(int64_t vh, MSFields f, SpinorPtr r, const MSState* m, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
   double acc[MAXSHIFT];
 #pragma unroll
   for (int k = 0; k < MAXSHIFT; ++k) acc[k] = 0.0;
   if (!red.done[0]) {
     const int ns2 = m->nshift2;
-    const double alpha = m->alpha;
+    const R alpha = R(m->alpha);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
          i += int64_t(gridDim.x) * blockDim.x) {
-      Cx<double> rv[12], pv[12], xv[12];
-      SpinorIO<PREC_DOUBLE>::load(r, i, rv);
-      SpinorIO<PREC_DOUBLE>::load(f.p[0], i, pv);
+      Cx<R> rv[12], pv[12], xv[12];
+      SpinorIO<SP>::load(r, i, rv);
+      SpinorIO<SP>::load(f.p[0], i, pv);
 #pragma unroll
       for (int k = 0; k < 12; ++k) pv[k] = alpha * pv[k] + rv[k];
-      SpinorIO<PREC_DOUBLE>::store(f.p[0], i, pv);
+      SpinorIO<SP>::store(f.p[0], i, pv);
 #pragma unroll
       for (int sh = 1; sh < MAXSHIFT; ++sh) {
         if (sh >= ns2) break;
-        const double bs = m->betas[sh], as = m->alphas[sh], z = m->zeta[sh];
-        SpinorIO<PREC_DOUBLE>::load(f.p[sh], i, pv);
-        SpinorIO<PREC_DOUBLE>::load(f.x[sh], i, xv);
-        double a2 = 0.0;
+        const R bs = R(m->betas[sh]), as = R(m->alphas[sh]), z = R(m->zeta[sh]);
+        SpinorIO<SP>::load(f.p[sh], i, pv);
+        SpinorIO<SP>::load(f.x[sh], i, xv);
 #pragma unroll
         for (int k = 0; k < 12; ++k) {
           xv[k] = xv[k] - bs * pv[k];
           pv[k] = as * pv[k] + z * rv[k];
-          a2 += pv[k].re * pv[k].re + pv[k].im * pv[k].im;
         }
+        double a2 = 0.0;
+        acc_norm<SP>(a2, pv);
         acc[sh] += a2;
-        SpinorIO<PREC_DOUBLE>::store(f.x[sh], i, xv);
-        SpinorIO<PREC_DOUBLE>::store(f.p[sh], i, pv);
+        SpinorIO<SP>::store(f.x[sh], i, xv);
+        SpinorIO<SP>::store(f.p[sh], i, pv);
       }
     }
   }
   block_reduce_finish<MAXSHIFT>(red, acc, 1, blockIdx.x, gridDim.x);
 }
 
-cudaError_t launch_ms_p(int64_t Vh, int nshift, const MSFields& f, SpinorPtr r, const MSState* m,
-                        const Reduce& red, int max_blocks, cudaStream_t st) {
+cudaError_t launch_ms_p(int prec, int64_t Vh, int nshift, const MSFields& f, SpinorPtr r,
+                        const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st) {
   LaunchCfg c = launch_cfg(Vh, 1, max_blocks);
-  ms_p_kernel<<<c.grid, c.block, 0, st>>>(Vh, f, r, m, red);
+  if (prec == PREC_DOUBLE)
+    ms_p_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(Vh, f, r, m, red);
+  else if (prec == PREC_SINGLE)
+    ms_p_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(Vh, f, r, m, red);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// reliable update of the mixed-precision multishift: x64_k += xlo_k, xlo_k = 0
+// for the shifts k < n (FP32 accumulators into the FP64 solutions)
+__global__ void ms_merge_kernel(int64_t vh, int n, MSFields x64, MSFields xlo) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    for (int k = 0; k < n; ++k) {
+      Cx<double> a[12];
+      Cx<float> b[12], z[12];
+      SpinorIO<PREC_DOUBLE>::load(x64.x[k], i, a);
+      SpinorIO<PREC_SINGLE>::load(xlo.x[k], i, b);
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        a[j] = a[j] + Cx<double>{double(b[j].re), double(b[j].im)};
+        z[j] = {0.f, 0.f};
+      }
+      SpinorIO<PREC_DOUBLE>::store(x64.x[k], i, a);
+      SpinorIO<PREC_SINGLE>::store(xlo.x[k], i, z);
+    }
+  }
+}
+
+cudaError_t launch_ms_merge(int64_t Vh, int n, const MSFields& x64, const MSFields& xlo,
+                            cudaStream_t st) {
+  const int blk = 256;
+  ms_merge_kernel<<<stream_grid(Vh, blk), blk, 0, st>>>(Vh, n, x64, xlo);
+  return cudaGetLastError();
+}
+
+// ---- shifted CG (the refinement of the mixed-precision multishift solve) ----------
+// r -= alpha (s + sigma p) per right-hand side (s = A p from the operator, the
+// shift sigma from the right-hand side's CGState); reduce |r|^2 (stage
+// ST_CG_BETA).  Right-hand sides that have left the iteration are skipped.
+template <int SP>
+__global__ void __launch_bounds__(256) cg_shift_r_kernel(int64_t n, int nrhs, SpinorPtr r, SpinorPtr s,
+                                                       SpinorPtr p, const CGState* state, Reduce red) {
+  using R = typename SpinorIO<SP>::Real;
+  double acc = 0.0;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = i0 % nrhs;  // the block is a multiple of nrhs: one rhs per thread
+  if (!red.done[rhs]) {
+    const R a = R(state[rhs].alpha), sg = R(state[rhs].sigma);
+    for (int64_t i = i0; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+      Cx<R> rv[12], sv[12], pv[12];
+      SpinorIO<SP>::load(r, i, rv);
+      SpinorIO<SP>::load(s, i, sv);
+      SpinorIO<SP>::load(p, i, pv);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) rv[k] = rv[k] - a * (sv[k] + sg * pv[k]);
+      acc_norm<SP>(acc, rv);
+      SpinorIO<SP>::store(r, i, rv);
+    }
+  }
+  block_reduce_finish<1>(red, &acc, nrhs, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_cg_shift_r(int prec, int64_t Vh, int nrhs, SpinorPtr r, SpinorPtr s, SpinorPtr p,
+                              const CGState* state, const Reduce& red, int max_blocks,
+                              cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, nrhs, max_blocks);
+  const int64_t n = Vh * nrhs;
+  switch (prec) {
+    case PREC_DOUBLE: cg_shift_r_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(n, nrhs, r, s, p, state, red); break;
+    case PREC_SINGLE: cg_shift_r_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(n, nrhs, r, s, p, state, red); break;
+    default: cg_shift_r_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(n, nrhs, r, s, p, state, red); break;
+  }
+  return cudaGetLastError();
+}
+
+// s += sigma_rhs x over FP64 elements (the shift of the shifted operator in
+// the FP64 residual recomputations)
+__global__ void shift_add_kernel(int64_t n, int nrhs, SpinorPtr s, SpinorPtr x, const CGState* state) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const double sg = state[i % nrhs].sigma;
+    if (sg == 0.0) continue;
+    Cx<double> sv[12], xv[12];
+    SpinorIO<PREC_DOUBLE>::load(s, i, sv);
+    SpinorIO<PREC_DOUBLE>::load(x, i, xv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) sv[k] = sv[k] + sg * xv[k];
+    SpinorIO<PREC_DOUBLE>::store(s, i, sv);
+  }
+}
+
+cudaError_t launch_shift_add(int64_t sites, int nrhs, SpinorPtr s, SpinorPtr x, const CGState* state,
+                             cudaStream_t st) {
+  const int64_t n = sites * nrhs;
+  const int blk = 256;
+  shift_add_kernel<<<stream_grid(n, blk), blk, 0, st>>>(n, nrhs, s, x, state);
+  return cudaGetLastError();
+}
+
+// FP64 block field (right-hand side k = shift k) from the shifts' single fields
+// in precision SPI: out[hs * ns + k] = x_k[hs]
+template <int SPI>
+__global__ void ms_pack_kernel(int64_t sites, int ns, MSFields f, SpinorPtr out) {
+  using RI = typename SpinorIO<SPI>::Real;
+  const int64_t n = sites * ns;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const int k = int(i % ns);
+    Cx<RI> a[12];
+    Cx<double> b[12];
+    SpinorIO<SPI>::load(f.x[k], i / ns, a);
+    cvt12(a, b);
+    SpinorIO<PREC_DOUBLE>::store(out, i, b);
+  }
+}
+
+cudaError_t launch_ms_pack(int prec, int64_t sites, int ns, const MSFields& f, SpinorPtr out,
+                           cudaStream_t st) {
+  const int64_t n = sites * ns;
+  const int blk = 256;
+  if (prec == PREC_SINGLE)
+    ms_pack_kernel<PREC_SINGLE><<<stream_grid(n, blk), blk, 0, st>>>(sites, ns, f, out);
+  else if (prec == PREC_DOUBLE)
+    ms_pack_kernel<PREC_DOUBLE><<<stream_grid(n, blk), blk, 0, st>>>(sites, ns, f, out);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// r_k = b - s_k - sigma_k x_k over an FP64 block of ns right-hand sides (one
+// per shift), b a single FP64 field: the residuals of the shifted systems
+__global__ void ms_block_residual_kernel(int64_t sites, int ns, SpinorPtr b, SpinorPtr s, SpinorPtr x,
+                                         ShiftList sg, SpinorPtr r) {
+  const int64_t n = sites * ns;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const double sk = sg.s[i % ns];
+    Cx<double> bv[12], sv[12], xv[12];
+    SpinorIO<PREC_DOUBLE>::load(b, i / ns, bv);
+    SpinorIO<PREC_DOUBLE>::load(s, i, sv);
+    SpinorIO<PREC_DOUBLE>::load(x, i, xv);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) bv[k] = bv[k] - sv[k] - sk * xv[k];
+    SpinorIO<PREC_DOUBLE>::store(r, i, bv);
+  }
+}
+
+cudaError_t launch_ms_block_residual(int64_t sites, int ns, SpinorPtr b, SpinorPtr s, SpinorPtr x,
+                                     const ShiftList& sg, SpinorPtr r, cudaStream_t st) {
+  const int64_t n = sites * ns;
+  const int blk = 256;
+  ms_block_residual_kernel<<<stream_grid(n, blk), blk, 0, st>>>(sites, ns, b, s, x, sg, r);
   return cudaGetLastError();
 }
 

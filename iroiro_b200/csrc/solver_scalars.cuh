@@ -28,6 +28,7 @@ struct CGState {
   int iter;        // iterations completed
   int conv_iter;   // 0-based index of the converging iteration, -1 before
   int xpend;       // x += alpha p of the iteration just completed is still due
+  double sigma;    // shift of the operator A + sigma (0: the plain normal operator)
 };
 
 // done[] flag values
@@ -38,6 +39,8 @@ enum { RUNNING = 0, CONVERGED = 1, STOPPED = 2, PAUSED = 3 };
 constexpr int MAXSHIFT = 16;
 struct MSState {
   double rr, rrp, pap, alpha, beta, alphap, betap, snorm, prec, sigma0;
+  double maxrr;   // (r,r) at the last reliable update (mixed precision)
+  double delta2;  // reliable-update trigger delta^2; 0 for the FP64 solver
   int nshift, nshift2, iter, conv_iter;
   double csh2[MAXSHIFT], zeta1[MAXSHIFT], zeta2[MAXSHIFT], zeta[MAXSHIFT];
   double betas[MAXSHIFT], alphas[MAXSHIFT], pp[MAXSHIFT];
@@ -74,7 +77,9 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
       for (int r = 0; r < nrhs; ++r) {
         s[r].xpend = 0;  // the previous iteration's p update has run
         if (R.done[r]) continue;
-        s[r].pap = tot[r];
+        // shifted operator: (p, (A + sigma) p) = |M p|^2 + sigma |p|^2, the
+        // second total being the launch's |x|^2 (x = p in its epilogue)
+        s[r].pap = s[r].sigma != 0.0 ? tot[r] + s[r].sigma * tot[nrhs + r] : tot[r];
         s[r].alpha = s[r].rr / s[r].pap;
       }
     } break;
@@ -171,7 +176,13 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
       m->betap = m->beta;
       const int it = m->iter;
       m->iter = it + 1;
-      if (m->rr * m->snorm < m->prec) {
+      if (m->delta2 > 0.0) {
+        // mixed precision: pause for a reliable update of shift 0's
+        // residual when |r| fell by delta since the last one or looks
+        // converged; convergence is decided on the FP64 true residual
+        if (m->rr < m->delta2 * m->maxrr || m->rr * m->snorm < m->prec) R.done[0] = PAUSED;
+        else if (m->iter >= R.max_iter) R.done[0] = STOPPED;
+      } else if (m->rr * m->snorm < m->prec) {
         m->conv_iter = it;
         R.done[0] = 1;
       } else if (m->iter >= R.max_iter) {

@@ -189,8 +189,12 @@ int cg_double(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* 
 
 }  // namespace
 
+// sigma[r]: the shift of right-hand side r's operator (A + sigma); target[r]:
+// its squared relative residual goal instead of prm->precision (both
+// optional; the refinement of the mixed-precision multishift solve)
 int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
-             const DevField* B, DevField* X, int nrhs, iro_solver_out* out);
+             const DevField* B, DevField* X, int nrhs, iro_solver_out* out,
+             const double* sigma = nullptr, const double* target = nullptr);
 
 static int cg_any(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
                   const DevField* B, DevField* X, int nrhs, iro_solver_out* out) {
@@ -250,16 +254,17 @@ extern "C" int iro_cg_solve_field(iro_ctx* c, int op, double mass, double csw,
 // MultiShiftSolver_CG::solve (lib/Solver/multiShiftSolver_CG.cpp:95-185) in FP64.
 // The solve itself; the shifted solutions stay in the context's workspaces
 // (*xs_out), and are exported to x when x is given.
-static int ms_run(iro_ctx* c, int op, double mass, double csw, const double* b, int nshift,
-                  const double* shifts, double* x, double precision, int max_iter,
-                  iro_solver_out* out, int* nconv, std::vector<DevField*>* xs_out,
-                  DevField** b_out) {
+// B: the FP64 source on the device.  The solutions go to the host array x
+// (nshift consecutive fields) and/or the FP64 block field xblock (right-hand
+// side k = shift k) when given.
+static int ms_run(iro_ctx* c, int op, double mass, double csw, const DevField* B, int nshift,
+                  const double* shifts, double* x, DevField* xblock, double precision,
+                  int max_iter, iro_solver_out* out, int* nconv, std::vector<DevField*>* xs_out) {
   CK(cudaSetDevice(device(c)));
   auto t0 = std::chrono::steady_clock::now();
   const int sub = op_subset(op);
   const bool full = op_is_full(op);
   int rc = IRO_OK;
-  DevField* B = workspace(c, sub, PREC_DOUBLE, 1, 30, &rc); if (!B) return rc;
   DevField* R = workspace(c, sub, PREC_DOUBLE, 1, 31, &rc); if (!R) return rc;
   DevField* S = workspace(c, sub, PREC_DOUBLE, 1, 32, &rc); if (!S) return rc;
   DevField* Q = workspace(c, sub, PREC_DOUBLE, 1, 33, &rc); if (!Q) return rc;
@@ -269,7 +274,6 @@ static int ms_run(iro_ctx* c, int op, double mass, double csw, const double* b, 
     PS[k] = workspace(c, sub, PREC_DOUBLE, 1, 40 + MAXSHIFT + k, &rc); if (!PS[k]) return rc;
   }
   cudaStream_t st = stream(c);
-  RC(import_field(c, b, full, *B));
   std::vector<double> bn;
   RC(norms(c, *B, nullptr, bn, nullptr));
   // solve_init (multiShiftSolver_CG.cpp:10-32): p_i = b, x_i = 0, r = b
@@ -313,9 +317,9 @@ static int ms_run(iro_ctx* c, int op, double mass, double csw, const double* b, 
     for (int i = 0; i < n; ++i) {
       RC(apply(c, op, mass, csw, false, *PS[0], *Q, &ralpha, RED_OUT2 | RED_X2, skip));
       RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
-      CK(launch_ms_xr(B->sites(), XS[0]->all(), R->all(), PS[0]->all(), S->all(), dm, rr,
-                      max_blocks(c), st));
-      CK(launch_ms_p(B->sites(), nshift, f, R->all(), dm, rpp, max_blocks(c), st));
+      CK(launch_ms_xr(PREC_DOUBLE, B->sites(), XS[0]->all(), R->all(), PS[0]->all(), S->all(), dm,
+                      rr, max_blocks(c), st));
+      CK(launch_ms_p(PREC_DOUBLE, B->sites(), nshift, f, R->all(), dm, rpp, max_blocks(c), st));
     }
     return IRO_OK;
   };
@@ -336,8 +340,8 @@ static int ms_run(iro_ctx* c, int op, double mass, double csw, const double* b, 
     const size_t nfield = size_t(24) * size_t(full ? 2 * vh(c) : vh(c));
     if (x) RC(export_field(c, *XS[k], full, x + size_t(k) * nfield));
   }
+  if (xblock) CK(launch_ms_pack(PREC_DOUBLE, B->sites(), nshift, f, xblock->all(), st));
   if (xs_out) *xs_out = XS;
-  if (b_out) *b_out = B;
   auto t1 = std::chrono::steady_clock::now();
   out->diff = std::sqrt(dmax);
   out->iterations = m.conv_iter;
@@ -361,8 +365,287 @@ extern "C" int iro_multishift_cg_solve(iro_ctx* c, int op, double mass, double c
                                        iro_solver_out* out, int* nconv) {
   if (!x || !ms_args_ok(c, op, b, nshift, shifts, precision, out, nconv))
     return set_error(c, IRO_BAD_ARG, "bad multishift arguments");
-  return ms_run(c, op, mass, csw, b, nshift, shifts, x, precision, max_iter, out, nconv, nullptr,
+  CK(cudaSetDevice(device(c)));
+  int rc = IRO_OK;
+  DevField* B = workspace(c, op_subset(op), PREC_DOUBLE, 1, 30, &rc); if (!B) return rc;
+  RC(import_field(c, b, op_is_full(op), *B));
+  return ms_run(c, op, mass, csw, B, nshift, shifts, x, nullptr, precision, max_iter, out, nconv,
                 nullptr);
+}
+
+// ---- mixed-precision multishift ------------------------------------------------------
+// MultiShiftSolver_CG::solve with the Krylov vectors in FP32: FP64 is kept
+// for the zeta/alpha/beta recurrences (MSState, the reference's update order
+// as in ms_run), the reductions, the residual recomputations and the
+// solutions.
+//   1. The reference's multishift iteration on FP32 vectors (r, p_k and
+//      per-shift FP32 accumulators of x_k) and the FP32 operator, with
+//      reliable updates on shift 0 (Sleijpen & van der Vorst; for multishift
+//      on GPUs, Clark et al., "Solving lattice QCD systems of equations using
+//      mixed precision solvers on GPUs", CPC 181 (2010)): when |r| fell by
+//      delta since the last update, or looks converged, the accumulators are
+//      added to the FP64 solutions and r = b - (A + sigma_0) x_0 is
+//      recomputed in FP64; shift 0 converges on that FP64 residual.
+//   2. r_k = b - (A + sigma_k) x_k in FP64 for every shift: after the first
+//      update the shifted residuals are no longer exactly collinear with r, so
+//      the shifted systems stop near the FP32 rounding level.
+//   3. A reliable-update CG on (A + sigma_k) e_k = r_k for the shifts above
+//      the goal, all of them as ONE block of right-hand sides, each to
+//      |r_k - (A + sigma_k) e_k|^2 < precision |b|^2; x_k += e_k.  This
+//      takes a few iterations: the remaining residuals are rounding noise,
+//      not unconverged low modes.
+//   4. The FP64 true residual of every shift.
+namespace {
+// reliable-update trigger of the FP32 multishift: every two decades (the
+// shifted systems' accuracy does not depend on it, the number of FP64
+// recomputations does)
+constexpr double kMsDelta = 0.01;
+
+int ms_mixed(iro_ctx* c, int op, double mass, double csw, const DevField* B, int nshift,
+             const double* shifts, double* x, DevField* xblock, double precision, int max_iter,
+             int inner, iro_solver_out* out, int* nconv) {
+  CK(cudaSetDevice(device(c)));
+  auto t0 = std::chrono::steady_clock::now();
+  const int sub = op_subset(op);
+  const bool full = op_is_full(op);
+  const int p1 = PREC_SINGLE;
+  int rc = IRO_OK;
+  DevField* R = workspace(c, sub, p1, 1, 31, &rc); if (!R) return rc;
+  DevField* S = workspace(c, sub, p1, 1, 32, &rc); if (!S) return rc;
+  DevField* Q = workspace(c, sub, p1, 1, 33, &rc); if (!Q) return rc;
+  DevField* R64 = workspace(c, sub, PREC_DOUBLE, 1, 31, &rc); if (!R64) return rc;
+  DevField* S64 = workspace(c, sub, PREC_DOUBLE, 1, 32, &rc); if (!S64) return rc;
+  DevField* Q64 = workspace(c, sub, PREC_DOUBLE, 1, 33, &rc); if (!Q64) return rc;
+  std::vector<DevField*> XS(nshift), PS(nshift), X64(nshift);
+  for (int k = 0; k < nshift; ++k) {
+    XS[k] = workspace(c, sub, p1, 1, 40 + k, &rc); if (!XS[k]) return rc;
+    PS[k] = workspace(c, sub, p1, 1, 40 + MAXSHIFT + k, &rc); if (!PS[k]) return rc;
+    X64[k] = workspace(c, sub, PREC_DOUBLE, 1, 40 + k, &rc); if (!X64[k]) return rc;
+  }
+  cudaStream_t st = stream(c);
+  std::vector<double> bn;
+  RC(norms(c, *B, nullptr, bn, nullptr));
+  // ---- 1. solve_init (multiShiftSolver_CG.cpp:10-32): p_k = b, x_k = 0, r = b
+  RC(convert(c, *B, *R));
+  for (int k = 0; k < nshift; ++k) {
+    RC(axpby(c, 1.0, *R, 0.0, *R, *PS[k]));
+    RC(axpby(c, 0.0, *R, 0.0, *R, *XS[k]));
+    RC(axpby(c, 0.0, *B, 0.0, *B, *X64[k]));
+  }
+  MSState m;
+  std::memset(&m, 0, sizeof(m));
+  m.rr = bn[0];
+  m.maxrr = bn[0];
+  m.delta2 = kMsDelta * kMsDelta;
+  m.alphap = 0.0;
+  m.betap = 1.0;
+  m.snorm = 1.0 / bn[0];
+  m.prec = precision;
+  m.sigma0 = shifts[0];
+  m.nshift = nshift;
+  m.nshift2 = nshift;
+  m.conv_iter = -1;
+  for (int k = 0; k < nshift; ++k) {
+    m.csh2[k] = shifts[k] - shifts[0];
+    m.zeta1[k] = m.zeta2[k] = 1.0;
+  }
+  int zero = 0;
+  CK(cudaMemcpyAsync(state(c), &m, sizeof(m), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(done(c), &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+  MSFields f, f64;
+  for (int k = 0; k < MAXSHIFT; ++k) {
+    f.x[k] = XS[k < nshift ? k : 0]->all();
+    f.p[k] = PS[k < nshift ? k : 0]->all();
+    f64.x[k] = X64[k < nshift ? k : 0]->all();
+    f64.p[k] = f.p[k];
+  }
+  RC(apply(c, op, mass, csw, false, *PS[0], *Q, nullptr, 0, nullptr));  // autotuning, outside capture
+  RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  const MSState* dm = static_cast<const MSState*>(state(c));
+  Reduce ralpha = reduce(c, ST_MS_ALPHA, max_iter);
+  Reduce rr = reduce(c, ST_MS_R, max_iter);
+  Reduce rpp = reduce(c, ST_MS_PP, max_iter);
+  const int* skip = done(c);
+  auto body = [&](int n) -> int {
+    for (int i = 0; i < n; ++i) {
+      RC(apply(c, op, mass, csw, false, *PS[0], *Q, &ralpha, RED_OUT2 | RED_X2, skip));
+      RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
+      CK(launch_ms_xr(p1, B->sites(), XS[0]->all(), R->all(), PS[0]->all(), S->all(), dm, rr,
+                      max_blocks(c), st));
+      CK(launch_ms_p(p1, B->sites(), nshift, f, R->all(), dm, rpp, max_blocks(c), st));
+    }
+    return IRO_OK;
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (st != nullptr) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int brc = body(kChunk);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (brc) return brc;
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaGraphInstantiate");
+  }
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() { if (e) cudaGraphExecDestroy(e); }
+  } guard{exec};
+  int* hpin = static_cast<int*>(pinned(c));
+  int merged_upto = nshift;  // shifts active since the last merge
+  int updates = 0, launched = 0;
+  bool converged = false;
+  ShiftList s0{};
+  s0.s[0] = shifts[0];
+  while (launched < max_iter) {
+    if (exec) CK(cudaGraphLaunch(exec, st));
+    else RC(body(kChunk));
+    launched += kChunk;
+    CK(cudaMemcpyAsync(hpin, done(c), sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hpin[0] == RUNNING) continue;
+    if (hpin[0] != PAUSED) break;  // stopped at max_iter
+    // reliable update: x_k += xlo_k; r = b - (A + sigma_0) x_0 in FP64
+    CK(cudaMemcpyAsync(&m, state(c), sizeof(m), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(launch_ms_merge(B->sites(), merged_upto, f64, f, st));
+    merged_upto = m.nshift2;
+    RC(apply(c, op, mass, csw, false, *X64[0], *Q64, nullptr, 0, nullptr));
+    RC(apply(c, op, mass, csw, true, *Q64, *S64, nullptr, 0, nullptr));
+    CK(launch_ms_block_residual(B->sites(), 1, B->all(), S64->all(), X64[0]->all(), s0, R64->all(), st));
+    std::vector<double> rt;
+    RC(norms(c, *R64, nullptr, rt, nullptr));
+    RC(convert(c, *R64, *R));
+    ++updates;
+    m.rr = rt[0];
+    m.maxrr = rt[0];
+    int dflag = RUNNING;
+    if (m.rr * m.snorm < precision) {
+      m.conv_iter = m.iter - 1;
+      dflag = CONVERGED;
+      converged = true;
+    } else if (m.iter >= max_iter) {
+      dflag = STOPPED;
+    }
+    CK(cudaMemcpyAsync(state(c), &m, sizeof(m), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(done(c), &dflag, sizeof(int), cudaMemcpyHostToDevice, st));
+    if (dflag != RUNNING) break;
+  }
+  CK(cudaMemcpyAsync(&m, state(c), sizeof(m), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (!converged) CK(launch_ms_merge(B->sites(), merged_upto, f64, f, st));
+  const int iter1 = m.iter;
+  // ---- 2. the shifted residuals in FP64, one block of nshift right-hand sides
+  DevField* XB = workspace(c, sub, PREC_DOUBLE, nshift, 70, &rc); if (!XB) return rc;
+  DevField* QB = workspace(c, sub, PREC_DOUBLE, nshift, 71, &rc); if (!QB) return rc;
+  DevField* SB = workspace(c, sub, PREC_DOUBLE, nshift, 72, &rc); if (!SB) return rc;
+  DevField* RB = workspace(c, sub, PREC_DOUBLE, nshift, 73, &rc); if (!RB) return rc;
+  DevField* EB = workspace(c, sub, PREC_DOUBLE, nshift, 74, &rc); if (!EB) return rc;
+  ShiftList sl{};
+  for (int k = 0; k < nshift; ++k) sl.s[k] = shifts[k];
+  CK(launch_ms_pack(PREC_DOUBLE, B->sites(), nshift, f64, XB->all(), st));
+  auto residuals = [&](std::vector<double>& rn) -> int {
+    RC(apply(c, op, mass, csw, false, *XB, *QB, nullptr, 0, nullptr));
+    RC(apply(c, op, mass, csw, true, *QB, *SB, nullptr, 0, nullptr));
+    CK(launch_ms_block_residual(B->sites(), nshift, B->all(), SB->all(), XB->all(), sl, RB->all(), st));
+    return norms(c, *RB, nullptr, rn, nullptr);
+  };
+  std::vector<double> rn;
+  RC(residuals(rn));
+  // ---- 3. refinement of the shifts above the goal, one block
+  bool refine = false;
+  for (int k = 0; k < nshift; ++k) refine = refine || !(rn[k] < precision * bn[0]);
+  int it2 = 0, upd2 = 0, applies2 = 0, rc2 = IRO_OK;
+  if (refine && converged) {
+    std::vector<double> goal(nshift);
+    for (int k = 0; k < nshift; ++k)
+      goal[k] = rn[k] > 0.0 ? 0.9 * precision * bn[0] / rn[k] : 1.0;
+    iro_cg_params p2;
+    p2.precision = precision;
+    p2.max_iter = max_iter;
+    p2.inner_prec = inner;
+    // FP32 inner storage carries the refinement (3-4 decades) to one FP64
+    // recomputation; FP16 needs one per decade
+    p2.delta = inner == PREC_SINGLE ? 1e-4 : 0.1;
+    p2.use_graph = 1;
+    std::vector<iro_solver_out> o2(nshift);
+    rc2 = cg_mixed(c, op, mass, csw, &p2, RB, EB, nshift, o2.data(), shifts, goal.data());
+    if (rc2 != IRO_OK && rc2 != IRO_NOT_CONVERGED) return rc2;
+    RC(axpby(c, 1.0, *XB, 1.0, *EB, *XB));
+    // the refinement's final FP64 true residual of (A + sigma_k) e_k = r_k is
+    // the shift's residual b - (A + sigma_k)(x_k + e_k), relative to |r_k|
+    for (int k = 0; k < nshift; ++k) rn[k] *= o2[k].diff * o2[k].diff;
+    for (int k = 0; k < nshift; ++k) {
+      if (o2[k].iterations + 1 > it2) it2 = o2[k].iterations + 1;
+      if (o2[k].reliable_updates > upd2) upd2 = o2[k].reliable_updates;
+      applies2 += o2[k].operator_applies;
+    }
+  }
+  // ---- 4. the true residuals
+  double dmax = 0.0;
+  for (int k = 0; k < nshift; ++k) {
+    const double d = rn[k] / bn[0];
+    if (d > dmax) dmax = d;
+  }
+  if (x) RC(export_field(c, *XB, full, x));
+  if (xblock) RC(axpby(c, 1.0, *XB, 0.0, *XB, *xblock));
+  auto t1 = std::chrono::steady_clock::now();
+  const bool conv = converged && dmax < precision && rc2 == IRO_OK;
+  out->diff = std::sqrt(dmax);
+  out->iterations = conv ? iter1 + it2 - 1 : -1;
+  out->timing_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  out->reliable_updates = updates + upd2;
+  out->operator_applies = iter1 + 2 * updates + applies2 + 2 * nshift;
+  *nconv = out->iterations;
+  if (!conv) return set_error(c, IRO_NOT_CONVERGED, "Not converged.");
+  return IRO_OK;
+}
+}  // namespace
+
+extern "C" int iro_multishift_cg_solve_mixed(iro_ctx* c, int op, double mass, double csw,
+                                             const double* b, int nshift, const double* shifts,
+                                             double* x, double precision, int max_iter,
+                                             int inner_prec, iro_solver_out* out, int* nconv) {
+  if (!x || !ms_args_ok(c, op, b, nshift, shifts, precision, out, nconv) || inner_prec < 0 ||
+      inner_prec > 2)
+    return set_error(c, IRO_BAD_ARG, "bad multishift arguments");
+  for (int k = 1; k < nshift; ++k)
+    if (!(shifts[k] >= shifts[k - 1]))
+      return set_error(c, IRO_BAD_ARG, "shifts must be ascending (the smallest first)");
+  CK(cudaSetDevice(device(c)));
+  int rc = IRO_OK;
+  DevField* B = workspace(c, op_subset(op), PREC_DOUBLE, 1, 30, &rc); if (!B) return rc;
+  RC(import_field(c, b, op_is_full(op), *B));
+  if (inner_prec == PREC_DOUBLE)
+    return ms_run(c, op, mass, csw, B, nshift, shifts, x, nullptr, precision, max_iter, out, nconv,
+                  nullptr);
+  if (op == IRO_OP_CLOVER_FULL || op == IRO_OP_CLOVER_SCHUR_EE) RC(clover_ready(c, mass, csw));
+  return ms_mixed(c, op, mass, csw, B, nshift, shifts, x, nullptr, precision, max_iter, inner_prec,
+                  out, nconv);
+}
+
+extern "C" int iro_multishift_cg_solve_field(iro_ctx* c, int op, double mass, double csw,
+                                             const iro_field* b, int nshift, const double* shifts,
+                                             iro_field* x, double precision, int max_iter,
+                                             int inner_prec, iro_solver_out* out, int* nconv) {
+  const DevField* B = field_dev(const_cast<iro_field*>(b));
+  DevField* X = field_dev(x);
+  if (!c || !B || !X || !shifts || !out || !nconv || nshift < 1 || nshift > MAXSHIFT ||
+      !solver_op_ok(op) || !(precision > 0.0) || inner_prec < 0 || inner_prec > 2 ||
+      B->prec != PREC_DOUBLE || B->nrhs != 1 || B->subset != op_subset(op) ||
+      X->prec != PREC_DOUBLE || X->nrhs != nshift || X->subset != op_subset(op))
+    return set_error(c, IRO_BAD_ARG, "bad multishift field arguments");
+  for (int k = 1; k < nshift; ++k)
+    if (!(shifts[k] >= shifts[k - 1]))
+      return set_error(c, IRO_BAD_ARG, "shifts must be ascending (the smallest first)");
+  CK(cudaSetDevice(device(c)));
+  if (inner_prec == PREC_DOUBLE)
+    return ms_run(c, op, mass, csw, B, nshift, shifts, nullptr, X, precision, max_iter, out, nconv,
+                  nullptr);
+  if (op == IRO_OP_CLOVER_FULL || op == IRO_OP_CLOVER_SCHUR_EE) RC(clover_ready(c, mass, csw));
+  return ms_mixed(c, op, mass, csw, B, nshift, shifts, nullptr, X, precision, max_iter, inner_prec,
+                  out, nconv);
 }
 
 // RationalSolver_CG::solve (lib/Solver/rationalSolver_CG.cpp:12-39): the
@@ -377,9 +660,11 @@ extern "C" int iro_rational_cg_solve(iro_ctx* c, int op, double mass, double csw
     return set_error(c, IRO_BAD_ARG, "bad rational solver arguments");
   CK(cudaSetDevice(device(c)));
   std::vector<DevField*> xs;
-  DevField* B = nullptr;
-  const int rc = ms_run(c, op, mass, csw, b, npole, poles, nullptr, precision, max_iter, out,
-                        nconv, &xs, &B);
+  int wrc0 = IRO_OK;
+  DevField* B = workspace(c, op_subset(op), PREC_DOUBLE, 1, 30, &wrc0); if (!B) return wrc0;
+  RC(import_field(c, b, op_is_full(op), *B));
+  const int rc = ms_run(c, op, mass, csw, B, npole, poles, nullptr, nullptr, precision, max_iter,
+                        out, nconv, &xs);
   if (rc != IRO_OK && rc != IRO_NOT_CONVERGED) return rc;
   const int sub = op_subset(op);
   int wrc = IRO_OK;
@@ -407,7 +692,8 @@ extern "C" int iro_rational_cg_solve(iro_ctx* c, int op, double mass, double csw
 // declared only on the FP64 true residual.  The starting guess is x0 = b as
 // in Solver_CG (solver_CG.cpp:40).
 int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* prm,
-             const DevField* B, DevField* X, int nrhs, iro_solver_out* out) {
+             const DevField* B, DevField* X, int nrhs, iro_solver_out* out, const double* sigma,
+             const double* target) {
   const int sub = op_subset(op);
   const bool full = op_is_full(op);
   const int pl = prm->inner_prec;
@@ -427,12 +713,17 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
 
   RC(axpby(c, 1.0, *B, 0.0, *B, *X));
   std::vector<CGState> hs(nrhs);
-  for (auto& s : hs) {
+  bool shifted = false;
+  for (int r = 0; r < nrhs; ++r) {
+    CGState& s = hs[r];
     std::memset(&s, 0, sizeof(s));
-    s.target = prm->precision;
+    s.target = target ? target[r] : prm->precision;
     s.delta2 = delta * delta;
     s.conv_iter = -1;
+    s.sigma = sigma ? sigma[r] : 0.0;
+    shifted = shifted || s.sigma != 0.0;
   }
+  const CGState* dstate = static_cast<const CGState*>(state(c));
   CK(cudaMemcpyAsync(state(c), hs.data(), sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
   // r = b - A x for x = b: only the inner iteration starts from this residual,
   // and the first reliable update recomputes it in FP64 from the FP64 x (which
@@ -443,6 +734,7 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   RC(apply(c, op, mass, csw, false, *Pl, *Ql, nullptr, 0, nullptr));
   RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, nullptr));
   RC(convert(c, *Sl, *S));
+  if (shifted) CK(launch_shift_add(B->sites(), nrhs, S->all(), B->all(), dstate, st));
   Reduce rinit = reduce(c, ST_CG_INIT, prm->max_iter);
   CK(launch_cg_init(PREC_DOUBLE, B->sites(), nrhs, B->all(), S->all(), R->all(), Q->all(), rinit,
                     max_blocks(c), st));
@@ -456,11 +748,18 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   Reduce rnone = reduce(c, ST_NONE, 0);
   auto body = [&](int n) -> int {
     for (int i = 0; i < n; ++i) {
-      RC(apply(c, op, mass, csw, false, *Pl, *Ql, &ralpha, RED_OUT2, skip));
-      RC(apply_cg(c, op, mass, csw, true, *Ql, *Sl, rbeta, skip,
-                  CGFuse{Rl, static_cast<const CGState*>(state(c))}));
-      CK(launch_cg_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(), Xl->all(),
-                     static_cast<const CGState*>(state(c)), done(c), st));
+      if (shifted) {
+        // (p, (A + sigma) p) from |M p|^2 and |p|^2; A p stored, then
+        // r -= alpha (A p + sigma p) in its own pass
+        RC(apply(c, op, mass, csw, false, *Pl, *Ql, &ralpha, RED_OUT2 | RED_X2, skip));
+        RC(apply(c, op, mass, csw, true, *Ql, *Sl, nullptr, 0, skip));
+        CK(launch_cg_shift_r(pl, Rl->sites(), nrhs, Rl->all(), Sl->all(), Pl->all(), dstate, rbeta,
+                             max_blocks(c), st));
+      } else {
+        RC(apply(c, op, mass, csw, false, *Pl, *Ql, &ralpha, RED_OUT2, skip));
+        RC(apply_cg(c, op, mass, csw, true, *Ql, *Sl, rbeta, skip, CGFuse{Rl, dstate}));
+      }
+      CK(launch_cg_p(pl, Pl->sites(), nrhs, Pl->all(), Rl->all(), Xl->all(), dstate, done(c), st));
     }
     return IRO_OK;
   };
@@ -509,6 +808,7 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
     CK(launch_mx_merge(pl, X->sites(), nrhs, X->all(), Xl->all(), dmask, st));
     RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
     RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+    if (shifted) CK(launch_shift_add(X->sites(), nrhs, S->all(), X->all(), dstate, st));
     CK(launch_mx_residual(pl, B->sites(), nrhs, B->all(), S->all(), R->all(), Rl->all(), dmask,
                           rnone, max_blocks(c), st));
     std::vector<double> rr(nrhs);
@@ -553,7 +853,8 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   for (int r = 0; r < nrhs; ++r) all_conv = all_conv && hdone[r] == CONVERGED;
   if (all_conv) {
     for (int r = 0; r < nrhs; ++r) {
-      const double bb = hs[r].target / prm->precision;  // target = precision |b|^2
+      // target = goal |b|^2
+      const double bb = hs[r].target / (target ? target[r] : prm->precision);
       out[r].diff = std::sqrt(hs[r].rr / bb);
       out[r].iterations = hs[r].conv_iter;
       out[r].reliable_updates = updates[r];
@@ -567,6 +868,7 @@ int cg_mixed(iro_ctx* c, int op, double mass, double csw, const iro_cg_params* p
   CK(launch_mx_merge(pl, X->sites(), nrhs, X->all(), Xl->all(), dmask, st));
   RC(apply(c, op, mass, csw, false, *X, *Q, nullptr, 0, nullptr));
   RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
+  if (shifted) CK(launch_shift_add(X->sites(), nrhs, S->all(), X->all(), dstate, st));
   RC(axpby(c, 1.0, *S, -1.0, *B, *R));
   std::vector<double> rn, bn;
   RC(norms(c, *R, B, rn, &bn));

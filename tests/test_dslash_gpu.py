@@ -158,3 +158,24 @@ def test_multi_rhs_equals_single(prec):
             # packed FP32x2 arithmetic: equal to FP32 rounding, not bitwise
             tol = TOL_FP32 if prec == "single" else TOL_FP16
             assert np.linalg.norm(blk[r] - one) < tol * np.linalg.norm(one)
+
+
+@pytest.mark.parametrize("prec", ["double", "single", "half"])
+@pytest.mark.parametrize("nrhs", [2, 4, 16])
+@pytest.mark.parametrize("op", [ib.OP_WILSON_FULL, ib.OP_WILSON_SCHUR_EE])
+def test_block_sizes_equal_single(prec, nrhs, op):
+    """Blocks of 2, 4 and 16 right-hand sides (every kernel variant the
+    autotuner tries for them, the shared-memory staged one included) on the
+    full and the Schur operator agree with the single-RHS operator."""
+    L = [4, 4, 4, 8]
+    V = int(np.prod(L))
+    n = V if op == ib.OP_WILSON_FULL else V // 2
+    c = ib.context(L)
+    c.upload_gauge(ib.synth_gauge(L, 0.2, 52, True), force=True)
+    m = 0.5 / 0.12 - 4
+    fs = np.stack([ib.synth_gaussian(n, 70 + r) for r in range(nrhs)])
+    blk = c.apply(op, m, 0.0, 0, fs.ravel(), prec, nrhs=nrhs).reshape(nrhs, -1)
+    tol = {"double": 1e-13, "single": TOL_FP32, "half": TOL_FP16}[prec]
+    for r in range(nrhs):
+        one = c.apply(op, m, 0.0, 0, fs[r], prec)
+        assert np.linalg.norm(blk[r] - one) < tol * np.linalg.norm(one)

@@ -126,3 +126,43 @@ def test_multishift_vs_reference(g, name):
     assert out.diff < TOL_RES
     for k in range(len(g["shifts"])):
         assert rel(xs[k], g[f"ms_{name}_x"][k]) < TOL_SOL
+
+
+@pytest.mark.parametrize("name", ["wilson_full", "wilson_eo"])
+@pytest.mark.parametrize("inner", ["single", "half"])
+def test_multishift_mixed_vs_reference(g, name, inner):
+    """The mixed-precision multishift (FP32 multishift with FP64 recurrences,
+    then one block of reliable-update CG refinements, one per shift): every
+    shift's solution within 1e-8 of the reference's, every FP64 true
+    residual below 1e-10."""
+    D, b = _dirac(g, name)
+    slv = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 5000, inner=inner)
+    xs = []
+    out = slv.solve(xs, b, g["shifts"])
+    assert out.diff < TOL_RES
+    assert out.Nconv > 0
+    for k in range(len(g["shifts"])):
+        assert rel(xs[k], g[f"ms_{name}_x"][k]) < TOL_SOL
+
+
+@pytest.mark.parametrize("inner", ["single", "half"])
+def test_multishift_mixed_12_shifts_8c8(inner):
+    """12 shifts 1e-4..10 at 8^4 on the clover Schur operator: the mixed
+    solver's solutions against the FP64 multishift's, and each shifted
+    system's residual checked with the operator itself."""
+    L = [8, 8, 8, 8]
+    V = int(np.prod(L))
+    c = ib.context(L)
+    u = ib.synth_gauge(L, 0.2, 81, True)
+    c.upload_gauge(u, force=True)
+    D = ib.Dirac_Clover_EvenOdd(0.5 / 0.12 - 4, 1.0, u, ctx=c)
+    b = ib.synth_gaussian(V // 2, 82)
+    shifts = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
+    x64, xm = [], []
+    ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 5000).solve(x64, b, shifts)
+    out = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-20, 5000, inner=inner).solve(xm, b, shifts)
+    assert out.diff < TOL_RES
+    for k, s in enumerate(shifts):
+        assert rel(xm[k], x64[k]) < TOL_SOL, k
+        r = D.mult_dag(D.mult(xm[k])) + s * xm[k] - b
+        assert np.linalg.norm(r) < 1.01 * TOL_RES * np.linalg.norm(b), k
