@@ -436,6 +436,114 @@ __global__ void __launch_bounds__(kFwdThreads) ptc_fwd_kernel(PtcGeo G, const fl
   if (warp == 0) tmem_dealloc(tmem, S::TCOLS);
 }
 
+// Double-buffered forward kernel (two A tiles, two accumulators): the A tile
+// of tile t+1 is built while the MMAs of tile t run, and tile t is read back
+// after that build, before the MMAs of tile t+1 are issued.  A CTA's tile
+// otherwise spends about a third of its time waiting for its MMAs (measured
+// with clock64 at 32^3x64: 3.5k of 9.5k cycles for an 8->8 layer).  The
+// shared memory holds [A1 | A0 | weights]: the MMA's rows 96..127 of A1 read
+// the first rows of A0, those of A0 the weights (padded to >= 32 rows); those
+// rows feed accumulator rows that are never read back.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kFwdThreads) ptc_fwd2_kernel(PtcGeo G, const float2* __restrict__ in,
+                                                               float2* __restrict__ out,
+                                                               const __nv_bfloat16* __restrict__ bop,
+                                                               int ntiles) {
+  using S = Ptc<CIN, COUT>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  // A tile of buffer b: A0 = smem + A96, A1 = smem
+  auto abuf = [&](int b) { return smem + (b ? 0 : S::A96_BYTES); };
+  unsigned char* B = smem + 2 * S::A96_BYTES;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tslot;
+  __shared__ int mma_ok;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) tmem_alloc(&tslot, 2 * S::TCOLS);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+  }
+  for (int b = S::B_BYTES + threadIdx.x * 16; b < S::BF_BYTES; b += kFwdThreads * 16)
+    *reinterpret_cast<uint4*>(B + b) = make_uint4(0, 0, 0, 0);
+  for (int idx = threadIdx.x; idx < S::NP * (S::KP / 8); idx += kFwdThreads) {
+    const int n = idx / (S::KP / 8), k0 = (idx - n * (S::KP / 8)) * 8;
+    *reinterpret_cast<uint4*>(B + canon(n, k0, S::KP)) =
+        __ldg(reinterpret_cast<const uint4*>(bop + size_t(n) * S::KP + k0));
+  }
+  // columns KF..KP of both tiles are never written by a job
+  for (int b = threadIdx.x * 16; b < 2 * S::A96_BYTES; b += kFwdThreads * 16)
+    *reinterpret_cast<uint4*>(smem + b) = make_uint4(0, 0, 0, 0);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem0 = tslot;
+  const uint32_t idesc = idesc_bf16(S::NP);
+  uint32_t ph = 0u;  // bit b: the mbarrier phase to wait for on buffer b
+  int prev = -1;     // the tile whose MMAs are in flight
+  for (int tile = blockIdx.x, it = 0;; tile += gridDim.x, ++it) {
+    const bool have = tile < ntiles;
+    const int sb = it & 1;
+    if (have) a_tile_job<CIN, S::KP>(G, in, tile * kFwdSites + lane, lane, warp, abuf(sb));
+    fence_async_smem();
+    __syncthreads();
+    tc_fence_after();
+    if (prev >= 0) {
+      // the previous tile: wait for its MMAs (bounded), read its accumulator back
+      const int pb = sb ^ 1;
+      if (warp == 0) {
+        bool ok = false;
+        for (int i = 0; i < kWaitLimit; ++i)
+          if (mbar_try_wait(&bar[pb], (ph >> pb) & 1u)) {
+            ok = true;
+            break;
+          }
+        if (lane == 0) {
+          mma_ok = ok ? 1 : 0;
+          if (!ok) atomicExch(G.err, 1);
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      ph ^= 1u << pb;
+      if (!mma_ok) break;  // the same flag in every thread: the CTA leaves together
+      if (warp < 3) {
+        const int r = warp * 32 + lane;
+        float v[S::NP];
+#pragma unroll
+        for (int c = 0; c < S::NP; c += 16)
+          tmem_ld16(tmem0 + uint32_t(pb * S::TCOLS) + (uint32_t(warp * 32) << 16) + c, v + c);
+        const int sl = r / 3, a = r - sl * 3;
+        const int s = prev * kFwdSites + sl;
+        if (s < G.V) {
+          float4* o4 = reinterpret_cast<float4*>(out) + size_t(a) * G.V + s;
+#pragma unroll
+          for (int q = 0; q < COUT / 2; ++q)
+            o4[size_t(3 * q) * G.V] = make_float4(v[4 * q], v[4 * q + 2], v[4 * q + 1], v[4 * q + 3]);
+        }
+      }
+      // the accumulator of the previous tile is read before it is reused
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+    }
+    if (!have) break;
+    if (threadIdx.x == 0) {
+      const uint32_t a0 = smem_u32(abuf(sb)), b0 = smem_u32(B);
+      constexpr uint32_t sbo = (S::KP / 8) * 128;
+#pragma unroll 1
+      for (int kb = 0; kb < S::KP / 16; ++kb)
+        umma_bf16(tmem0 + uint32_t(sb * S::TCOLS), smem_desc(a0 + kb * 256, 128, sbo),
+                  smem_desc(b0 + kb * 256, 128, sbo), idesc, kb > 0 ? 1u : 0u);
+      umma_commit(&bar[sb]);
+    }
+    prev = tile;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem0, 2 * S::TCOLS);
+}
+
 // ---- backward: dA = dY B, stored as FP32 rows (site, colour) x KP ------------------
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThreads) ptc_da_kernel(PtcGeo G, const float2* __restrict__ dy,
@@ -612,10 +720,43 @@ static int sm_count() {
   return n;
 }
 
+// CTAs of `threads` threads of kernel f that fit on one SM by registers (65536
+// per SM, allocated per warp in units of 256): the persistent forward kernels
+// launch no more than this many per SM, so that no CTA waits for another to
+// finish before it starts its share of the tiles
+static int fit_by_registers(const void* f, int threads) {
+  cudaFuncAttributes a;
+  if (cudaFuncGetAttributes(&a, f) != cudaSuccess || a.numRegs <= 0) return 1 << 20;
+  const int per_warp = (a.numRegs * 32 + 255) / 256 * 256;
+  const int n = 65536 / (per_warp * ((threads + 31) / 32));
+  return n > 0 ? n : 1;
+}
+
 template <int CIN, int COUT>
 static cudaError_t fwd_t(const PtcGeo& G, const float2* in, float2* out, const __nv_bfloat16* bop,
                          cudaStream_t st) {
   using S = Ptc<CIN, COUT>;
+  const int ntiles2 = (G.V + kFwdSites - 1) / kFwdSites;
+  // double-buffered where two A tiles leave room for at least two CTAs per SM
+  // in ~200 KB of shared memory (CIN <= 8); one tile otherwise
+  const int smem2 = 2 * S::A96_BYTES + S::BF_BYTES;
+  if ((200 * 1024) / (smem2 + 1024) >= 2) {
+    static bool attr2 = false;
+    if (!attr2) {
+      cudaError_t e = cudaFuncSetAttribute(ptc_fwd2_kernel<CIN, COUT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem2);
+      if (e != cudaSuccess) return e;
+      attr2 = true;
+    }
+    int per_sm = (200 * 1024) / (smem2 + 1024);
+    if (per_sm > 2048 / kFwdThreads) per_sm = 2048 / kFwdThreads;
+    const int regs = fit_by_registers(reinterpret_cast<const void*>(ptc_fwd2_kernel<CIN, COUT>), kFwdThreads);
+    if (per_sm > regs) per_sm = regs;
+    int grid = sm_count() * per_sm;
+    if (grid > ntiles2) grid = ntiles2;
+    ptc_fwd2_kernel<CIN, COUT><<<grid, kFwdThreads, smem2, st>>>(G, in, out, bop, ntiles2);
+    return cudaGetLastError();
+  }
   const int smem = S::A96_BYTES + S::BF_BYTES;
   static bool attr = false;
   if (!attr) {
@@ -630,6 +771,8 @@ static cudaError_t fwd_t(const PtcGeo& G, const float2* in, float2* out, const _
   // for the neighbour gathers), at most one per tile
   int per_sm = (150 * 1024) / (smem + 1024);
   if (per_sm > 2048 / kFwdThreads) per_sm = 2048 / kFwdThreads;
+  const int regs = fit_by_registers(reinterpret_cast<const void*>(ptc_fwd_kernel<CIN, COUT>), kFwdThreads);
+  if (per_sm > regs) per_sm = regs;
   if (per_sm < 1) per_sm = 1;
   int grid = sm_count() * per_sm;
   if (grid > ntiles) grid = ntiles;
