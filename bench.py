@@ -402,13 +402,14 @@ def batched_solves(torch, device):
     return out
 
 
-def learned_solves(torch, device, nfields=24, epochs=15, widths=(4, 8, 8, 4), nkrylov=16):
+def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), nkrylov=16):
     """Learned preconditioner: a PTC network trained by the library's own
     forward/backward kernels on pairs (b = D^dag D v, v) from `nfields` seeded
     16^3x32 gauge fields (eps=0.2, kappa=0.12), then applied inside flexible
-    GCR at 32^3x64 (unseen field, one Gaussian source) against GCR without it
-    and against CG on the same full-lattice D^dag D: FP64 and mixed precision.
-    Every solve stops on the FP64 true residual 1e-10."""
+    GCR at 32^3x64 and 48^3x96 (unseen fields, one Gaussian source each)
+    against GCR without it and against CG on the same full-lattice D^dag D:
+    FP64 and mixed precision.  Every solve stops on the FP64 true residual
+    1e-10."""
     import iroiro_b200 as ib
     from iroiro_b200 import learned
     t0 = time.perf_counter()
@@ -420,17 +421,7 @@ def learned_solves(torch, device, nfields=24, epochs=15, widths=(4, 8, 8, 4), nk
     W = net0.W
     for pr in pairs:
         pr.ctx.close()
-    Lb = [32, 32, 32, 64]
-    Vb = int(np.prod(Lb))
-    ctx = ib.Context(Lb, device)
-    s = torch.cuda.current_stream()
-    ctx.set_stream(s.cuda_stream)
-    u = ib.synth_gauge(Lb, EPS, SEED + 301)
-    ctx.upload_gauge(u, force=True)
-    D = ib.Dirac_Wilson(MASS, u, ctx=ctx)
-    b = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(Vb, SEED + 302))
-    net = learned.PTCNet(ctx, widths, W)
-    out = {"op": "full-lattice Wilson D^dag D 32^3x64, kappa=0.12, one Gaussian source",
+    out = {"op": "full-lattice Wilson D^dag D, kappa=0.12, one Gaussian source, unseen field",
            "network": {"widths": list(widths), "train_fields": nfields, "train_lattice": "16^3x32",
                        "epochs": epochs, "train_s": round(train_s, 1),
                        "loss_first": round(hist[0], 4), "loss_last": round(hist[-1], 4)}}
@@ -443,29 +434,46 @@ def learned_solves(torch, device, nfields=24, epochs=15, widths=(4, 8, 8, 4), nk
         torch.cuda.synchronize()
         return (time.perf_counter() - t) * 1e3, r
 
-    for name, n in (("gcr_network", net), ("gcr_plain", None)):
-        x = ib.DeviceField(ctx, 2, "double")
-        slv = learned.Solver_GCR(D, n, nkrylov=nkrylov)
-        ms, (o, rc) = timed(lambda: slv.solve_field(b, x))
-        out[name] = {"ms": round(ms, 1), "iterations": o.iterations, "true_residual": o.diff,
-                     "cg_fallback": bool(o.fallback), "converged": rc == ib.OK}
-        x.close()
-    for inner in ("double", "single", "half"):
-        x = ib.DeviceField(ctx, 2, "double")
-        slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner)
-        ms, (outs, rc) = timed(lambda: slv.solve_field(b, x))
-        out["cg_" + inner] = {"ms": round(ms, 1), "iterations": outs[0].Iterations,
-                              "true_residual": outs[0].diff, "converged": rc == ib.OK}
-        x.close()
-    a = ib.DeviceField(ctx, 2, "single").upload(ib.synth_gaussian(Vb, SEED + 303))
-    c2 = ib.DeviceField(ctx, 2, "single")
-    apply_ms, _ = timed(lambda: ctx.check(net.L.iro_ptc_apply_field(ctx.h, net.h, a.h, c2.h), "apply"))
-    out["network_apply_ms"] = round(apply_ms, 3)
-    best_cg = min(out["cg_single"]["ms"], out["cg_half"]["ms"])
-    out["gcr_network_vs_best_mixed_cg"] = round(best_cg / out["gcr_network"]["ms"], 2)
-    out["iteration_ratio_vs_gcr_plain"] = round(out["gcr_plain"]["iterations"] /
-                                                max(1, out["gcr_network"]["iterations"]), 2)
-    ctx.close()
+    for Lb, tag, seed in (([32, 32, 32, 64], "", SEED + 301), ([48, 48, 48, 96], "_48x48x48x96", SEED + 311)):
+        Vb = int(np.prod(Lb))
+        ctx = ib.Context(Lb, device)
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        u = ib.synth_gauge(Lb, EPS, seed)
+        ctx.upload_gauge(u, force=True)
+        D = ib.Dirac_Wilson(MASS, u, ctx=ctx)
+        b = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(Vb, seed + 1))
+        net = learned.PTCNet(ctx, widths, W)
+        res = {}
+        for name, n in (("gcr_network", net), ("gcr_plain", None)):
+            x = ib.DeviceField(ctx, 2, "double")
+            slv = learned.Solver_GCR(D, n, nkrylov=nkrylov)
+            ms, (o, rc) = timed(lambda: slv.solve_field(b, x))
+            res[name] = {"ms": round(ms, 1), "iterations": o.iterations, "true_residual": o.diff,
+                         "cg_fallback": bool(o.fallback), "converged": rc == ib.OK}
+            x.close()
+        for inner in ("double", "single", "half"):
+            x = ib.DeviceField(ctx, 2, "double")
+            slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner)
+            ms, (outs, rc) = timed(lambda: slv.solve_field(b, x))
+            res["cg_" + inner] = {"ms": round(ms, 1), "iterations": outs[0].Iterations,
+                                  "true_residual": outs[0].diff, "converged": rc == ib.OK}
+            x.close()
+        a = ib.DeviceField(ctx, 2, "single").upload(ib.synth_gaussian(Vb, seed + 2))
+        c2 = ib.DeviceField(ctx, 2, "single")
+        apply_ms, _ = timed(lambda: ctx.check(net.L.iro_ptc_apply_field(ctx.h, net.h, a.h, c2.h), "apply"))
+        res["network_apply_ms"] = round(apply_ms, 3)
+        best_cg = min(res["cg_single"]["ms"], res["cg_half"]["ms"])
+        res["gcr_network_vs_best_mixed_cg"] = round(best_cg / res["gcr_network"]["ms"], 2)
+        res["iteration_ratio_vs_gcr_plain"] = round(res["gcr_plain"]["iterations"] /
+                                                    max(1, res["gcr_network"]["iterations"]), 2)
+        if tag:
+            out["at" + tag] = res
+        else:
+            out.update(res)
+        for f in (a, c2, b):
+            f.close()
+        net.close()
+        ctx.close()
     return out
 
 
@@ -843,6 +851,12 @@ def summarise(line, peak):
         out["learned_iterations"] = {k: g(lr, k, "iterations") for k in ("gcr_network", "cg_half")}
         out["learned_network_apply_ms"] = lr.get("network_apply_ms")
         out["gcr_network_vs_best_mixed_cg"] = lr.get("gcr_network_vs_best_mixed_cg")
+        l48 = lr.get("at_48x48x48x96")
+        if l48:
+            out["learned_48x48x48x96_ms"] = {k: g(l48, k, "ms") for k in
+                                             ("gcr_network", "gcr_plain", "cg_half")}
+            out["learned_48x48x48x96_iterations"] = {k: g(l48, k, "iterations") for k in
+                                                     ("gcr_network", "gcr_plain", "cg_half")}
     m = line["mixed48"]
     if m:
         out["mixed48_clover_12rhs"] = {"fp64_ms": g(m, "double", "ms"), "fp16_ms": g(m, "half", "ms"),

@@ -1411,6 +1411,7 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
     LRC(convert(c, *R, *r32));
     LRC(axpby(c, 0.0, *r32, 0.0, *r32, *e32));
     const double rr_start = rr;
+    double rr_it = rr;  // the iterated |r|^2
     std::vector<double> nw(m, 0.0);
     for (int j = 0; j < m && iters < prm->max_iter; ++j) {
       // z_j = N(r) (or r without a network), w_j = A z_j
@@ -1433,17 +1434,18 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
         LRC(caxpy(ws, beta, *W[j]));
         LRC(caxpy(zs, beta, *Z[j]));
       }
-      std::vector<std::complex<double>> g1, g2;
-      LRC(cdots({W[j]}, *W[j], g1));
-      LRC(cdots({W[j]}, *r32, g2));
-      nw[j] = g1[0].real();
-      const std::complex<double> alpha = g2[0] / nw[j];
+      // |w_j|^2 and <w_j, r> in one pass: <w_j, w_j> and <r, w_j> = conj(<w_j, r>)
+      std::vector<std::complex<double>> g;
+      LRC(cdots({W[j], r32}, *W[j], g));
+      nw[j] = g[0].real();
+      const std::complex<double> alpha = std::conj(g[1]) / nw[j];
       LRC(caxpy({Z[j]}, {alpha}, *e32));
       LRC(caxpy({W[j]}, {-alpha}, *r32));
-      std::vector<std::complex<double>> rn;
-      LRC(cdots({r32}, *r32, rn));
+      // the new |r|^2 = |r|^2 - |<w_j, r>|^2 / |w_j|^2 (r minus its projection
+      // on w_j); only the restart test reads it, the FP64 residual decides
+      rr_it = rr_it - std::norm(g[1]) / nw[j];
       ++iters;
-      if (rn[0].real() < target || rn[0].real() < delta * delta * rr_start) break;
+      if (rr_it < target || rr_it < delta * delta * rr_start) break;
     }
     // x += e, r = b - A x in FP64
     LCK(launch_mx_merge(PREC_SINGLE, X->sites(), 1, X->all(), e32->all(), dmask, st));
