@@ -658,6 +658,11 @@ def run_ours(args, world, rank, local):
     import torch
     import iroiro_b200 as ib
 
+    if world > 1:
+        # replicas: every rank runs the headline (and its e2e and variants);
+        # the solver sections are single-GPU configurations and would only
+        # hold the other GPUs while they run
+        args.no_solve = True
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     V = int(np.prod(L))
