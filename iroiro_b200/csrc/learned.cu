@@ -1413,6 +1413,14 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
     const double rr_start = rr;
     double rr_it = rr;  // the iterated |r|^2
     std::vector<double> nw(m, 0.0);
+    // The z_j are kept as the network produced them; the orthogonalised
+    // directions are z'_j = sum_i T[i][j] z_i (T unit upper triangular, from
+    // the Gram-Schmidt coefficients of the w_j), and the correction of the
+    // cycle e = sum_j alpha_j z'_j = sum_i gamma_i z_i is formed once at its
+    // end: one pass over the z_i instead of updating z_j and e every step.
+    std::vector<std::vector<std::complex<double>>> T(m, std::vector<std::complex<double>>(m));
+    std::vector<std::complex<double>> alph(m);
+    int jdone = 0;
     for (int j = 0; j < m && iters < prm->max_iter; ++j) {
       // z_j = N(r) (or r without a network), w_j = A z_j
       if (net) {
@@ -1425,27 +1433,40 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
       }
       LRC(apply(c, op, mass, csw, false, *Z[j], *t32, nullptr, 0, nullptr));
       LRC(apply(c, op, mass, csw, true, *t32, *W[j], nullptr, 0, nullptr));
+      for (int i = 0; i < m; ++i) T[i][j] = 0.0;
+      T[j][j] = 1.0;
       if (j > 0) {
-        std::vector<const DevField*> ws(W.begin(), W.begin() + j), zs(Z.begin(), Z.begin() + j);
+        std::vector<const DevField*> ws(W.begin(), W.begin() + j);
         std::vector<std::complex<double>> cw;
         LRC(cdots(ws, *W[j], cw));
         std::vector<std::complex<double>> beta(j);
         for (int q = 0; q < j; ++q) beta[q] = -cw[q] / nw[q];
         LRC(caxpy(ws, beta, *W[j]));
-        LRC(caxpy(zs, beta, *Z[j]));
+        // z'_j = z_j + sum_q beta_q z'_q
+        for (int q = 0; q < j; ++q)
+          for (int i = 0; i <= q; ++i) T[i][j] += beta[q] * T[i][q];
       }
       // |w_j|^2 and <w_j, r> in one pass: <w_j, w_j> and <r, w_j> = conj(<w_j, r>)
       std::vector<std::complex<double>> g;
       LRC(cdots({W[j], r32}, *W[j], g));
       nw[j] = g[0].real();
       const std::complex<double> alpha = std::conj(g[1]) / nw[j];
-      LRC(caxpy({Z[j]}, {alpha}, *e32));
+      alph[j] = alpha;
+      jdone = j + 1;
       LRC(caxpy({W[j]}, {-alpha}, *r32));
       // the new |r|^2 = |r|^2 - |<w_j, r>|^2 / |w_j|^2 (r minus its projection
       // on w_j); only the restart test reads it, the FP64 residual decides
       rr_it = rr_it - std::norm(g[1]) / nw[j];
       ++iters;
       if (rr_it < target || rr_it < delta * delta * rr_start) break;
+    }
+    // e = sum_i gamma_i z_i, gamma = T alpha
+    if (jdone > 0) {
+      std::vector<const DevField*> zs(Z.begin(), Z.begin() + jdone);
+      std::vector<std::complex<double>> gam(jdone);
+      for (int i = 0; i < jdone; ++i)
+        for (int j = i; j < jdone; ++j) gam[i] += T[i][j] * alph[j];
+      LRC(caxpy(zs, gam, *e32));
     }
     // x += e, r = b - A x in FP64
     LCK(launch_mx_merge(PREC_SINGLE, X->sites(), 1, X->all(), e32->all(), dmask, st));
