@@ -2,7 +2,7 @@
 
 Workload (one "step"): one application of the even-odd Schur operator
 Dirac_Wilson_EvenOdd<Dirac_Wilson>::mult, M f_e = f_e - kappa^2 H_eo H_oe f_e
-(lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:80-84), on a 32^3x64 lattice, kappa =
+(lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:79-83), on a 32^3x64 lattice, kappa =
 0.12, seeded synthetic SU(3) links exp(i*0.2*H) followed by a random gauge
 transformation, FP64 storage and arithmetic (the reference's own arithmetic),
 reconstruct-12 links.  One step = two launches of the hopping kernel.
@@ -18,7 +18,9 @@ value     GB/s of the step on compulsory bytes, fields resident in HBM, L2
           roofline.algorithmic_GBps.
 e2e       the same metric through the C ABI with host buffers:
           iro_dirac_apply() on pinned Format_F arrays, H2D + D2H inside the
-          timed region.
+          timed region (the library moves the field in chunks of t-slices,
+          both copy directions overlapped with each other and the stencils;
+          equals_plain_path: the result equals the unchunked path's bitwise).
 roofline  achieved = compulsory bytes per step / mean step time; traffic =
           DRAM bytes (read + write) of one step from the committed ncu
           capture of this lattice, scaled by the sites processed.
@@ -738,6 +740,8 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     e2e_ms = reduce_max(es.elapsed_time(ee), world)
     e2e_val = world * step_bytes * args.steps / (e2e_ms * 1e-3) / 1e9
+    # page-locked arrays take the overlapped path, pageable ones the plain one
+    e2e_exact = bool(np.array_equal(hout.numpy(), ctx.apply(ib.OP_WILSON_SCHUR_EE, MASS, 0.0, 0, h)))
 
     # other precisions and operators, same protocol (reported, not the headline)
     nvar = max(10, min(args.steps, 200))
@@ -812,7 +816,8 @@ def run_ours(args, world, rank, local):
                                                 "spinors + 8 links + output) + f_e",
                      "gflops": round(FLOPS_SCHUR * Vh / t_step / 1e9, 1)},
         "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": 24 * 8 * Vh,
-                "d2h_bytes_per_step": 24 * 8 * Vh, "ms_per_step": round(e2e_ms / args.steps, 3)},
+                "d2h_bytes_per_step": 24 * 8 * Vh, "ms_per_step": round(e2e_ms / args.steps, 3),
+                "equals_plain_path": e2e_exact},
         "gpu_launches": 2 * args.steps,
         "clocks": ck,
         "cpu_baseline": cpu,

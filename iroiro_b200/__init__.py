@@ -263,11 +263,18 @@ class Context:
             self._gauge_ref = u
 
     def apply(self, op: int, mass: float, csw: float, dag: bool, f: np.ndarray, prec=PREC_DOUBLE,
-              nrhs: int = 1) -> np.ndarray:
+              nrhs: int = 1, out: np.ndarray = None) -> np.ndarray:
+        """`out`, when given, is a contiguous float64 array of the result's size
+        (e.g. page-locked memory: the Schur operator between page-locked arrays
+        overlaps its copies with the stencils)."""
         full = op in (OP_WILSON_FULL, OP_CLOVER_FULL)
         n = (24 * self.V if full else 12 * self.V) * nrhs
         f = _f64(f, n, "spinor")
-        out = np.empty(n)
+        if out is None:
+            out = np.empty(n)
+        elif (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.size != n
+              or not out.flags.c_contiguous or not out.flags.writeable):
+            raise IroError(BAD_ARG, f"apply: out must be a writable contiguous float64 array of {n}")
         self.check(self._lib.iro_dirac_apply(self.h, op, mass, csw, int(bool(dag)), _PREC[prec],
                                              _ptr(f), _ptr(out), nrhs), "iro_dirac_apply")
         return out

@@ -57,6 +57,10 @@ struct iro_ctx {
   // pinned host ring for large copies to and from pageable host memory
   char* ring[2] = {nullptr, nullptr};
   cudaEvent_t ring_ev[2] = {nullptr, nullptr};
+  // copy streams (host-to-device, device-to-host) and chunk events of the
+  // overlapped Schur operator between pinned host arrays
+  cudaStream_t xs[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> xev;
 
   // reduction scratch and solver state
   double* partials = nullptr;
@@ -370,8 +374,12 @@ static cudaError_t launch_variant(iro_ctx* c, HopLaunch L, cudaStream_t st) {
   return launch_hop(L, st);
 }
 
+std::tuple<int, int, int, int, int, int> tune_key(const HopLaunch& L) {
+  return std::make_tuple(L.prec, L.recon, int(L.dag), L.epi, L.nrhs, L.nparity);
+}
+
 int launch_tuned(iro_ctx* c, HopLaunch L) {
-  auto key = std::make_tuple(L.prec, L.recon, int(L.dag), L.epi, L.nrhs, L.nparity);
+  const auto key = tune_key(L);
   cudaStream_t st = c->stream;
   static const char* forced = std::getenv("IRO_HOP_VARIANT");
   auto it = c->tuned.find(key);
@@ -433,6 +441,29 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
   return IRO_OK;
 }
 
+// The two stencils of the even/odd Schur operator on fields of L1's
+// precision, dagger and nrhs (L1 comes from base_launch):
+//   L1: t_o   = [A_oo^-1] (-kappa H_oe f_e)
+//   L2: out_e = [A_ee] f_e + kappa H_eo t_o  =  f - Deo(Doe f)
+// (Dirac_Wilson_EvenOdd::mult, lib/Dirac_ops/dirac_wilson_EvenOdd.hpp:79-83)
+void schur_launches(iro_ctx* c, bool cl, double k, const DevField& in, DevField& t,
+                    DevField& out, HopLaunch& L1, HopLaunch& L2) {
+  L2 = L1;
+  L1.p0 = 1;
+  L1.in[0] = in.half(0);
+  L1.out[0] = t.half(1);
+  L1.epi = cl ? EPI_SCALE_CLOV : EPI_SCALE;
+  if (cl) L1.clov[0] = clover_ptr(c, L1.prec, 1, true);
+  L1.scale = -k;
+  L2.p0 = 0;
+  L2.in[0] = t.half(1);
+  L2.out[0] = out.half(0);
+  L2.xin[0] = in.half(0);
+  L2.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
+  if (cl) L2.clov[0] = clover_ptr(c, L1.prec, 0, false);
+  L2.scale = k;
+}
+
 // out = op(in) on device fields.  `red`/`red_mask`, when given, attach a
 // reduction to the last kernel of the operator (|out|^2, |xin|^2, (xin,out)),
 // and `skip` lets converged right-hand sides be left untouched.
@@ -489,25 +520,10 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
       int rc = IRO_OK;
       DevField* t = ws(c, 1, prec, nrhs, 0, &rc);
       if (!t) return rc;
-      const bool cl = op == IRO_OP_CLOVER_SCHUR_EE;
-      // t_o = [A_oo^-1] (-kappa H_oe f_e)
-      L.p0 = 1;
-      L.in[0] = in.half(0);
-      L.out[0] = t->half(1);
-      L.epi = cl ? EPI_SCALE_CLOV : EPI_SCALE;
-      if (cl) L.clov[0] = clover_ptr(c, prec, 1, true);
-      L.scale = -k;
-      { int rt = launch_tuned(c, L); if (rt) return rt; }
-      // out_e = [A_ee] f_e + kappa H_eo t_o  =  f - Deo(Doe f)
-      HopLaunch L2 = base_launch(c, prec, dag, nrhs);
+      HopLaunch L2;
+      schur_launches(c, op == IRO_OP_CLOVER_SCHUR_EE, k, in, *t, out, L, L2);
       L2.skip = skip;
-      L2.p0 = 0;
-      L2.in[0] = t->half(1);
-      L2.out[0] = out.half(0);
-      L2.xin[0] = in.half(0);
-      L2.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
-      if (cl) L2.clov[0] = clover_ptr(c, prec, 0, false);
-      L2.scale = k;
+      { int rt = launch_tuned(c, L); if (rt) return rt; }
       if (red) { L2.red = *red; L2.red_mask = red_mask; }
       if (fuse) {
         L2.cg = 1;
@@ -707,7 +723,10 @@ int iro_ctx_destroy(iro_ctx* c) {
   for (int i = 0; i < 2; ++i) {
     if (c->ring[i]) cudaFreeHost(c->ring[i]);
     if (c->ring_ev[i]) cudaEventDestroy(c->ring_ev[i]);
+    if (c->xs[i]) cudaStreamDestroy(c->xs[i]);
   }
+  for (cudaEvent_t e : c->xev)
+    if (e) cudaEventDestroy(e);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return IRO_OK;
@@ -793,12 +812,137 @@ int iro_field_strength(iro_ctx* c, int mu, int nu, double* out) {
   return copy_d2h(c, out, c->stage, bytes);
 }
 
+// The even/odd Schur operator between pinned host arrays with the copies
+// overlapped.  The even half field moves in chunks of whole t-slices, host to
+// device on one copy stream and device to host on another, so that both
+// directions of the host link are busy at once, and the stencils of a chunk
+// run as soon as the chunks they read have arrived: chunk j of the odd
+// intermediate reads input chunks j-1..j+1 (a t hop crosses one slice), and
+// chunk j of the output reads intermediate chunks j-1..j+1.  The input goes
+// in the order n-1, 0, 1, ..., n-2; output chunk j leaves once its
+// neighbourhood is complete, the five around chunk n-2 last.  The stage
+// buffer holds both directions: output chunk j overwrites input chunk j
+// after the import of j has read it (both on the compute stream).  Every
+// site is computed by the kernels of apply_dev, so the result is the same to
+// the bit.  Returns with *handled false (and nothing done) when the
+// stencils are not tuned yet: the caller takes the plain path, which tunes.
+constexpr int kPipeMaxChunks = 64;
+constexpr size_t kPipeMinChunkBytes = size_t(4) << 20;
+
+int pipe_chunks(const iro_ctx* c) {
+  const size_t slice = size_t(c->g.st) * 24 * sizeof(double);
+  int per = int((kPipeMinChunkBytes + slice - 1) / slice);
+  if (const char* e = std::getenv("IRO_PIPE_SLICES")) per = std::max(1, std::atoi(e));
+  const int n = c->L[3] / per;
+  return n < kPipeMaxChunks ? n : kPipeMaxChunks;
+}
+
+int schur_host_pipelined(iro_ctx* c, int op, double mass, double csw, bool dag, int prec,
+                         const double* in, double* out, bool* handled) {
+  *handled = false;
+  const int n = pipe_chunks(c);
+  const bool cl = op == IRO_OP_CLOVER_SCHUR_EE;
+  if (cl) RCK(ensure_clover(c, mass, csw));
+  int rc = IRO_OK;
+  DevField* fi = ws(c, 0, prec, 1, 10, &rc);
+  if (!fi) return rc;
+  DevField* fo = ws(c, 0, prec, 1, 11, &rc);
+  if (!fo) return rc;
+  DevField* t = ws(c, 1, prec, 1, 0, &rc);
+  if (!t) return rc;
+  HopLaunch L1 = base_launch(c, prec, dag, 1), L2;
+  schur_launches(c, cl, kappa_of(mass), *fi, *t, *fo, L1, L2);
+  if (!c->tuned.count(tune_key(L1)) || !c->tuned.count(tune_key(L2))) return IRO_OK;
+  RCK(ensure_stage(c, size_t(c->Vh) * 24 * sizeof(double)));
+  for (int i = 0; i < 2; ++i)
+    if (!c->xs[i]) CK(cudaStreamCreateWithFlags(&c->xs[i], cudaStreamNonBlocking));
+  while (c->xev.size() < size_t(2 * kPipeMaxChunks + 1)) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->xev.push_back(e);
+  }
+  *handled = true;
+  cudaStream_t cs = c->stream, h2d = c->xs[0], d2h = c->xs[1];
+  cudaEvent_t* arrived = c->xev.data();
+  cudaEvent_t* exported = arrived + kPipeMaxChunks;
+  cudaEvent_t start = arrived[2 * kPipeMaxChunks];
+  // chunk j: half-sites [lo(j), lo(j + 1)), whole t-slices (host index = half-site)
+  auto lo = [&](int j) { return int64_t(j) * c->L[3] / n * c->g.st; };
+  auto run = [&]() -> int {
+    CK(cudaEventRecord(start, cs));  // earlier work of the stream may still use the stage
+    CK(cudaStreamWaitEvent(h2d, start, 0));
+    for (int q = 0; q < n; ++q) {
+      const int j = (q + n - 1) % n;
+      CK(cudaMemcpyAsync(c->stage + lo(j) * 24, in + lo(j) * 24,
+                         size_t(lo(j + 1) - lo(j)) * 24 * sizeof(double), cudaMemcpyHostToDevice, h2d));
+      CK(cudaEventRecord(arrived[j], h2d));
+    }
+    auto import = [&](int j) -> int {
+      CK(cudaStreamWaitEvent(cs, arrived[j], 0));
+      CK(launch_import_spinor(c->g, c->stage, 1, 0, c->Vh, 1, prec, fi->half(0), cs, lo(j),
+                              lo(j + 1) - lo(j)));
+      return IRO_OK;
+    };
+    auto hop1 = [&](int j) -> int {
+      L1.hs0 = int(lo(j));
+      L1.nhs = int(lo(j + 1) - lo(j));
+      return launch_tuned(c, L1);
+    };
+    auto hop2 = [&](int j) -> int {
+      L2.hs0 = int(lo(j));
+      L2.nhs = int(lo(j + 1) - lo(j));
+      RCK(launch_tuned(c, L2));
+      CK(launch_export_spinor(c->g, c->stage, 1, 0, c->Vh, 1, prec, fo->half(0), cs, lo(j),
+                              lo(j + 1) - lo(j)));
+      CK(cudaEventRecord(exported[j], cs));
+      CK(cudaStreamWaitEvent(d2h, exported[j], 0));
+      CK(cudaMemcpyAsync(out + lo(j) * 24, c->stage + lo(j) * 24,
+                         size_t(lo(j + 1) - lo(j)) * 24 * sizeof(double), cudaMemcpyDeviceToHost, d2h));
+      return IRO_OK;
+    };
+    RCK(import(n - 1));
+    RCK(import(0));
+    RCK(import(1));
+    RCK(hop1(0));
+    for (int k = 2; k <= n - 2; ++k) {
+      RCK(import(k));
+      RCK(hop1(k - 1));
+      if (k >= 3) RCK(hop2(k - 2));
+    }
+    RCK(hop1(n - 2));
+    RCK(hop1(n - 1));
+    for (int j : {n - 3, n - 2, n - 1, 0}) RCK(hop2(j));
+    return IRO_OK;
+  };
+  rc = run();
+  // the copies read and write the caller's arrays: wait for them on every path
+  const cudaError_t e1 = cudaStreamSynchronize(h2d);
+  const cudaError_t e2 = cudaStreamSynchronize(d2h);
+  const cudaError_t e3 = cudaStreamSynchronize(cs);
+  if (rc) return rc;
+  CK(e1);
+  CK(e2);
+  CK(e3);
+  return IRO_OK;
+}
+
 int iro_dirac_apply(iro_ctx* c, int op, double mass, double csw, int dagger, int prec,
                     const double* in, double* out, int nrhs) {
   if (!c || !in || !out || nrhs < 1 || nrhs > kMaxRhs || prec < 0 || prec > 2 || !op_valid(op))
     return fail(c, IRO_BAD_ARG, "bad operator arguments");
   CK(cudaSetDevice(c->device));
   int rc = IRO_OK;
+  if (nrhs == 1 && (op == IRO_OP_WILSON_SCHUR_EE || op == IRO_OP_CLOVER_SCHUR_EE) && c->has_gauge &&
+      (prec == PREC_DOUBLE || c->recon == 12) && pipe_chunks(c) >= 6 &&
+      (out + c->Vh * 24 <= in || in + c->Vh * 24 <= out) && host_pinned(in) && host_pinned(out)) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c->stream, &cs));
+    if (cs == cudaStreamCaptureStatusNone) {
+      bool handled = false;
+      rc = schur_host_pipelined(c, op, mass, csw, dagger != 0, prec, in, out, &handled);
+      if (rc || handled) return rc;
+    }
+  }
   const int si = input_subset(op), so = output_subset(op);
   DevField* fi = ws(c, si, prec, nrhs, 10, &rc);
   if (!fi) return rc;

@@ -161,6 +161,8 @@ struct HopParams {
   int cg;
   SpinorPtr cr[2];  // indexed like out[]
   const CGState* cst;
+  // the output half-sites [hs0, hs0 + nhs) of this launch (all: 0, Vh)
+  int hs0, nhs;
 };
 
 // VAR bit 0: at least two 256-thread blocks per SM (register cap 128);
@@ -193,12 +195,13 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
   const int yi = blockIdx.y;
   const int p = P.p0 ^ yi;
   const int nrhs = P.nrhs;
-  const int nthreads = P.g.Vh * nrhs;  // < 2^31, checked at context creation
+  const int nthreads = P.nhs * nrhs;  // < 2^31, checked at context creation
+  const int e0 = P.hs0 * nrhs;         // element index of the first output
   double red[3] = {0.0, 0.0, 0.0};
   // the grid stride is a multiple of nrhs, so each thread keeps one rhs
   const int r = (nrhs == 1) ? 0 : int((blockIdx.x * blockDim.x + threadIdx.x) % unsigned(nrhs));
-  for (int tid = blockIdx.x * blockDim.x + threadIdx.x; tid < nthreads;
-       tid += gridDim.x * blockDim.x) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nthreads; t += gridDim.x * blockDim.x) {
+    const int tid = e0 + t;
     const int hs = (nrhs == 1) ? tid : int(unsigned(tid) / unsigned(nrhs));
     if (P.skip && P.skip[r]) continue;
     const Coord c = coord_of(P.g, hs, p);

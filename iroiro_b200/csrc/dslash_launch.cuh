@@ -31,7 +31,9 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   for (int i = 0; i < 2; ++i) {
     P.cr[i] = L.cr[i];
   }
-  LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs, L.max_blocks,
+  P.hs0 = L.hs0;
+  P.nhs = L.nhs < 0 ? L.g.Vh - L.hs0 : L.nhs;
+  LaunchCfg c = launch_cfg(P.nhs, L.nrhs, L.max_blocks,
                            L.block_cap < HopBounds<VAR>::threads ? L.block_cap
                                                                  : HopBounds<VAR>::threads);
   // programmatic dependent launch: the blocks of this grid may be scheduled
@@ -57,7 +59,7 @@ static cudaError_t hop_go_pair(const HopLaunch& L, cudaStream_t st) {
   if constexpr (SP == PREC_DOUBLE || RECON != 12) {
     return cudaErrorInvalidValue;
   } else {
-    if (L.nrhs % 2 != 0) return cudaErrorInvalidValue;
+    if (L.nrhs % 2 != 0 || L.hs0 != 0 || (L.nhs >= 0 && L.nhs != L.g.Vh)) return cudaErrorInvalidValue;
     HopParams P;
     P.g = L.g;
     P.p0 = L.p0;
@@ -91,7 +93,7 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
   if constexpr (SP == PREC_DOUBLE || RECON != 12) {
     return cudaErrorInvalidValue;
   } else {
-    if (L.nrhs % 2 != 0) return cudaErrorInvalidValue;
+    if (L.nrhs % 2 != 0 || L.hs0 != 0 || (L.nhs >= 0 && L.nhs != L.g.Vh)) return cudaErrorInvalidValue;
     HopParams P;
     P.g = L.g;
     P.p0 = L.p0;

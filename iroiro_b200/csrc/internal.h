@@ -59,6 +59,10 @@ struct HopLaunch {
   int cg = 0;
   SpinorPtr cr[2];
   const CGState* cst = nullptr;
+  // output half-sites [hs0, hs0 + nhs) only (nhs < 0: all); one-RHS-per-thread
+  // variants only (the overlapped host-array path)
+  int hs0 = 0;
+  int nhs = -1;
 };
 cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st);
 
@@ -136,12 +140,13 @@ cudaError_t launch_mx_p(int plo, int64_t sites, int nrhs, SpinorPtr p, SpinorPtr
 // host Format_F doubles (already on the device in `stage`) <-> device field.
 // layout 0: full lexicographic lattice; 1: half field of parity p (hs order).
 // nrhs consecutive host fields of `host_sites` sites each.
+// [hs0, hs0 + nhs): the half-sites converted (nhs < 0: to the end)
 cudaError_t launch_import_spinor(const Geom& g, const double* stage, int layout, int p,
                                  int64_t host_sites, int nrhs, int prec, SpinorPtr out,
-                                 cudaStream_t st);
+                                 cudaStream_t st, int64_t hs0 = 0, int64_t nhs = -1);
 cudaError_t launch_export_spinor(const Geom& g, double* stage, int layout, int p,
                                  int64_t host_sites, int nrhs, int prec, SpinorPtr in,
-                                 cudaStream_t st);
+                                 cudaStream_t st, int64_t hs0 = 0, int64_t nhs = -1);
 // F (a full-lattice FP64 field of F.nrhs right-hand sides) = the spin-colour
 // point sources r = first .. first + F.nrhs - 1 at half-site hs of parity p:
 // right-hand side j is 1 at the real part of spin-colour component first + j

@@ -634,10 +634,9 @@ __device__ __forceinline__ int64_t host_site(const Geom& g, int layout, int p, i
 
 template <int SP>
 __global__ void import_kernel(Geom g, const double* stage, int layout, int p, int64_t host_sites,
-                              int nrhs, SpinorPtr out) {
+                              int nrhs, SpinorPtr out, int64_t i0, int64_t n) {
   using R = typename SpinorIO<SP>::Real;
-  const int64_t n = int64_t(g.Vh) * nrhs;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+  for (int64_t i = i0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < i0 + n;
        i += int64_t(gridDim.x) * blockDim.x) {
     const int hs = int(i / nrhs);
     const int r = int(i - int64_t(hs) * nrhs);
@@ -651,10 +650,9 @@ __global__ void import_kernel(Geom g, const double* stage, int layout, int p, in
 
 template <int SP>
 __global__ void export_kernel(Geom g, double* stage, int layout, int p, int64_t host_sites,
-                              int nrhs, SpinorPtr in) {
+                              int nrhs, SpinorPtr in, int64_t i0, int64_t n) {
   using R = typename SpinorIO<SP>::Real;
-  const int64_t n = int64_t(g.Vh) * nrhs;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+  for (int64_t i = i0 + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < i0 + n;
        i += int64_t(gridDim.x) * blockDim.x) {
     const int hs = int(i / nrhs);
     const int r = int(i - int64_t(hs) * nrhs);
@@ -690,24 +688,28 @@ cudaError_t launch_point_sources(const DevField& F, int p, int64_t hs, int first
 
 cudaError_t launch_import_spinor(const Geom& g, const double* stage, int layout, int p,
                                  int64_t host_sites, int nrhs, int prec, SpinorPtr out,
-                                 cudaStream_t st) {
-  const int grid = grid_for(int64_t(g.Vh) * nrhs, 256);
+                                 cudaStream_t st, int64_t hs0, int64_t nhs) {
+  if (nhs < 0) nhs = g.Vh - hs0;
+  const int64_t i0 = hs0 * nrhs, n = nhs * nrhs;
+  const int grid = grid_for(n, 256);
   switch (prec) {
-    case PREC_DOUBLE: import_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out); break;
-    case PREC_SINGLE: import_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out); break;
-    default: import_kernel<PREC_HALF><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out); break;
+    case PREC_DOUBLE: import_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out, i0, n); break;
+    case PREC_SINGLE: import_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out, i0, n); break;
+    default: import_kernel<PREC_HALF><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, out, i0, n); break;
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_export_spinor(const Geom& g, double* stage, int layout, int p,
                                  int64_t host_sites, int nrhs, int prec, SpinorPtr in,
-                                 cudaStream_t st) {
-  const int grid = grid_for(int64_t(g.Vh) * nrhs, 256);
+                                 cudaStream_t st, int64_t hs0, int64_t nhs) {
+  if (nhs < 0) nhs = g.Vh - hs0;
+  const int64_t i0 = hs0 * nrhs, n = nhs * nrhs;
+  const int grid = grid_for(n, 256);
   switch (prec) {
-    case PREC_DOUBLE: export_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in); break;
-    case PREC_SINGLE: export_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in); break;
-    default: export_kernel<PREC_HALF><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in); break;
+    case PREC_DOUBLE: export_kernel<PREC_DOUBLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in, i0, n); break;
+    case PREC_SINGLE: export_kernel<PREC_SINGLE><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in, i0, n); break;
+    default: export_kernel<PREC_HALF><<<grid, 256, 0, st>>>(g, stage, layout, p, host_sites, nrhs, in, i0, n); break;
   }
   return cudaGetLastError();
 }
