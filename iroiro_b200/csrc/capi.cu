@@ -827,20 +827,42 @@ int iro_field_strength(iro_ctx* c, int mu, int nu, double* out) {
 // the bit.  Returns with *handled false (and nothing done) when the
 // stencils are not tuned yet: the caller takes the plain path, which tunes.
 constexpr int kPipeMaxChunks = 64;
-constexpr size_t kPipeMinChunkBytes = size_t(4) << 20;
+constexpr size_t kPipeMinChunkBytes = size_t(8) << 20;
 
-int pipe_chunks(const iro_ctx* c) {
+// The chunks' first t-slices b[0..n-1] (b[n] = Lt); returns n.  Chunks of
+// `per` slices (at least kPipeMinChunkBytes); when that is more than one
+// slice, chunks 0..3 and n-4..n-1 (the first input chunks to arrive and the
+// output chunks that wait for the last one) are single slices, which
+// shortens the pipeline's fill and drain.
+int pipe_plan(const iro_ctx* c, int* b) {
+  const int Lt = c->L[3];
   const size_t slice = size_t(c->g.st) * 24 * sizeof(double);
   int per = int((kPipeMinChunkBytes + slice - 1) / slice);
   if (const char* e = std::getenv("IRO_PIPE_SLICES")) per = std::max(1, std::atoi(e));
-  const int n = c->L[3] / per;
-  return n < kPipeMaxChunks ? n : kPipeMaxChunks;
+  int n = 0;
+  if (per > 1 && Lt - 8 >= 2 * per) {
+    const int mid = Lt - 8, m = std::min(mid / per, kPipeMaxChunks - 8);
+    for (int k = 0; k < 4; ++k) b[n++] = k;
+    for (int i = 0; i < m; ++i) b[n++] = 4 + i * mid / m;
+    for (int k = 0; k < 4; ++k) b[n++] = Lt - 4 + k;
+  } else {
+    const int m = std::min(std::max(Lt / per, 1), kPipeMaxChunks);
+    for (int i = 0; i < m; ++i) b[n++] = i * Lt / m;
+  }
+  b[n] = Lt;
+  return n;
+}
+
+int pipe_chunks(const iro_ctx* c) {
+  int b[kPipeMaxChunks + 1];
+  return pipe_plan(c, b);
 }
 
 int schur_host_pipelined(iro_ctx* c, int op, double mass, double csw, bool dag, int prec,
                          const double* in, double* out, bool* handled) {
   *handled = false;
-  const int n = pipe_chunks(c);
+  int b[kPipeMaxChunks + 1];
+  const int n = pipe_plan(c, b);
   const bool cl = op == IRO_OP_CLOVER_SCHUR_EE;
   if (cl) RCK(ensure_clover(c, mass, csw));
   int rc = IRO_OK;
@@ -867,7 +889,7 @@ int schur_host_pipelined(iro_ctx* c, int op, double mass, double csw, bool dag, 
   cudaEvent_t* exported = arrived + kPipeMaxChunks;
   cudaEvent_t start = arrived[2 * kPipeMaxChunks];
   // chunk j: half-sites [lo(j), lo(j + 1)), whole t-slices (host index = half-site)
-  auto lo = [&](int j) { return int64_t(j) * c->L[3] / n * c->g.st; };
+  auto lo = [&](int j) { return int64_t(b[j]) * c->g.st; };
   auto run = [&]() -> int {
     CK(cudaEventRecord(start, cs));  // earlier work of the stream may still use the stage
     CK(cudaStreamWaitEvent(h2d, start, 0));

@@ -185,7 +185,8 @@ def test_block_sizes_equal_single(prec, nrhs, op):
 @pytest.mark.parametrize("op,csw", [(ib.OP_WILSON_SCHUR_EE, 0.0), (ib.OP_CLOVER_SCHUR_EE, 1.0)])
 def test_schur_pinned_overlapped_equals_plain(big, prec, op, csw):
     """The Schur operator between page-locked arrays (chunked copies in both
-    directions overlapped with the stencils, 12 chunks at 24^3x48) gives the
+    directions overlapped with the stencils, 13 chunks at 24^3x48, single
+    t-slices among them) gives the
     plain path's result to the bit.  The first call of a shape may tune the
     stencils on the plain path; the calls after it take the overlapped one."""
     import torch
