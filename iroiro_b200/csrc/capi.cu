@@ -1077,6 +1077,9 @@ int apply_cg(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFie
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc) {
   return ws(c, subset, prec, nrhs, slot, rc);
 }
+bool workspace_exists(iro_ctx* c, int subset, int prec, int nrhs, int slot) {
+  return c->ws.count(std::make_tuple(subset, prec, nrhs, slot)) != 0;
+}
 int import_field(iro_ctx* c, const double* host, bool full, DevField& f) {
   return import_host(c, host, full ? 1 : 0, f);
 }

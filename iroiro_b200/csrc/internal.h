@@ -106,6 +106,26 @@ struct MSFields {
 };
 cudaError_t launch_ms_p(int prec, int64_t Vh, int nshift, const MSFields& f, SpinorPtr r,
                         const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st);
+// FP64 multishift with a residual window: the ring of residual slots and the
+// fold's fields
+struct SlotList {
+  SpinorPtr s[MSW_MAX + 1];
+};
+// r_{k+1} = r_k + beta (s + sigma0 p0) from slot k % nslots into slot
+// (k + 1) % nslots, |r_{k+1}|^2 (stage ST_MSW_R)
+cudaError_t launch_msw_r(int64_t Vh, const SlotList& sl, int nslots, SpinorPtr p0, SpinorPtr s,
+                         const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st);
+// p0 = alpha p0 + r_{k+1} (stage ST_MSW_P)
+cudaError_t launch_msw_p(int64_t Vh, const SlotList& sl, int nslots, SpinorPtr p0, const MSState* m,
+                         const Reduce& red, int max_blocks, cudaStream_t st);
+// Fold of a window of n iterations that began at k0, for shifts k < nx:
+//   x_k += X_k p_k + sum_{j<n} C_kj r_{k0+1+j};
+//   p_k  = P_k p_k + sum_{j<n} D_kj r_{k0+1+j}   (p formed for plo <= k < nx)
+// coef[k * kMswCoef + {0, 1, 2 + j, 2 + MSW_MAX + j}] = X_k, P_k, C_kj, D_kj;
+// r_{k0+1+j} is in slot (s1 + j) % nslots
+constexpr int kMswCoef = 2 + 2 * MSW_MAX;
+cudaError_t launch_msw_fold(int64_t Vh, const SlotList& sl, int nslots, int s1, int n,
+                            const MSFields& f, int nx, int plo, const double* coef, cudaStream_t st);
 // x64_k += xlo_k (FP32), xlo_k = 0 for k < n
 cudaError_t launch_ms_merge(int64_t Vh, int n, const MSFields& x64, const MSFields& xlo,
                             cudaStream_t st);

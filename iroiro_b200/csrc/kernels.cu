@@ -477,6 +477,144 @@ cudaError_t launch_ms_p(int prec, int64_t Vh, int nshift, const MSFields& f, Spi
   return cudaGetLastError();
 }
 
+// ---- FP64 multishift with a residual window ------------------------------------
+// The x and p of the shifts are not updated every iteration: the iteration
+// keeps its residuals r_k in a ring of slots, and every shift's x and p after
+// a window of iterations are linear combinations of its x and p before it and
+// of the window's residuals, with coefficients from the step scalars (formed
+// on the host, ms_run).  An iteration then moves shift 0's vectors only.
+
+// multiShiftSolver_CG.cpp:49-57 without the x update: s += sigma0 p0,
+// r += beta s, into the next slot
+__global__ void __launch_bounds__(256) msw_r_kernel(int64_t vh, SlotList sl, int nslots, SpinorPtr p0,
+                                                    SpinorPtr s, const MSState* m, Reduce red) {
+  double acc = 0.0;
+  if (!red.done[0]) {
+    const double beta = m->beta, s0 = m->sigma0;
+    const int it = m->iter;
+    const SpinorPtr rc = sl.s[it % nslots], rn = sl.s[(it + 1) % nslots];
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
+         i += int64_t(gridDim.x) * blockDim.x) {
+      Cx<double> rv[12], pv[12], sv[12];
+      SpinorIO<PREC_DOUBLE>::load(rc, i, rv);
+      SpinorIO<PREC_DOUBLE>::load(p0, i, pv);
+      SpinorIO<PREC_DOUBLE>::load(s, i, sv);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) {
+        sv[k] = sv[k] + s0 * pv[k];
+        rv[k] = rv[k] + beta * sv[k];
+      }
+      acc_norm<PREC_DOUBLE>(acc, rv);
+      SpinorIO<PREC_DOUBLE>::store(rn, i, rv);
+    }
+  }
+  block_reduce_finish<1>(red, &acc, 1, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_msw_r(int64_t Vh, const SlotList& sl, int nslots, SpinorPtr p0, SpinorPtr s,
+                         const MSState* m, const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, 1, max_blocks);
+  msw_r_kernel<<<c.grid, c.block, 0, st>>>(Vh, sl, nslots, p0, s, m, red);
+  return cudaGetLastError();
+}
+
+// multiShiftSolver_CG.cpp:59-63: p0 = alpha p0 + r; the reduction only
+// carries the stage (pruning, convergence, window full) to the last block
+__global__ void __launch_bounds__(256) msw_p_kernel(int64_t vh, SlotList sl, int nslots, SpinorPtr p0,
+                                                    const MSState* m, Reduce red) {
+  double acc = 0.0;
+  if (!red.done[0]) {
+    const double alpha = m->alpha;
+    const SpinorPtr rn = sl.s[(m->iter + 1) % nslots];
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < vh;
+         i += int64_t(gridDim.x) * blockDim.x) {
+      Cx<double> rv[12], pv[12];
+      SpinorIO<PREC_DOUBLE>::load(rn, i, rv);
+      SpinorIO<PREC_DOUBLE>::load(p0, i, pv);
+#pragma unroll
+      for (int k = 0; k < 12; ++k) pv[k] = alpha * pv[k] + rv[k];
+      SpinorIO<PREC_DOUBLE>::store(p0, i, pv);
+    }
+  }
+  block_reduce_finish<1>(red, &acc, 1, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_msw_p(int64_t Vh, const SlotList& sl, int nslots, SpinorPtr p0, const MSState* m,
+                         const Reduce& red, int max_blocks, cudaStream_t st) {
+  LaunchCfg c = launch_cfg(Vh, 1, max_blocks);
+  msw_p_kernel<<<c.grid, c.block, 0, st>>>(Vh, sl, nslots, p0, m, red);
+  return cudaGetLastError();
+}
+
+// One thread per (element, chunk, group of four shifts): lanes are 32
+// consecutive elements (a warp block's chunk q is 512 contiguous bytes),
+// threadIdx.y the chunk q of 12, and consecutive blocks the shift groups of
+// one tile of 32 elements, so that a tile's residual chunks come from DRAM
+// once and from L2 for the other groups.  A thread keeps its shifts' x and p
+// chunks in registers (few registers: several blocks per SM to cover the
+// load latency); the coefficients are staged in shared memory.
+constexpr int kFoldGroup = 4;
+__global__ void __launch_bounds__(32 * 12) msw_fold_kernel(int64_t vh, SlotList sl, int nslots, int s1, int n,
+                                                           MSFields f, int nx, int plo, int ngroups,
+                                                           const double* __restrict__ coef) {
+  __shared__ double cs[kFoldGroup * kMswCoef];
+  const int64_t tile = blockIdx.x / ngroups;
+  const int k0 = (blockIdx.x % ngroups) * kFoldGroup;
+  const int nk = min(kFoldGroup, nx - k0);
+  for (int t = threadIdx.y * 32 + threadIdx.x; t < nk * kMswCoef; t += 32 * 12)
+    cs[t] = coef[k0 * kMswCoef + t];
+  __syncthreads();
+  const int64_t i = tile * 32 + threadIdx.x;
+  if (i >= vh) return;
+  const int q = threadIdx.y;
+  double2 xa[kFoldGroup], pa[kFoldGroup];
+#pragma unroll
+  for (int k = 0; k < kFoldGroup; ++k) xa[k] = pa[k] = make_double2(0.0, 0.0);
+#pragma unroll 8
+  for (int j = 0; j < n; ++j) {
+    const double2 rv =
+        __ldg(chunk0<12>(static_cast<const double2*>(sl.s[(s1 + j) % nslots].data), i) + 32 * q);
+#pragma unroll
+    for (int k = 0; k < kFoldGroup; ++k) {
+      if (k < nk) {
+        const double C = cs[k * kMswCoef + 2 + j], D = cs[k * kMswCoef + 2 + MSW_MAX + j];
+        xa[k] = make_double2(fma(C, rv.x, xa[k].x), fma(C, rv.y, xa[k].y));
+        pa[k] = make_double2(fma(D, rv.x, pa[k].x), fma(D, rv.y, pa[k].y));
+      }
+    }
+  }
+  double2 pv[kFoldGroup], xv[kFoldGroup];
+#pragma unroll
+  for (int k = 0; k < kFoldGroup; ++k) {
+    if (k < nk) {
+      pv[k] = *(chunk0<12>(static_cast<const double2*>(f.p[k0 + k].data), i) + 32 * q);
+      xv[k] = *(chunk0<12>(static_cast<const double2*>(f.x[k0 + k].data), i) + 32 * q);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kFoldGroup; ++k) {
+    if (k < nk) {
+      const double X = cs[k * kMswCoef], P = cs[k * kMswCoef + 1];
+      *(chunk0<12>(static_cast<double2*>(f.x[k0 + k].data), i) + 32 * q) =
+          make_double2(xv[k].x + fma(X, pv[k].x, xa[k].x), xv[k].y + fma(X, pv[k].y, xa[k].y));
+      if (k0 + k >= plo)
+        *(chunk0<12>(static_cast<double2*>(f.p[k0 + k].data), i) + 32 * q) =
+            make_double2(fma(P, pv[k].x, pa[k].x), fma(P, pv[k].y, pa[k].y));
+    }
+  }
+}
+
+cudaError_t launch_msw_fold(int64_t Vh, const SlotList& sl, int nslots, int s1, int n,
+                            const MSFields& f, int nx, int plo, const double* coef, cudaStream_t st) {
+  if (nx < 1 || nx > MAXSHIFT || n < 1 || n > MSW_MAX) return cudaErrorInvalidValue;
+  const int ngroups = (nx + kFoldGroup - 1) / kFoldGroup;
+  const int64_t grid = (Vh + 31) / 32 * ngroups;
+  if (grid > 0x7fffffff) return cudaErrorInvalidValue;
+  msw_fold_kernel<<<unsigned(grid), dim3(32, 12), 0, st>>>(Vh, sl, nslots, s1, n, f, nx, plo, ngroups,
+                                                           coef);
+  return cudaGetLastError();
+}
+
 // reliable update of the mixed-precision multishift: x64_k += xlo_k, xlo_k = 0
 // for the shifts k < n (FP32 accumulators into the FP64 solutions)
 __global__ void ms_merge_kernel(int64_t vh, int n, MSFields x64, MSFields xlo) {

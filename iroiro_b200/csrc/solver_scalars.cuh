@@ -37,6 +37,9 @@ enum { RUNNING = 0, CONVERGED = 1, STOPPED = 2, PAUSED = 3 };
 // Multishift CG state (MultiShiftSolver_CG::solve_step,
 // lib/Solver/multiShiftSolver_CG.cpp:34-93); shift arrays have MAXSHIFT slots.
 constexpr int MAXSHIFT = 16;
+// iterations per window of the FP64 multishift solver that keeps the
+// residuals instead of updating every shift's x and p (ms_run)
+constexpr int MSW_MAX = 32;
 struct MSState {
   double rr, rrp, pap, alpha, beta, alphap, betap, snorm, prec, sigma0;
   double maxrr;   // (r,r) at the last reliable update (mixed precision)
@@ -44,6 +47,18 @@ struct MSState {
   int nshift, nshift2, iter, conv_iter;
   double csh2[MAXSHIFT], zeta1[MAXSHIFT], zeta2[MAXSHIFT], zeta[MAXSHIFT];
   double betas[MAXSHIFT], alphas[MAXSHIFT], pp[MAXSHIFT];
+  // Residual window (stages ST_MSW_*): the window began at iteration k0 and
+  // holds wsize iterations; q[k] is |p_k|^2 carried by its recurrence; the
+  // step scalars of window iteration w are kept for the host's fold:
+  // shift 0's beta and alpha, the shifts updated (nshift2) and every other
+  // shift's betas, alphas and zeta.
+  int k0, wsize;
+  double q[MAXSHIFT];
+  double hbeta[MSW_MAX], halpha[MSW_MAX];
+  int hn2[MSW_MAX];
+  double hbetas[MSW_MAX][MAXSHIFT], halphas[MSW_MAX][MAXSHIFT], hzeta[MSW_MAX][MAXSHIFT];
+  // the fold's coefficients, written by the host (launch_msw_fold)
+  double wcoef[MAXSHIFT * (2 + 2 * MSW_MAX)];
 };
 
 enum Stage {
@@ -53,7 +68,9 @@ enum Stage {
   ST_MS_ALPHA = 3,  // totals[0]=|Mp|^2, [1]=|p|^2   -> pap incl. sigma0, beta
   ST_MS_R = 4,      // totals[0] = (r,r)             -> alpha, zeta recurrences
   ST_MS_PP = 5,     // totals[k] = |p_k|^2 (k>=1)    -> pruning, convergence
-  ST_CG_INIT = 6    // totals[0] = (r,r), [1] = |b|^2 -> rr, target
+  ST_CG_INIT = 6,   // totals[0] = (r,r), [1] = |b|^2 -> rr, target
+  ST_MSW_R = 7,     // as ST_MS_R, and the step's scalars into the window history
+  ST_MSW_P = 8      // |p_k|^2 by recurrence -> pruning, convergence, window full
 };
 
 // blocks per first-level group of a reduction (see block_reduce_finish)
@@ -187,6 +204,61 @@ __device__ inline void stage_update(const Reduce& R, const double* tot, int nred
         R.done[0] = 1;
       } else if (m->iter >= R.max_iter) {
         R.done[0] = 2;
+      }
+    } break;
+    case ST_MSW_R: {
+      MSState* m = static_cast<MSState*>(R.state);
+      if (R.done[0]) break;
+      m->rr = tot[0];
+      m->alpha = m->rr / m->rrp;
+      m->pp[0] = m->rr;
+      const int w = m->iter - m->k0;
+      m->hbeta[w] = m->beta;
+      m->halpha[w] = m->alpha;
+      m->hn2[w] = m->nshift2;
+      const double alphah = 1.0 + m->alphap * m->beta / m->betap;
+      for (int k = 1; k < m->nshift2; ++k) {
+        double zeta = (alphah - m->csh2[k] * m->beta) / m->zeta1[k] + (1.0 - alphah) / m->zeta2[k];
+        zeta = 1.0 / zeta;
+        const double zr = zeta / m->zeta1[k];
+        m->betas[k] = m->beta * zr;
+        m->alphas[k] = m->alpha * zr * zr;
+        m->zeta[k] = zeta;
+        m->hbetas[w][k] = m->betas[k];
+        m->halphas[w][k] = m->alphas[k];
+        m->hzeta[w][k] = zeta;
+      }
+    } break;
+    case ST_MSW_P: {
+      MSState* m = static_cast<MSState*>(R.state);
+      if (R.done[0]) break;
+      // p_k' = alphas_k p_k + zeta_k r' with r' orthogonal to p_k (a CG
+      // residual is orthogonal to the Krylov space of the earlier
+      // iterations, which holds every p_k): |p_k'|^2 = alphas^2 |p_k|^2 +
+      // zeta^2 |r'|^2, anchored to the stored p_k's norms at every fold
+      for (int k = 1; k < m->nshift2; ++k) {
+        m->q[k] = m->alphas[k] * m->alphas[k] * m->q[k] + m->zeta[k] * m->zeta[k] * m->rr;
+        m->pp[k] = m->q[k] * m->snorm;
+        m->zeta2[k] = m->zeta1[k];
+        m->zeta1[k] = m->zeta[k];
+      }
+      for (int k = m->nshift2 - 1; k >= 0; --k) {
+        if (m->pp[k] > m->prec) {
+          m->nshift2 = k + 1;
+          break;
+        }
+      }
+      m->alphap = m->alpha;
+      m->betap = m->beta;
+      const int it = m->iter;
+      m->iter = it + 1;
+      if (m->rr * m->snorm < m->prec) {
+        m->conv_iter = it;
+        R.done[0] = CONVERGED;
+      } else if (m->iter >= R.max_iter) {
+        R.done[0] = STOPPED;
+      } else if (m->iter - m->k0 >= m->wsize) {
+        R.done[0] = PAUSED;  // the window is full: the host folds it
       }
     } break;
     case ST_CG_INIT: {

@@ -3,6 +3,7 @@
 // the device (solver_scalars.cuh); the host only launches a chunk of
 // iterations (optionally as one CUDA graph) and polls the convergence flags
 // between chunks.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -19,6 +20,7 @@ int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField&
 int apply_cg(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in,
              DevField& out, const Reduce& red, const int* skip, const CGFuse& fuse);
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
+bool workspace_exists(iro_ctx* c, int subset, int prec, int nrhs, int slot);
 int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
 int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
 // host <-> device copies (large pageable ones through the context's pinned ring)
@@ -251,6 +253,125 @@ extern "C" int iro_cg_solve_field(iro_ctx* c, int op, double mass, double csw,
 }
 
 // ---- multishift CG ---------------------------------------------------------------------
+// The iterations of MultiShiftSolver_CG::solve (multiShiftSolver_CG.cpp:34-93)
+// with a window of W residuals.  Shift 0's x and every other shift's x and p
+// are not touched per iteration: over a window that began at iteration k0,
+// each is a linear combination of its value at k0 and of the residuals
+// r_{k0+1}, r_{k0+2}, ... that the iteration leaves in the ring of slots:
+//   p_k <- alphas_k p_k + zeta_k r_{j+1},  x_k <- x_k - betas_k p_k
+// unrolled over the window's steps gives x_k = x_k + X p_k + sum_j C_j r_j
+// and p_k = P p_k + sum_j D_j r_j, with X, P, C_j, D_j formed on the host in
+// FP64 from the step scalars the device recorded (MSState::h*).  One pass
+// (launch_msw_fold) then updates all shifts: it reads the window's residuals
+// once instead of every shift's x and p once per iteration.  A shift is
+// updated exactly at the steps the reference updates it (nshift2 recorded
+// per step); its |p_k|^2 for the pruning test follows the recurrence of
+// stage ST_MSW_P between folds and is recomputed from the stored p_k at each
+// fold.  The slots: R = slot 0 holds r_0 = b; r_j goes to slot j % (W + 1).
+static int ms_window(iro_ctx* c, int op, double mass, double csw, const DevField* B, int nshift,
+                     int max_iter, MSState& m, const std::vector<DevField*>& slots, DevField* P0,
+                     DevField* Q, DevField* S, const MSFields& f, const std::vector<DevField*>& PS,
+                     double bb) {
+  cudaStream_t st = stream(c);
+  const int W = int(slots.size()) - 1, nslots = W + 1;
+  MSState* dm = static_cast<MSState*>(state(c));
+  const int* skip = done(c);
+  int* hdone = static_cast<int*>(pinned(c));
+  SlotList sl{};
+  for (int j = 0; j < nslots; ++j) sl.s[j] = slots[j]->all();
+  RC(axpby(c, 1.0, *B, 0.0, *B, *P0));  // p_0 = b, the live search direction
+  m.k0 = 0;
+  m.wsize = W;
+  for (int k = 0; k < nshift; ++k) m.q[k] = bb;  // |p_k|^2 = |b|^2
+  CK(cudaMemcpyAsync(dm, &m, sizeof(m), cudaMemcpyHostToDevice, st));
+  Reduce ralpha = reduce(c, ST_MS_ALPHA, max_iter);
+  Reduce rr = reduce(c, ST_MSW_R, max_iter);
+  Reduce rp = reduce(c, ST_MSW_P, max_iter);
+  auto body = [&](int n) -> int {
+    for (int i = 0; i < n; ++i) {
+      RC(apply(c, op, mass, csw, false, *P0, *Q, &ralpha, RED_OUT2 | RED_X2, skip));
+      RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
+      CK(launch_msw_r(B->sites(), sl, nslots, P0->all(), S->all(), dm, rr, max_blocks(c), st));
+      CK(launch_msw_p(B->sites(), sl, nslots, P0->all(), dm, rp, max_blocks(c), st));
+    }
+    return IRO_OK;
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (st != nullptr) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int brc = body(kChunk);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (brc) return brc;
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_error(c, e, "cudaGraphInstantiate");
+  }
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() { if (e) cudaGraphExecDestroy(e); }
+  } guard{exec};
+  // x_k += X p_k + sum C r, p_k = P p_k + sum D r for the steps since k0
+  auto fold = [&]() -> int {
+    const int n = m.iter - m.k0;
+    if (n <= 0) return IRO_OK;
+    int nx = 1;
+    for (int w = 0; w < n; ++w) nx = std::max(nx, m.hn2[w]);
+    for (int k = 0; k < nx; ++k) {
+      double X = 0.0, P = 1.0, C[MSW_MAX] = {}, D[MSW_MAX] = {};
+      for (int w = 0; w < n; ++w) {
+        if (k >= m.hn2[w]) continue;  // pruned before this step
+        const double bs = k == 0 ? m.hbeta[w] : m.hbetas[w][k];
+        const double as = k == 0 ? m.halpha[w] : m.halphas[w][k];
+        const double z = k == 0 ? 1.0 : m.hzeta[w][k];
+        X -= bs * P;  // x -= betas p
+        for (int j = 0; j < w; ++j) C[j] -= bs * D[j];
+        P *= as;  // p = alphas p + zeta r_{k0+1+w}
+        for (int j = 0; j < w; ++j) D[j] *= as;
+        D[w] = z;
+      }
+      double* cf = m.wcoef + k * kMswCoef;
+      cf[0] = X;
+      cf[1] = P;
+      for (int j = 0; j < MSW_MAX; ++j) {
+        cf[2 + j] = C[j];
+        cf[2 + MSW_MAX + j] = D[j];
+      }
+    }
+    CK(cudaMemcpyAsync(dm->wcoef, m.wcoef, sizeof(m.wcoef), cudaMemcpyHostToDevice, st));
+    CK(launch_msw_fold(B->sites(), sl, nslots, (m.k0 + 1) % nslots, n, f, nx, 1, dm->wcoef, st));
+    // shift 0's p is the live one; its stored copy is the next window's base
+    RC(axpby(c, 1.0, *P0, 0.0, *P0, *PS[0]));
+    return IRO_OK;
+  };
+  if (max_iter > 0) {
+    for (;;) {
+      if (exec) CK(cudaGraphLaunch(exec, st));
+      else RC(body(kChunk));
+      CK(cudaMemcpyAsync(hdone, done(c), sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (hdone[0] == RUNNING) continue;
+      const int status = hdone[0];
+      CK(cudaMemcpyAsync(&m, dm, sizeof(m), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      RC(fold());
+      if (status != PAUSED) break;
+      // the next window: |p_k|^2 from the folded p_k, the window's base, run on
+      for (int k = 1; k < m.nshift2; ++k) {
+        std::vector<double> pn;
+        RC(norms(c, *PS[k], nullptr, pn, nullptr));
+        m.q[k] = pn[0];
+      }
+      m.k0 = m.iter;
+      const int running = RUNNING;
+      CK(cudaMemcpyAsync(dm, &m, sizeof(m), cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(done(c), &running, sizeof(int), cudaMemcpyHostToDevice, st));
+    }
+  }
+  return IRO_OK;
+}
+
 // MultiShiftSolver_CG::solve (lib/Solver/multiShiftSolver_CG.cpp:95-185) in FP64.
 // The solve itself; the shifted solutions stay in the context's workspaces
 // (*xs_out), and are exported to x when x is given.
@@ -308,22 +429,42 @@ static int ms_run(iro_ctx* c, int op, double mass, double csw, const DevField* B
   // autotune the two operator launches outside the graph capture (scratch Q, S only)
   RC(apply(c, op, mass, csw, false, *PS[0], *Q, nullptr, 0, nullptr));
   RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, nullptr));
-  const MSState* dm = static_cast<const MSState*>(state(c));
-  Reduce ralpha = reduce(c, ST_MS_ALPHA, max_iter);
-  Reduce rr = reduce(c, ST_MS_R, max_iter);
-  Reduce rpp = reduce(c, ST_MS_PP, max_iter);
+  MSState* dm = static_cast<MSState*>(state(c));
   const int* skip = done(c);
-  auto body = [&](int n) -> int {
-    for (int i = 0; i < n; ++i) {
-      RC(apply(c, op, mass, csw, false, *PS[0], *Q, &ralpha, RED_OUT2 | RED_X2, skip));
-      RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
-      CK(launch_ms_xr(PREC_DOUBLE, B->sites(), XS[0]->all(), R->all(), PS[0]->all(), S->all(), dm,
-                      rr, max_blocks(c), st));
-      CK(launch_ms_p(PREC_DOUBLE, B->sites(), nshift, f, R->all(), dm, rpp, max_blocks(c), st));
+  // The residual window: slot 0 is R, slots 1..W further workspaces while the
+  // device keeps 2 GiB free.  With W >= 8 an iteration moves shift 0's
+  // vectors only and every W iterations one pass folds the window into all
+  // shifts' x and p (ms_window); otherwise every iteration updates them all.
+  std::vector<DevField*> slots{R};
+  for (int j = 1; j <= MSW_MAX; ++j) {
+    if (!workspace_exists(c, sub, PREC_DOUBLE, 1, 200 + j)) {
+      size_t fr = 0, tot = 0;
+      CK(cudaMemGetInfo(&fr, &tot));
+      if (fr < R->bytes_data + (size_t(2) << 30)) break;
     }
-    return IRO_OK;
-  };
-  RC(iterate(c, 1, max_iter, true, body));
+    DevField* sj = workspace(c, sub, PREC_DOUBLE, 1, 200 + j, &rc); if (!sj) return rc;
+    slots.push_back(sj);
+  }
+  const int W = int(slots.size()) - 1;
+  if (W >= 8) {
+    DevField* P0 = workspace(c, sub, PREC_DOUBLE, 1, 199, &rc); if (!P0) return rc;
+    RC(ms_window(c, op, mass, csw, B, nshift, max_iter, m, slots, P0, Q, S, f, PS, bn[0]));
+  } else {
+    Reduce ralpha = reduce(c, ST_MS_ALPHA, max_iter);
+    Reduce rr = reduce(c, ST_MS_R, max_iter);
+    Reduce rpp = reduce(c, ST_MS_PP, max_iter);
+    auto body = [&](int n) -> int {
+      for (int i = 0; i < n; ++i) {
+        RC(apply(c, op, mass, csw, false, *PS[0], *Q, &ralpha, RED_OUT2 | RED_X2, skip));
+        RC(apply(c, op, mass, csw, true, *Q, *S, nullptr, 0, skip));
+        CK(launch_ms_xr(PREC_DOUBLE, B->sites(), XS[0]->all(), R->all(), PS[0]->all(), S->all(), dm,
+                        rr, max_blocks(c), st));
+        CK(launch_ms_p(PREC_DOUBLE, B->sites(), nshift, f, R->all(), dm, rpp, max_blocks(c), st));
+      }
+      return IRO_OK;
+    };
+    RC(iterate(c, 1, max_iter, true, body));
+  }
   CK(cudaMemcpyAsync(&m, state(c), sizeof(m), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   // true residuals of every shift (multiShiftSolver_CG.cpp:166-177)

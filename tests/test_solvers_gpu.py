@@ -166,3 +166,27 @@ def test_multishift_mixed_12_shifts_8c8(inner):
         assert rel(xm[k], x64[k]) < TOL_SOL, k
         r = D.mult_dag(D.mult(xm[k])) + s * xm[k] - b
         assert np.linalg.norm(r) < 1.01 * TOL_RES * np.linalg.norm(b), k
+
+
+def test_multishift_windows_vs_oracle(port):
+    """12 shifts 1e-4..10 at 8^3x16 on the e/o Wilson operator, to
+    |r|^2/|b|^2 < 1e-22: more than 32 iterations, so the FP64 solver folds
+    several windows of residuals into the shifts' x and p.  The iteration
+    count equals the oracle's (MultiShiftSolver_CG restated), and every
+    shift's solution agrees with the oracle's to 1e-10."""
+    import oracle
+    L = [8, 8, 8, 16]
+    V = int(np.prod(L))
+    mass = 0.5 / 0.12 - 4
+    u = ib.synth_gauge(L, 0.2, 91, True)
+    c = ib.context(L)
+    c.upload_gauge(u, force=True)
+    D = ib.Dirac_Wilson_EvenOdd(mass, u, ctx=c)
+    b = ib.synth_gaussian(V // 2, 92)
+    shifts = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
+    xs = []
+    out = ib.MultiShiftSolver_CG(ib.Fopr_DdagD(D), 1e-22, 5000).solve(xs, b, shifts)
+    xo, nco, _ = port.multishift(L, u, oracle.WILSON_EO, mass, 0.0, b, shifts, 1e-22, 5000)
+    assert out.Nconv == nco and nco > 64
+    for k in range(len(shifts)):
+        assert rel(xs[k], xo[k]) < 1e-10, k
