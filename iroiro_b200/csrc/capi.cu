@@ -26,6 +26,12 @@ struct iro_field {
   DevField f;
 };
 
+// an autotuner choice: stencil variant, block size cap, and whether the grid
+// covers every site (one pass) or is capped at max_blocks (grid-stride loop)
+struct Tune {
+  int variant, block, free_grid;
+};
+
 struct iro_ctx {
   int L[4];
   Geom g;
@@ -73,7 +79,7 @@ struct iro_ctx {
   std::map<std::tuple<int, int, int, int>, DevField> ws;
 
   // stencil autotuner: (prec, recon, dag, epilogue, nrhs, nparity) -> (variant, block cap)
-  std::map<std::tuple<int, int, int, int, int, int>, std::pair<int, int>> tuned;
+  std::map<std::tuple<int, int, int, int, int, int>, Tune> tuned;
   std::map<std::tuple<int, int, int, int, int, int>, float> tuned_ms;
 };
 
@@ -343,8 +349,11 @@ HopLaunch base_launch(iro_ctx* c, int prec, bool dag, int nrhs) {
 // An untuned shape is timed once in every candidate configuration on the
 // caller's own fields (without reductions, so solver state is untouched; the
 // launch is idempotent) before the real launch; during stream capture the
-// default configuration is used.  IRO_HOP_VARIANT="<variant>,<block>" fixes
-// the choice.
+// default configuration is used.  IRO_HOP_VARIANT="<variant>,<block>[,<free
+// grid 0/1>]" fixes the choice.  The grid is either capped at max_blocks
+// blocks, whose threads loop over the sites, or covers every site in one
+// pass (launches with a reduction keep the cap: the reduction's scratch
+// holds max_blocks partials per parity).
 // Candidates (see hop_var): all precisions 0..3; FP64 4, 5 and, on an SU(3)
 // field, 6..11 = 0..5 on the stored 18-real links (no third-row
 // reconstruction: fewer FP64 operations, more link bytes); FP32/FP16 with an
@@ -387,12 +396,12 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
     // the forced variant, modulo the candidates of the shape: FP64 6 (12 on
     // an SU(3) field); otherwise 13, a variant the shape lacks falling back
     // to its number modulo 4
-    int v = 0, b = 256;
-    std::sscanf(forced, "%d,%d", &v, &b);
+    int v = 0, b = 256, g = 0;
+    std::sscanf(forced, "%d,%d,%d", &v, &b, &g);
     if (L.prec == PREC_DOUBLE) v %= (L.recon == 12 ? 12 : 6);
     else if (!variant_ok(L, v % kHopVariants)) v %= 4;
     else v %= kHopVariants;
-    c->tuned[key] = {v, b};
+    c->tuned[key] = Tune{v, b, g != 0};
     it = c->tuned.find(key);
   }
   if (it == c->tuned.end()) {
@@ -411,32 +420,35 @@ int launch_tuned(iro_ctx* c, HopLaunch L) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
-    std::pair<int, int> pick{0, 256};
+    Tune pick{0, 256, 0};
     for (int v = 0; v < kHopVariants; ++v)
-      for (int b : {256, 128}) {
-        if (!variant_ok(L, v)) continue;
-        T.variant = v;
-        T.block_cap = b;
-        CK(launch_variant(c, T, st));  // warm-up
-        CK(cudaEventRecord(e0, st));
-        for (int i = 0; i < 3; ++i) CK(launch_variant(c, T, st));
-        CK(cudaEventRecord(e1, st));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) {
-          best = ms;
-          pick = {v, b};
+      for (int b : {256, 128})
+        for (int g : {0, 1}) {
+          if (!variant_ok(L, v)) continue;
+          T.variant = v;
+          T.block_cap = b;
+          T.grid_free = g;
+          CK(launch_variant(c, T, st));  // warm-up
+          CK(cudaEventRecord(e0, st));
+          for (int i = 0; i < 3; ++i) CK(launch_variant(c, T, st));
+          CK(cudaEventRecord(e1, st));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best) {
+            best = ms;
+            pick = {v, b, g};
+          }
         }
-      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->tuned[key] = pick;
     c->tuned_ms[key] = best / 3;
     it = c->tuned.find(key);
   }
-  L.variant = it->second.first;
-  L.block_cap = it->second.second;
+  L.variant = it->second.variant;
+  L.block_cap = it->second.block;
+  L.grid_free = it->second.free_grid;
   CK(launch_variant(c, L, st));
   return IRO_OK;
 }
@@ -743,10 +755,10 @@ int iro_autotune_report(const iro_ctx* c, char* buf, int len) {
     auto ms = c->tuned_ms.find(k);
     std::snprintf(item, sizeof(item),
                   "%s{\"prec\":%d,\"recon\":%d,\"dag\":%d,\"epilogue\":%d,\"nrhs\":%d,"
-                  "\"parities\":%d,\"variant\":%d,\"block\":%d,\"ms\":%.5f}",
+                  "\"parities\":%d,\"variant\":%d,\"block\":%d,\"free_grid\":%d,\"ms\":%.5f}",
                   s.size() > 1 ? "," : "", std::get<0>(k), std::get<1>(k), std::get<2>(k),
-                  std::get<3>(k), std::get<4>(k), std::get<5>(k), kv.second.first, kv.second.second,
-                  ms == c->tuned_ms.end() ? -1.0 : double(ms->second));
+                  std::get<3>(k), std::get<4>(k), std::get<5>(k), kv.second.variant, kv.second.block,
+                  kv.second.free_grid, ms == c->tuned_ms.end() ? -1.0 : double(ms->second));
     s += item;
   }
   s += "]";

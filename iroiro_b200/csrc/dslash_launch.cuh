@@ -33,7 +33,7 @@ static cudaError_t hop_go(const HopLaunch& L, cudaStream_t st) {
   }
   P.hs0 = L.hs0;
   P.nhs = L.nhs < 0 ? L.g.Vh - L.hs0 : L.nhs;
-  LaunchCfg c = launch_cfg(P.nhs, L.nrhs, L.max_blocks,
+  LaunchCfg c = launch_cfg(P.nhs, L.nrhs, L.grid_cap(),
                            L.block_cap < HopBounds<VAR>::threads ? L.block_cap
                                                                  : HopBounds<VAR>::threads);
   // programmatic dependent launch: the blocks of this grid may be scheduled
@@ -80,7 +80,7 @@ static cudaError_t hop_go_pair(const HopLaunch& L, cudaStream_t st) {
     for (int i = 0; i < 2; ++i) {
       P.cr[i] = L.cr[i];
     }
-    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, L.block_cap);
+    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.grid_cap(), L.block_cap);
     dim3 grid(c.grid, L.nparity);
     hop_pair_kernel<SP, DAG, EPI, VAR><<<grid, c.block, 0, st>>>(P);
     return cudaGetLastError();
@@ -118,7 +118,7 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
     // to (FP32: 976 B per thread, so at most 232 threads)
     int cap = L.block_cap;
     while (cap > 32 && stage_bytes<SP>() * cap > 232448) cap /= 2;
-    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.max_blocks, cap);
+    LaunchCfg c = launch_cfg(L.g.Vh, L.nrhs / 2, L.grid_cap(), cap);
     if (stage_bytes<SP>() * c.block > 232448) return cudaErrorInvalidValue;
     const int smem = stage_bytes<SP>() * c.block;
     static int opted = 0;  // largest dynamic shared memory already allowed

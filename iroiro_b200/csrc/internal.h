@@ -63,6 +63,10 @@ struct HopLaunch {
   // variants only (the overlapped host-array path)
   int hs0 = 0;
   int nhs = -1;
+  // grid over every site instead of max_blocks (ignored when the launch
+  // reduces: the reduction scratch holds max_blocks partials per parity)
+  int grid_free = 0;
+  int grid_cap() const { return (grid_free && !red_mask && !cg) ? 0x7fffffff : max_blocks; }
 };
 cudaError_t launch_hop(const HopLaunch& L, cudaStream_t st);
 
