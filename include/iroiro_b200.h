@@ -225,7 +225,12 @@ int iro_cg_solve_field(iro_ctx* ctx, int op, double mass, double csw, const iro_
    convergence on shift 0 only, pruning of converged shifts by
    |p_i|^2/|b|^2 <= precision.  x holds nshift consecutive fields.  *diff is
    sqrt of the largest squared relative true residual, *nconv the iteration
-   index of convergence (-1 if not). */
+   index of convergence (-1 if not).  An iteration updates shift 0's vectors
+   only; the residuals of up to 32 iterations are kept and folded into every
+   shift's x and p in one pass.  The context keeps those residual fields (up
+   to 32 of the operator's size, as many as leave 2 GiB of device memory free;
+   below 8 every iteration updates all shifts) as workspaces until it is
+   destroyed. */
 int iro_multishift_cg_solve(iro_ctx* ctx, int op, double mass, double csw, const double* b,
                             int nshift, const double* shifts, double* x, double precision,
                             int max_iter, iro_solver_out* out, int* nconv);
