@@ -190,3 +190,31 @@ def test_multishift_windows_vs_oracle(port):
     assert out.Nconv == nco and nco > 64
     for k in range(len(shifts)):
         assert rel(xs[k], xo[k]) < 1e-10, k
+
+
+def test_multishift_stopped_mid_window_vs_oracle(port):
+    """Stopped by the iteration limit (45, inside the second window of
+    residuals): the solver reports IRO_NOT_CONVERGED and returns every
+    shift's x after 45 iterations, as the oracle does."""
+    import ctypes
+    import oracle
+    L = [8, 8, 8, 16]
+    V = int(np.prod(L))
+    mass = 0.5 / 0.12 - 4
+    u = ib.synth_gauge(L, 0.2, 93, True)
+    c = ib.context(L)
+    c.upload_gauge(u, force=True)
+    b = ib.synth_gaussian(V // 2, 94)
+    shifts = np.array([1e-4 * (1e5) ** (k / 11) for k in range(12)])
+    x = np.empty(b.size * shifts.size)
+    o = ib.SolverOut()
+    nconv = ctypes.c_int(0)
+    rc = c._lib.iro_multishift_cg_solve_mixed(c.h, ib.OP_WILSON_SCHUR_EE, mass, 0.0, ib._ptr(b),
+                                              shifts.size, ib._ptr(shifts), ib._ptr(x), 1e-22, 45,
+                                              ib.PREC_DOUBLE, ctypes.byref(o), ctypes.byref(nconv))
+    assert rc == ib.NOT_CONVERGED and nconv.value == -1
+    xo, nco, _ = port.multishift(L, u, oracle.WILSON_EO, mass, 0.0, b, shifts, 1e-22, 45)
+    assert nco == -1
+    x = x.reshape(shifts.size, -1)
+    for k in range(shifts.size):
+        assert rel(x[k], xo[k]) < 1e-10, k
