@@ -24,6 +24,10 @@ e2e       the same metric through the C ABI with host buffers:
 roofline  achieved = compulsory bytes per step / mean step time; traffic =
           DRAM bytes (read + write) of one step from the committed ncu
           capture of this lattice, scaled by the sites processed.
+reference_beside  the reference's full-lattice Wilson CG, e/o multishift CG (12
+          shifts) and full-lattice clover mult on one host core at 8^3x16,
+          beside ours through the host-array API (same inputs; iteration
+          counts reported for both).
 summary   (last key) the headline numbers of every configuration.
 
 --impl reference runs the reference's own C++ (compiled from its sources
@@ -654,6 +658,105 @@ def cpu_baseline_leg():
                       f"({s:.1f} s)"}
 
 
+# The reference's solvers and clover operator on the host cores, beside ours on the GPU, at a
+# size where the reference finishes in seconds (8^3x16): full-lattice Wilson CG (D^dag D to
+# |r|^2/|b|^2 < 1e-20), e/o multishift CG (12 shifts 1e-4..10) and the full-lattice clover mult
+# (the reference's takes ~24 s per call at 24^3x48 on one core).  The reference keeps one
+# lattice per process, so it runs in a child process that loads only oracle/ libraries; its
+# results go to a file (the reference's clover prints on every call).
+REF_SOLVER_SPECS = {
+    "8x8x8x16": {"L": [8, 8, 8, 16], "seed": SEED + 500},
+}
+SHIFTS12 = [1e-4 * (1e5) ** (k / 11) for k in range(12)]
+
+
+def ref_solver_child(name, path):
+    import oracle
+    spec = REF_SOLVER_SPECS[name]
+    Lr = spec["L"]
+    V = int(np.prod(Lr))
+    P = oracle.port()
+    R = oracle.ref()
+    R.init(Lr)
+    u = P.synth_gauge(Lr, EPS, spec["seed"], True)
+    out = {}
+    b = P.synth_gaussian(V, spec["seed"] + 1)
+    t = time.perf_counter()
+    _, it, diff, _ = R.cg(u, oracle.WILSON_FULL, MASS, 0.0, b, 1e-20, 5000)
+    out["cg_wilson_full"] = {"ms": (time.perf_counter() - t) * 1e3, "iterations": it, "diff": diff}
+    bh = P.synth_gaussian(V // 2, spec["seed"] + 2)
+    t = time.perf_counter()
+    _, nc, diff = R.multishift(u, oracle.WILSON_EO, MASS, 0.0, bh, SHIFTS12, 1e-20, 5000)
+    out["multishift12_wilson_eo"] = {"ms": (time.perf_counter() - t) * 1e3, "nconv": nc, "diff": diff}
+    f = P.synth_gaussian(V, spec["seed"] + 3)
+    R.clover_full(u, MASS, 1.0, 0, f)
+    t = time.perf_counter()
+    R.clover_full(u, MASS, 1.0, 0, f)
+    out["clover_full_mult"] = {"ms": (time.perf_counter() - t) * 1e3}
+    with open(path, "w") as fh:
+        json.dump(out, fh)
+
+
+def reference_solvers_beside(torch, device):
+    """Each item: the reference (host cores, one thread: its Dslash has no
+    threading) and ours (GPU, through the host-array API, copies included)."""
+    import tempfile
+    import oracle
+    import iroiro_b200 as ib
+    if not oracle.ref_available():
+        return None
+    res = {}
+    for name, spec in REF_SOLVER_SPECS.items():
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "ref.json")
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-solver-child", name, path],
+                               stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, timeout=600)
+            if r.returncode != 0 or not os.path.exists(path):
+                res[name] = {"error": r.stderr.decode(errors="replace")[-300:]}
+                continue
+            with open(path) as fh:
+                ref = json.load(fh)
+        Lr = spec["L"]
+        V = int(np.prod(Lr))
+        ctx = ib.Context(Lr, device)
+        u = ib.synth_gauge(Lr, EPS, spec["seed"], gauge_transform=True)
+        ctx.upload_gauge(u, force=True)
+
+        def timed(fn):
+            fn()
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            return (time.perf_counter() - t) * 1e3, r
+
+        D = ib.Dirac_Wilson(MASS, u, ctx=ctx)
+        b = ib.synth_gaussian(V, spec["seed"] + 1)
+        x = np.empty_like(b)
+        ms, o = timed(lambda: ib.Solver_CG(1e-20, 5000, ib.Fopr_DdagD(D)).solve(x, b))
+        rc = ref["cg_wilson_full"]
+        res["cg_wilson_full_" + name] = {
+            "reference_ms": round(rc["ms"], 2), "reference_iterations": rc["iterations"],
+            "ours_ms": round(ms, 2), "ours_iterations": o.Iterations, "speedup": round(rc["ms"] / ms, 1)}
+        De = ib.Dirac_Wilson_EvenOdd(MASS, u, ctx=ctx)
+        bh = ib.synth_gaussian(V // 2, spec["seed"] + 2)
+        xs = []
+        ms, o = timed(lambda: ib.MultiShiftSolver_CG(ib.Fopr_DdagD(De), 1e-20, 5000).solve(xs, bh, SHIFTS12))
+        rm = ref["multishift12_wilson_eo"]
+        res["multishift12_wilson_eo_" + name] = {
+            "reference_ms": round(rm["ms"], 2), "reference_nconv": rm["nconv"],
+            "ours_ms": round(ms, 2), "ours_nconv": o.Nconv, "speedup": round(rm["ms"] / ms, 1)}
+        f = ib.synth_gaussian(V, spec["seed"] + 3)
+        ms, _ = timed(lambda: ctx.apply(ib.OP_CLOVER_FULL, MASS, 1.0, 0, f))
+        rk = ref["clover_full_mult"]
+        res["clover_full_mult_" + name] = {
+            "reference_ms": round(rk["ms"], 2), "ours_ms": round(ms, 3), "speedup": round(rk["ms"] / ms, 1)}
+        ctx.close()
+    res["note"] = ("reference: oracle/_ref on one host core in a child process; ours: the host-array "
+                   "API on the GPU, copies included; same seeded inputs")
+    return res
+
+
 # ---- our arm --------------------------------------------------------------------------------
 
 def run_ours(args, world, rank, local):
@@ -795,6 +898,7 @@ def run_ours(args, world, rank, local):
     if rank != 0:
         return 0
     cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline_leg()
+    beside = None if args.no_cpu_baseline or world > 1 else reference_solvers_beside(torch, local)
     traffic, traffic_src = traffic_per_step(Vh)
     t_step = (t_ms / args.steps) * 1e-3
     line = {
@@ -821,6 +925,7 @@ def run_ours(args, world, rank, local):
         "gpu_launches": 2 * args.steps,
         "clocks": ck,
         "cpu_baseline": cpu,
+        "reference_beside": beside,
         "variants": variants,
         "solve": solve,
         "learned": learned_res,
@@ -872,6 +977,10 @@ def summarise(line, peak):
         out["mixed48_clover_12rhs"] = {"fp64_ms": g(m, "double", "ms"), "fp16_ms": g(m, "half", "ms"),
                                        "speedup": g(m, "half", "speedup_vs_fp64_block_cg"),
                                        "max_error_vs_fp64": g(m, "half", "error_vs_fp64_max")}
+    rb = line.get("reference_beside")
+    if rb:
+        out["reference_beside_8x8x8x16_speedup"] = {k.replace("_8x8x8x16", ""): g(rb, k, "speedup")
+                                                     for k in rb if k != "note"}
     c = line["callers"]
     if c:
         out["qprop_block12_half_speedup"] = g(c, "qprop_evenodd_32x32x32x64",
@@ -1030,7 +1139,11 @@ def main():
                     help="skip the 48^3x96 mixed-precision 12-RHS configuration (~1 min)")
     ap.add_argument("--kernel", default=None, help="profiling driver: OP,PREC,NRHS")
     ap.add_argument("--lattice", default="24,24,24,48")
+    ap.add_argument("--ref-solver-child", nargs=2, default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.ref_solver_child:
+        ref_solver_child(*args.ref_solver_child)
+        return 0
     if args.kernel:
         return kernel_only(args)
     world, rank, local = (1, 0, 0) if args.impl == "reference" and _env_int("WORLD_SIZE", 1) == 1 \
