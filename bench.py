@@ -661,7 +661,7 @@ def cpu_baseline_leg():
 # The reference's solvers and clover operator on the host cores, beside ours on the GPU, at a
 # size where the reference finishes in seconds (8^3x16): full-lattice Wilson CG (D^dag D to
 # |r|^2/|b|^2 < 1e-20), e/o multishift CG (12 shifts 1e-4..10) and the full-lattice clover mult
-# (the reference's takes ~24 s per call at 24^3x48 on one core).  The reference keeps one
+# (the reference's took ~24 s per call at 24^3x48 on one core of the build machine).  The reference keeps one
 # lattice per process, so it runs in a child process that loads only oracle/ libraries; its
 # results go to a file (the reference's clover prints on every call).
 REF_SOLVER_SPECS = {
