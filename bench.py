@@ -415,7 +415,8 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
     GCR at 32^3x64 and 48^3x96 (unseen fields, one Gaussian source each)
     against GCR without it and against CG on the same full-lattice D^dag D:
     FP64 and mixed precision.  Every solve stops on the FP64 true residual
-    1e-10."""
+    1e-10; each is timed after an untimed call, as the median of 3 runs at
+    32^3x64 and one run at 48^3x96."""
     import iroiro_b200 as ib
     from iroiro_b200 import learned
     t0 = time.perf_counter()
@@ -432,15 +433,25 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
                        "epochs": epochs, "train_s": round(train_s, 1),
                        "loss_first": round(hist[0], 4), "loss_last": round(hist[-1], 4)}}
 
-    def timed(fn):
+    samples = {}
+
+    def timed(fn, reps=1):
+        # one untimed call (tuning, workspaces), then the median of `reps`
+        # timed calls: the solves sync with the host every iteration, and a
+        # single run of GCR here has varied by up to 3x from box-side jitter
         fn()
         torch.cuda.synchronize()
-        t = time.perf_counter()
-        r = fn()
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t) * 1e3, r
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t) * 1e3)
+        samples["last"] = [round(v, 1) for v in ts]
+        return statistics.median(ts), r
 
-    for Lb, tag, seed in (([32, 32, 32, 64], "", SEED + 301), ([48, 48, 48, 96], "_48x48x48x96", SEED + 311)):
+    for Lb, tag, seed, reps in (([32, 32, 32, 64], "", SEED + 301, 3),
+                                ([48, 48, 48, 96], "_48x48x48x96", SEED + 311, 1)):
         Vb = int(np.prod(Lb))
         ctx = ib.Context(Lb, device)
         ctx.set_stream(torch.cuda.current_stream().cuda_stream)
@@ -453,16 +464,17 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
         for name, n in (("gcr_network", net), ("gcr_plain", None)):
             x = ib.DeviceField(ctx, 2, "double")
             slv = learned.Solver_GCR(D, n, nkrylov=nkrylov)
-            ms, (o, rc) = timed(lambda: slv.solve_field(b, x))
-            res[name] = {"ms": round(ms, 1), "iterations": o.iterations, "true_residual": o.diff,
-                         "cg_fallback": bool(o.fallback), "converged": rc == ib.OK}
+            ms, (o, rc) = timed(lambda: slv.solve_field(b, x), reps)
+            res[name] = {"ms": round(ms, 1), "ms_samples": samples["last"], "iterations": o.iterations,
+                         "true_residual": o.diff, "cg_fallback": bool(o.fallback), "converged": rc == ib.OK}
             x.close()
         for inner in ("double", "single", "half"):
             x = ib.DeviceField(ctx, 2, "double")
             slv = ib.Solver_CG(1e-20, 20000, ib.Fopr_DdagD(D), inner=inner)
-            ms, (outs, rc) = timed(lambda: slv.solve_field(b, x))
-            res["cg_" + inner] = {"ms": round(ms, 1), "iterations": outs[0].Iterations,
-                                  "true_residual": outs[0].diff, "converged": rc == ib.OK}
+            ms, (outs, rc) = timed(lambda: slv.solve_field(b, x), reps)
+            res["cg_" + inner] = {"ms": round(ms, 1), "ms_samples": samples["last"],
+                                  "iterations": outs[0].Iterations, "true_residual": outs[0].diff,
+                                  "converged": rc == ib.OK}
             x.close()
         a = ib.DeviceField(ctx, 2, "single").upload(ib.synth_gaussian(Vb, seed + 2))
         c2 = ib.DeviceField(ctx, 2, "single")
