@@ -231,15 +231,20 @@ cudaError_t launch_force(const Geom& g, const GaugePtr& gauge, int recon, int p,
 // ---- learned preconditioner (learned.cu) -------------------------------------------
 struct PtcGeo;
 constexpr int kMaxVec = 16;
+constexpr int kMaxList = kMaxVec + 2;  // a cycle's directions and two more fields
 struct CFieldList {
-  SpinorPtr f[kMaxVec];
+  SpinorPtr f[kMaxList];
 };
 struct CCoef {
-  float re[kMaxVec], im[kMaxVec];
+  float re[kMaxList], im[kMaxList];
 };
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
                         cudaStream_t st);
 cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
                          cudaStream_t st);
+// one Gram-Schmidt step of GCR in one pass: wj += sum_{q<m} c_q w_q, then
+// r -= a wj with the updated wj
+cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const CCoef& c, SpinorPtr wj,
+                              float are, float aim, SpinorPtr r, cudaStream_t st);
 
 }  // namespace iro

@@ -925,16 +925,16 @@ int loss_blocks() { return kRedBlocks; }
 // ---- complex linear algebra for GCR on FP32 fields ---------------------------------------
 // <w_q, t> = sum conj(w_q) t for q < m, per-block partials [block][2m]
 __global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double* part) {
-  __shared__ double sm[2 * kMaxVec][64];
-  double acc[2 * kMaxVec];
+  __shared__ double sm[2 * kMaxList][64];
+  double acc[2 * kMaxList];
 #pragma unroll
-  for (int q = 0; q < 2 * kMaxVec; ++q) acc[q] = 0.0;
+  for (int q = 0; q < 2 * kMaxList; ++q) acc[q] = 0.0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     Cx<float> tv[12], wv[12];
     SpinorIO<PREC_SINGLE>::load(t, i, tv);
 #pragma unroll
-    for (int q = 0; q < kMaxVec; ++q) {
+    for (int q = 0; q < kMaxList; ++q) {
       if (q >= m) break;
       SpinorIO<PREC_SINGLE>::load(w.f[q], i, wv);
       double re = 0.0, im = 0.0;
@@ -975,6 +975,36 @@ __global__ void caxpy_kernel(int64_t n, int m, CFieldList x, CCoef c, SpinorPtr 
     }
     SpinorIO<PREC_SINGLE>::store(y, i, yv);
   }
+}
+
+// wj += sum_q c_q w_q; r -= a wj (the updated wj), one pass over the fields
+__global__ void gcr_update_kernel(int64_t n, int m, CFieldList w, CCoef c, SpinorPtr wj, float are,
+                                  float aim, SpinorPtr r) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    Cx<float> yv[12], xv[12];
+    SpinorIO<PREC_SINGLE>::load(wj, i, yv);
+    for (int q = 0; q < m; ++q) {
+      SpinorIO<PREC_SINGLE>::load(w.f[q], i, xv);
+      const Cx<float> cq = {c.re[q], c.im[q]};
+#pragma unroll
+      for (int k = 0; k < 12; ++k) yv[k] = yv[k] + cq * xv[k];
+    }
+    SpinorIO<PREC_SINGLE>::store(wj, i, yv);
+    SpinorIO<PREC_SINGLE>::load(r, i, xv);
+    const Cx<float> a = {are, aim};
+#pragma unroll
+    for (int k = 0; k < 12; ++k) xv[k] = xv[k] - a * yv[k];
+    SpinorIO<PREC_SINGLE>::store(r, i, xv);
+  }
+}
+
+cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const CCoef& c, SpinorPtr wj,
+                              float are, float aim, SpinorPtr r, cudaStream_t st) {
+  int grid = int((n + 255) / 256);
+  if (grid > 148 * 16) grid = 148 * 16;
+  gcr_update_kernel<<<grid, 256, 0, st>>>(n, m, w, c, wj, are, aim, r);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
@@ -1354,13 +1384,13 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   const int64_t nel = R->sites();
   const int blocks = 296;
   double* part = nullptr;
-  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * blocks * 2 * kMaxVec, st));
+  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * blocks * 2 * kMaxList, st));
   struct Free {
     double* p;
     cudaStream_t s;
     ~Free() { if (p) cudaFreeAsync(p, s); }
   } free_part{part, st};
-  std::vector<double> hp(size_t(blocks) * 2 * kMaxVec);
+  std::vector<double> hp(size_t(blocks) * 2 * kMaxList);
   // <w_q, t> for the listed fields, summed on the host in block order
   auto cdots = [&](const std::vector<const DevField*>& ws, const DevField& t,
                    std::vector<std::complex<double>>& res) -> int {
@@ -1435,28 +1465,57 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
       LRC(apply(c, op, mass, csw, true, *t32, *W[j], nullptr, 0, nullptr));
       for (int i = 0; i < m; ++i) T[i][j] = 0.0;
       T[j][j] = 1.0;
-      if (j > 0) {
-        std::vector<const DevField*> ws(W.begin(), W.begin() + j);
-        std::vector<std::complex<double>> cw;
-        LRC(cdots(ws, *W[j], cw));
-        std::vector<std::complex<double>> beta(j);
-        for (int q = 0; q < j; ++q) beta[q] = -cw[q] / nw[q];
-        LRC(caxpy(ws, beta, *W[j]));
-        // z'_j = z_j + sum_q beta_q z'_q
-        for (int q = 0; q < j; ++q)
-          for (int i = 0; i <= q; ++i) T[i][j] += beta[q] * T[i][q];
-      }
-      // |w_j|^2 and <w_j, r> in one pass: <w_j, w_j> and <r, w_j> = conj(<w_j, r>)
+      // One pass forms <w_q, w_j> (q < j), |w_j|^2 and <r, w_j>.  The w_q are
+      // orthogonal and r is orthogonal to every w_q (GCR keeps it so), hence
+      // for w'_j = w_j + sum_q beta_q w_q, beta_q = -<w_q, w_j>/|w_q|^2:
+      // |w'_j|^2 = |w_j|^2 - sum_q |<w_q, w_j>|^2/|w_q|^2 and <w'_j, r> =
+      // <w_j, r>.  A second pass then orthogonalises w_j and updates r.
+      std::vector<const DevField*> ws(W.begin(), W.begin() + j);
+      ws.push_back(W[j]);
+      ws.push_back(r32);
       std::vector<std::complex<double>> g;
-      LRC(cdots({W[j], r32}, *W[j], g));
-      nw[j] = g[0].real();
-      const std::complex<double> alpha = std::conj(g[1]) / nw[j];
+      LRC(cdots(ws, *W[j], g));
+      std::vector<std::complex<double>> beta(j);
+      double nwj = g[j].real();
+      for (int q = 0; q < j; ++q) {
+        beta[q] = -g[q] / nw[q];
+        nwj -= std::norm(g[q]) / nw[q];
+      }
+      std::complex<double> rw = g[j + 1];  // <r, w'_j>
+      ws.resize(j);
+      std::complex<double> alpha;
+      if (nwj > 1e-4 * g[j].real()) {
+        nw[j] = nwj;
+        alpha = std::conj(rw) / nw[j];
+        CFieldList L{};
+        CCoef C{};
+        for (int q = 0; q < j; ++q) {
+          L.f[q] = ws[q]->all();
+          C.re[q] = float(beta[q].real());
+          C.im[q] = float(beta[q].imag());
+        }
+        LCK(launch_gcr_update(nel, j, L, C, W[j]->all(), float(alpha.real()), float(alpha.imag()),
+                              r32->all(), st));
+      } else {
+        // w_j nearly in the span of the w_q: orthogonalise first, then form
+        // |w'_j|^2 and <r, w'_j> from the vectors themselves
+        if (j > 0) LRC(caxpy(ws, beta, *W[j]));
+        std::vector<std::complex<double>> g2;
+        LRC(cdots({W[j], r32}, *W[j], g2));
+        nw[j] = g2[0].real();
+        rw = g2[1];
+        alpha = std::conj(rw) / nw[j];
+        LRC(caxpy({W[j]}, {-alpha}, *r32));
+      }
+      // z'_j = z_j + sum_q beta_q z'_q
+      for (int q = 0; q < j; ++q)
+        for (int i = 0; i <= q; ++i) T[i][j] += beta[q] * T[i][q];
       alph[j] = alpha;
       jdone = j + 1;
-      LRC(caxpy({W[j]}, {-alpha}, *r32));
-      // the new |r|^2 = |r|^2 - |<w_j, r>|^2 / |w_j|^2 (r minus its projection
-      // on w_j); only the restart test reads it, the FP64 residual decides
-      rr_it = rr_it - std::norm(g[1]) / nw[j];
+      // the new |r|^2 = |r|^2 - |<w'_j, r>|^2 / |w'_j|^2 (r minus its
+      // projection on w'_j); only the restart test reads it, the FP64
+      // residual decides
+      rr_it = rr_it - std::norm(rw) / nw[j];
       ++iters;
       if (rr_it < target || rr_it < delta * delta * rr_start) break;
     }
