@@ -131,10 +131,11 @@ int iro_field_strength(iro_ctx* ctx, int mu, int nu, double* out);
    (dagger=1; Dirac_Wilson::mult_dag, dirac_wilson.cpp:34-36).  `in` and
    `out` hold nrhs consecutive fields of the op's size (24*V doubles for full
    lattice ops, 12*V for e/o ops).  Storage and arithmetic in `prec`.
-   The Schur operators on one field between page-locked, non-overlapping
-   `in` and `out` move the field in chunks of t-slices with both copy
-   directions overlapped with each other and with the stencils (once the
-   operator's stencils are tuned); the result is the same to the bit. */
+   The Schur and full-lattice operators on one field between page-locked,
+   non-overlapping `in` and `out` move the field in chunks of t-slices with
+   both copy directions overlapped with each other and with the stencils
+   (once the operator's stencils are tuned); the result is the same to the
+   bit. */
 int iro_dirac_apply(iro_ctx* ctx, int op, double mass, double csw, int dagger, int prec,
                     const double* in, double* out, int nrhs);
 

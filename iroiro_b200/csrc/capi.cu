@@ -476,6 +476,22 @@ void schur_launches(iro_ctx* c, bool cl, double k, const DevField& in, DevField&
   L2.scale = k;
 }
 
+// The full-lattice operator as one launch over both parities (L from
+// base_launch): out_p = [A_pp] in_p - kappa H_{p,1-p} in_{1-p}
+// (Dirac_Wilson::mult, lib/Dirac_ops/dirac_wilson.cpp:28-32)
+void full_launch(iro_ctx* c, bool cl, double k, const DevField& in, DevField& out, HopLaunch& L) {
+  L.p0 = 0;
+  L.nparity = 2;
+  for (int y = 0; y < 2; ++y) {
+    L.in[y] = in.half(1 - y);
+    L.out[y] = out.half(y);
+    L.xin[y] = in.half(y);
+    if (cl) L.clov[y] = clover_ptr(c, L.prec, y, false);
+  }
+  L.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
+  L.scale = -k;
+}
+
 // out = op(in) on device fields.  `red`/`red_mask`, when given, attach a
 // reduction to the last kernel of the operator (|out|^2, |xin|^2, (xin,out)),
 // and `skip` lets converged right-hand sides be left untouched.
@@ -546,17 +562,7 @@ int apply_dev(iro_ctx* c, int op, double mass, double csw, bool dag, const DevFi
     } break;
     case IRO_OP_WILSON_FULL:
     case IRO_OP_CLOVER_FULL: {
-      const bool cl = op == IRO_OP_CLOVER_FULL;
-      L.p0 = 0;
-      L.nparity = 2;
-      for (int y = 0; y < 2; ++y) {
-        L.in[y] = in.half(1 - y);
-        L.out[y] = out.half(y);
-        L.xin[y] = in.half(y);
-        if (cl) L.clov[y] = clover_ptr(c, prec, y, false);
-      }
-      L.epi = cl ? EPI_XPAY_CLOV : EPI_XPAY;
-      L.scale = -k;
+      full_launch(c, op == IRO_OP_CLOVER_FULL, k, in, out, L);
       if (red) { L.red = *red; L.red_mask = red_mask; }
       if (fuse) {
         L.cg = 1;
@@ -960,20 +966,115 @@ int schur_host_pipelined(iro_ctx* c, int op, double mass, double csw, bool dag, 
   return IRO_OK;
 }
 
+// The full-lattice operators between pinned host arrays, overlapped like the
+// Schur operator above (same chunks of t-slices, streams and events): the
+// host array is lexicographic, so a chunk of t-slices is one contiguous host
+// range and one half-site range in each parity.  Output chunk j reads input
+// chunks j-1..j+1, so it is computed and sent back as soon as input chunk j+1
+// has arrived.  The same single launch over both parities as apply_dev, on
+// the chunk's half-sites: the result is the same to the bit.
+int full_host_pipelined(iro_ctx* c, int op, double mass, double csw, bool dag, int prec,
+                        const double* in, double* out, bool* handled) {
+  *handled = false;
+  int b[kPipeMaxChunks + 1];
+  const int n = pipe_plan(c, b);
+  const bool cl = op == IRO_OP_CLOVER_FULL;
+  if (cl) RCK(ensure_clover(c, mass, csw));
+  int rc = IRO_OK;
+  DevField* fi = ws(c, 2, prec, 1, 10, &rc);
+  if (!fi) return rc;
+  DevField* fo = ws(c, 2, prec, 1, 11, &rc);
+  if (!fo) return rc;
+  HopLaunch L = base_launch(c, prec, dag, 1);
+  full_launch(c, cl, kappa_of(mass), *fi, *fo, L);
+  if (!c->tuned.count(tune_key(L))) return IRO_OK;
+  RCK(ensure_stage(c, size_t(c->V) * 24 * sizeof(double)));
+  for (int i = 0; i < 2; ++i)
+    if (!c->xs[i]) CK(cudaStreamCreateWithFlags(&c->xs[i], cudaStreamNonBlocking));
+  while (c->xev.size() < size_t(2 * kPipeMaxChunks + 1)) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->xev.push_back(e);
+  }
+  *handled = true;
+  cudaStream_t cs = c->stream, h2d = c->xs[0], d2h = c->xs[1];
+  cudaEvent_t* arrived = c->xev.data();
+  cudaEvent_t* exported = arrived + kPipeMaxChunks;
+  cudaEvent_t start = arrived[2 * kPipeMaxChunks];
+  // chunk j: half-sites [lo(j), lo(j + 1)) of each parity; host sites
+  // [2 lo(j), 2 lo(j + 1)) (a t-slice holds 2 st lexicographic sites)
+  auto lo = [&](int j) { return int64_t(b[j]) * c->g.st; };
+  auto bytes = [&](int j) { return size_t(lo(j + 1) - lo(j)) * 2 * 24 * sizeof(double); };
+  auto run = [&]() -> int {
+    CK(cudaEventRecord(start, cs));
+    CK(cudaStreamWaitEvent(h2d, start, 0));
+    for (int q = 0; q < n; ++q) {
+      const int j = (q + n - 1) % n;
+      CK(cudaMemcpyAsync(c->stage + 2 * lo(j) * 24, in + 2 * lo(j) * 24, bytes(j),
+                         cudaMemcpyHostToDevice, h2d));
+      CK(cudaEventRecord(arrived[j], h2d));
+    }
+    auto import = [&](int j) -> int {
+      CK(cudaStreamWaitEvent(cs, arrived[j], 0));
+      for (int p = 0; p < 2; ++p)
+        CK(launch_import_spinor(c->g, c->stage, 0, p, c->V, 1, prec, fi->half(p), cs, lo(j),
+                                lo(j + 1) - lo(j)));
+      return IRO_OK;
+    };
+    auto apply_chunk = [&](int j) -> int {
+      L.hs0 = int(lo(j));
+      L.nhs = int(lo(j + 1) - lo(j));
+      RCK(launch_tuned(c, L));
+      for (int p = 0; p < 2; ++p)
+        CK(launch_export_spinor(c->g, c->stage, 0, p, c->V, 1, prec, fo->half(p), cs, lo(j),
+                                lo(j + 1) - lo(j)));
+      CK(cudaEventRecord(exported[j], cs));
+      CK(cudaStreamWaitEvent(d2h, exported[j], 0));
+      CK(cudaMemcpyAsync(out + 2 * lo(j) * 24, c->stage + 2 * lo(j) * 24, bytes(j),
+                         cudaMemcpyDeviceToHost, d2h));
+      return IRO_OK;
+    };
+    RCK(import(n - 1));
+    RCK(import(0));
+    RCK(import(1));
+    RCK(apply_chunk(0));
+    for (int k = 2; k <= n - 2; ++k) {
+      RCK(import(k));
+      RCK(apply_chunk(k - 1));
+    }
+    RCK(apply_chunk(n - 2));
+    RCK(apply_chunk(n - 1));
+    return IRO_OK;
+  };
+  rc = run();
+  const cudaError_t e1 = cudaStreamSynchronize(h2d);
+  const cudaError_t e2 = cudaStreamSynchronize(d2h);
+  const cudaError_t e3 = cudaStreamSynchronize(cs);
+  if (rc) return rc;
+  CK(e1);
+  CK(e2);
+  CK(e3);
+  return IRO_OK;
+}
+
 int iro_dirac_apply(iro_ctx* c, int op, double mass, double csw, int dagger, int prec,
                     const double* in, double* out, int nrhs) {
   if (!c || !in || !out || nrhs < 1 || nrhs > kMaxRhs || prec < 0 || prec > 2 || !op_valid(op))
     return fail(c, IRO_BAD_ARG, "bad operator arguments");
   CK(cudaSetDevice(c->device));
   int rc = IRO_OK;
-  if (nrhs == 1 && (op == IRO_OP_WILSON_SCHUR_EE || op == IRO_OP_CLOVER_SCHUR_EE) && c->has_gauge &&
-      (prec == PREC_DOUBLE || c->recon == 12) && pipe_chunks(c) >= 6 &&
-      (out + c->Vh * 24 <= in || in + c->Vh * 24 <= out) && host_pinned(in) && host_pinned(out)) {
+  const bool schur = op == IRO_OP_WILSON_SCHUR_EE || op == IRO_OP_CLOVER_SCHUR_EE;
+  const bool full = op == IRO_OP_WILSON_FULL || op == IRO_OP_CLOVER_FULL;
+  const int64_t len = (full ? c->V : c->Vh) * 24;
+  if (nrhs == 1 && (schur || full) && c->has_gauge && (prec == PREC_DOUBLE || c->recon == 12) &&
+      pipe_chunks(c) >= 6 && (out + len <= in || in + len <= out) && host_pinned(in) &&
+      host_pinned(out)) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(c->stream, &cs));
     if (cs == cudaStreamCaptureStatusNone) {
       bool handled = false;
-      rc = schur_host_pipelined(c, op, mass, csw, dagger != 0, prec, in, out, &handled);
+      rc = schur ? schur_host_pipelined(c, op, mass, csw, dagger != 0, prec, in, out, &handled)
+                 : full_host_pipelined(c, op, mass, csw, dagger != 0, prec, in, out, &handled);
       if (rc || handled) return rc;
     }
   }
