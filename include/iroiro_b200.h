@@ -104,8 +104,9 @@ void* iro_ctx_get_stream(const iro_ctx* ctx);
 int iro_ctx_set_stream(iro_ctx* ctx, void* stream);
 /* The stencil autotuner's choices so far, as a JSON array (one object per
    tuned launch shape: precision, reconstruction, dagger, epilogue, nrhs,
-   parities -> kernel variant, block size, time per launch in ms).  The
-   reference has no autotuner. */
+   parities -> kernel variant, block size, free_grid (1: the grid covers every
+   site in one pass; 0: at most 8 blocks per SM loop over the sites), time per
+   launch in ms).  The reference has no autotuner. */
 int iro_autotune_report(const iro_ctx* ctx, char* buf, int len);
 
 /* ---- gauge and clover ---------------------------------------------------- */
