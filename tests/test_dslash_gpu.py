@@ -246,3 +246,22 @@ def test_full_pinned_overlapped_equals_plain(big, prec, op, csw):
             pin_out[:] = np.nan
             c.apply(op, m, csw, dag, pin_in, prec, out=pin_out)
             assert np.array_equal(pin_out, ref)
+
+
+@pytest.mark.parametrize("slices", ["1", "5"])
+def test_overlapped_chunk_plans_equal_plain(big, slices, monkeypatch):
+    """Other chunk plans (IRO_PIPE_SLICES: 48 single-slice chunks; 5-slice
+    middle chunks between single-slice ends) give the plain path's result to
+    the bit for the Schur and the full-lattice operator."""
+    import torch
+    monkeypatch.setenv("IRO_PIPE_SLICES", slices)
+    c, m = big["c"], big["m"]
+    for op, f in ((ib.OP_WILSON_SCHUR_EE, big["h"]), (ib.OP_WILSON_FULL, big["f"])):
+        pin_in = torch.empty(f.size, dtype=torch.float64, pin_memory=True).numpy()
+        pin_out = torch.empty(f.size, dtype=torch.float64, pin_memory=True).numpy()
+        pin_in[:] = f
+        ref = c.apply(op, m, 0.0, 0, f)
+        for _ in range(2):
+            pin_out[:] = np.nan
+            c.apply(op, m, 0.0, 0, pin_in, out=pin_out)
+            assert np.array_equal(pin_out, ref)
