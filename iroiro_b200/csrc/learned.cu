@@ -372,6 +372,18 @@ __device__ __forceinline__ void a_tile_job(const PtcGeo& G, const float2* __rest
 // accumulator back.  The mbarrier phase alternates per tile; every wait is
 // bounded and a time-out stops the CTA with the error flag set.
 constexpr int kFwdSites = 32;
+
+// First site of forward tile `tile`: even and odd tiles alternate (tile 2k is
+// even-parity half-sites [32k, 32k + 32), tile 2k + 1 the same odd ones), so
+// that a feature or link read as a neighbour by one parity's tiles is read
+// again as the centre of the other parity's tiles shortly after, from L2.
+// Tiling the even sites before the odd ones read each of them from DRAM twice
+// (8->8 layer at 24^3x48: 512 MB of DRAM reads per launch, 261 MB now, the
+// input features and links once).
+// (The volume is a multiple of 64, so each parity is a whole number of tiles.)
+__device__ __forceinline__ int fwd_tile_site0(const PtcGeo& G, int tile) {
+  return (tile & 1) * G.g.Vh + (tile >> 1) * kFwdSites;
+}
 constexpr int kFwdThreads = 288;
 
 template <int CIN, int COUT>
@@ -406,7 +418,7 @@ __global__ void __launch_bounds__(kFwdThreads) ptc_fwd_kernel(PtcGeo G, const fl
   const uint32_t tmem = tslot;
   uint32_t phase = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int site0 = tile * kFwdSites;
+    const int site0 = fwd_tile_site0(G, tile);
     a_tile_job<CIN, S::KP>(G, in, site0 + lane, lane, warp, A);
     const bool ok = mma_and_wait<S::KP>(A, B, tmem, idesc_bf16(S::NP), &bar, phase, G.err);
     phase ^= 1u;
@@ -486,7 +498,7 @@ __global__ void __launch_bounds__(kFwdThreads, (CIN <= 4 ? 4 : (CIN <= 8 ? 3 : 1
   for (int tile = blockIdx.x, it = 0;; tile += gridDim.x, ++it) {
     const bool have = tile < ntiles;
     const int sb = it & 1;
-    if (have) a_tile_job<CIN, S::KP>(G, in, tile * kFwdSites + lane, lane, warp, abuf(sb));
+    if (have) a_tile_job<CIN, S::KP>(G, in, fwd_tile_site0(G, tile) + lane, lane, warp, abuf(sb));
     fence_async_smem();
     __syncthreads();
     tc_fence_after();
@@ -517,7 +529,7 @@ __global__ void __launch_bounds__(kFwdThreads, (CIN <= 4 ? 4 : (CIN <= 8 ? 3 : 1
         for (int c = 0; c < S::NP; c += 16)
           tmem_ld16(tmem0 + uint32_t(pb * S::TCOLS) + (uint32_t(warp * 32) << 16) + c, v + c);
         const int sl = r / 3, a = r - sl * 3;
-        const int s = prev * kFwdSites + sl;
+        const int s = fwd_tile_site0(G, prev) + sl;
         if (s < G.V) {
           float4* o4 = reinterpret_cast<float4*>(out) + size_t(a) * G.V + s;
 #pragma unroll
