@@ -299,22 +299,30 @@ __device__ __forceinline__ void a_tile_job(const PtcGeo& G, const float2* __rest
     int src = s;
     Su3<float> U;
     bool fwd = true;
+    int mu = 0, n = hs;
     if (d > 0) {
       const Coord c = coord_of(G.g, hs, p);
       int nb[8];
       neighbours(G.g, c, hs, nb);
-      const int mu = (d - 1) >> 1;
+      mu = (d - 1) >> 1;
       fwd = ((d - 1) & 1) == 0;
-      const int n = nb[d - 1];
+      n = nb[d - 1];
       src = (1 - p) * Vh + n;
+    }
+    // channels 2q, 2q+1 of the source site, one float4 row per colour (see fidx)
+    const float4* f4 = reinterpret_cast<const float4*>(in) + src;
+    const size_t V = size_t(G.V);
+    // all of the job's feature rows requested at once (into L1), so that the
+    // loads below, which the register budget spreads over the channel
+    // pairs, find them there instead of each pair waiting on memory
+#pragma unroll
+    for (int q = 0; q < 3 * NW; ++q) asm volatile("prefetch.global.L1 [%0];" ::"l"(f4 + q * V));
+    if (d > 0) {
       if (fwd)
         GaugeIO<PREC_SINGLE, 12>::load(G.gauge, p, mu, hs, U);
       else
         GaugeIO<PREC_SINGLE, 12>::load(G.gauge, 1 - p, mu, n, U);
     }
-    // channels 2q, 2q+1 of the source site, one float4 row per colour (see fidx)
-    const float4* f4 = reinterpret_cast<const float4*>(in) + src;
-    const size_t V = size_t(G.V);
 #pragma unroll
     for (int q = 0; q < NW; ++q) {
       const float4 a = __ldg(f4 + (3 * q) * V), b = __ldg(f4 + (3 * q + 1) * V),
