@@ -530,28 +530,12 @@ __global__ void __launch_bounds__(kFwdThreads, (CIN <= 4 ? 4 : (CIN <= 8 ? 3 : 1
       tc_fence_after();
       ph ^= 1u << pb;
       if (!mma_ok) break;  // the same flag in every thread: the CTA leaves together
-      if (warp < 3) {
-        const int r = warp * 32 + lane;
-        float v[S::NP];
-#pragma unroll
-        for (int c = 0; c < S::NP; c += 16)
-          tmem_ld16(tmem0 + uint32_t(pb * S::TCOLS) + (uint32_t(warp * 32) << 16) + c, v + c);
-        const int sl = r / 3, a = r - sl * 3;
-        const int s = fwd_tile_site0(G, prev) + sl;
-        if (s < G.V) {
-          float4* o4 = reinterpret_cast<float4*>(out) + size_t(a) * G.V + s;
-#pragma unroll
-          for (int q = 0; q < COUT / 2; ++q)
-            o4[size_t(3 * q) * G.V] = make_float4(v[4 * q], v[4 * q + 2], v[4 * q + 1], v[4 * q + 3]);
-        }
-      }
-      // the accumulator of the previous tile is read before it is reused
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
     }
-    if (!have) break;
-    if (threadIdx.x == 0) {
+    // This tile's MMAs go out before the previous tile is read back, so that
+    // the read-back overlaps them (the two use different accumulators; A of
+    // this tile and its accumulator were last used two tiles ago, which the
+    // barriers above have ordered).
+    if (have && threadIdx.x == 0) {
       const uint32_t a0 = smem_u32(abuf(sb)), b0 = smem_u32(B);
       constexpr uint32_t sbo = (S::KP / 8) * 128;
 #pragma unroll 1
@@ -560,6 +544,26 @@ __global__ void __launch_bounds__(kFwdThreads, (CIN <= 4 ? 4 : (CIN <= 8 ? 3 : 1
                   smem_desc(b0 + kb * 256, 128, sbo), idesc, kb > 0 ? 1u : 0u);
       umma_commit(&bar[sb]);
     }
+    if (prev >= 0 && warp < 3) {
+      const int pb = sb ^ 1;
+      const int r = warp * 32 + lane;
+      float v[S::NP];
+#pragma unroll
+      for (int c = 0; c < S::NP; c += 16)
+        tmem_ld16(tmem0 + uint32_t(pb * S::TCOLS) + (uint32_t(warp * 32) << 16) + c, v + c);
+      const int sl = r / 3, a = r - sl * 3;
+      const int s = fwd_tile_site0(G, prev) + sl;
+      if (s < G.V) {
+        float4* o4 = reinterpret_cast<float4*>(out) + size_t(a) * G.V + s;
+#pragma unroll
+        for (int q = 0; q < COUT / 2; ++q)
+          o4[size_t(3 * q) * G.V] = make_float4(v[4 * q], v[4 * q + 2], v[4 * q + 1], v[4 * q + 3]);
+      }
+    }
+    // the read-back's tensor-memory loads are ordered before the next
+    // iteration's barrier, after which that accumulator is written again
+    tc_fence_before();
+    if (!have) break;
     prev = tile;
   }
   tc_fence_before();
