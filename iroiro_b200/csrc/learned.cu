@@ -457,8 +457,8 @@ __global__ void __launch_bounds__(kFwdThreads) ptc_fwd_kernel(PtcGeo G, const fl
 }
 
 // Double-buffered forward kernel (two A tiles, two accumulators): the A tile
-// of tile t+1 is built while the MMAs of tile t run, and tile t is read back
-// after that build, before the MMAs of tile t+1 are issued.  A CTA's tile
+// of tile t+1 is built while the MMAs of tile t run; then the MMAs of tile t+1
+// are issued and tile t is read back while they run.  A CTA's tile
 // otherwise spends about a third of its time waiting for its MMAs (measured
 // with clock64 at 32^3x64: 3.5k of 9.5k cycles for an 8->8 layer).  The
 // shared memory holds [A1 | A0 | weights]: the MMA's rows 96..127 of A1 read
