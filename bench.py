@@ -415,7 +415,7 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
     GCR at 32^3x64 and 48^3x96 (unseen fields, one Gaussian source each)
     against GCR without it and against CG on the same full-lattice D^dag D:
     FP64 and mixed precision.  Every solve stops on the FP64 true residual
-    1e-10; each is timed after an untimed call, as the median of 3 runs at
+    1e-10; each is timed after an untimed call, as the median of 5 runs at
     32^3x64 and one run at 48^3x96."""
     import iroiro_b200 as ib
     from iroiro_b200 import learned
@@ -437,8 +437,8 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
 
     def timed(fn, reps=1):
         # one untimed call (tuning, workspaces), then the median of `reps`
-        # timed calls: the solves sync with the host every iteration, and a
-        # single run of GCR here has varied by up to 3x from box-side jitter
+        # timed calls: the solves sync with the host every iteration, and
+        # single runs of GCR here have varied by up to 3.7x (box-side jitter)
         fn()
         torch.cuda.synchronize()
         ts = []
@@ -450,7 +450,7 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
         samples["last"] = [round(v, 1) for v in ts]
         return statistics.median(ts), r
 
-    for Lb, tag, seed, reps in (([32, 32, 32, 64], "", SEED + 301, 3),
+    for Lb, tag, seed, reps in (([32, 32, 32, 64], "", SEED + 301, 5),
                                 ([48, 48, 48, 96], "_48x48x48x96", SEED + 311, 1)):
         Vb = int(np.prod(Lb))
         ctx = ib.Context(Lb, device)
