@@ -39,7 +39,7 @@ enum {
   IRO_BAD_ARG = 2,       /* the reference asserts on size mismatches
                             (include/common_fields.hpp:48) */
   IRO_CUDA_ERROR = 3,
-  IRO_TIMEOUT = 4,       /* a device-side wait hit its iteration limit */
+  IRO_TIMEOUT = 4,       /* a device-side wait hit its time or iteration limit */
   IRO_NO_GAUGE = 5,      /* operator applied before iro_gauge_upload */
   IRO_NO_CLOVER = 6,     /* clover operator applied before iro_clover_setup */
   IRO_OUT_OF_MEMORY = 7,
@@ -363,6 +363,14 @@ typedef struct {
 int iro_gcr_solve_field(iro_ctx* ctx, int op, double mass, double csw, const iro_ptc* net,
                         const iro_gcr_params* prm, const iro_field* b, iro_field* x,
                         iro_gcr_out* out);
+
+/* Self-test of the device-side bounded waits (no counterpart in the
+   reference): the tensor-core kernels wait on mbarriers for at most 1 s and
+   then set an error flag that the host turns into IRO_TIMEOUT, leaving the
+   context usable.  This runs the same wait on an mbarrier that nothing
+   arrives at, for limit_ms (0 < limit_ms <= 1000), and returns IRO_TIMEOUT
+   with the time it waited in *waited_ms. */
+int iro_selftest_bounded_wait(iro_ctx* ctx, double limit_ms, double* waited_ms);
 
 /* ---- synthetic inputs (host) ---------------------------------------------- */
 /* Seeded SU(3) field U = exp(i eps H), H = sum theta_a lambda_a / 2,

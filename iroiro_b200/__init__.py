@@ -113,6 +113,7 @@ def _declare(L):
         "iro_field_norm": (I, [_VP, _VP, _D]),
         "iro_field_dot": (I, [_VP, _VP, _VP, _D]),
         "iro_norm_noalloc": (I, [_VP, ctypes.c_int64, _VP, _VP]),
+        "iro_selftest_bounded_wait": (I, [_VP, D, _D]),
         "iro_cg_solve": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _D, _D, I,
                              ctypes.POINTER(SolverOut)]),
         "iro_cg_solve_field": (I, [_VP, I, D, D, ctypes.POINTER(CGParams), _VP, _VP,

@@ -77,6 +77,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
       : "memory");
   return ok != 0;
 }
+
+// A wait on an mbarrier gives up after kWaitNs nanoseconds of global time
+// (or kWaitLimit polls, whichever comes first): the kernel then sets its
+// error flag and leaves, and the host reports IRO_TIMEOUT.
+constexpr int kWaitLimit = 1 << 24;
+constexpr uint64_t kWaitNs = 1000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Polls the barrier until `phase` completes; false after limit_ns of global
+// time or kWaitLimit polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase,
+                                                  uint64_t limit_ns = kWaitNs) {
+  const uint64_t t0 = global_ns();
+  for (int it = 0; it < kWaitLimit; ++it) {
+    if (mbar_try_wait(bar, phase)) return true;
+    if ((it & 63) == 63 && global_ns() - t0 > limit_ns) return false;
+  }
+  return false;
+}
 // D(tmem) (+)= A(smem) * B(smem)^T, BF16 inputs, FP32 accumulation
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                           uint32_t idesc, uint32_t accumulate) {
@@ -126,7 +150,6 @@ __host__ __device__ __forceinline__ uint32_t canon(int r, int k, int K) {
 
 constexpr int kTileSites = 42;  // 126 of the 128 MMA rows
 constexpr int kThreads = 128;
-constexpr int kWaitLimit = 1 << 24;
 
 template <int CIN, int COUT>
 struct Ptc {
@@ -264,12 +287,7 @@ __device__ bool mma_and_wait(const unsigned char* A, const unsigned char* B, uin
       umma_commit(bar);
     }
     __syncwarp();
-    bool ok = false;
-    for (int it = 0; it < kWaitLimit; ++it)
-      if (mbar_try_wait(bar, phase)) {
-        ok = true;
-        break;
-      }
+    const bool ok = mbar_wait_bounded(bar, phase);
     if (threadIdx.x == 0) {
       mma_ok = ok ? 1 : 0;
       if (!ok && err) atomicExch(err, 1);
@@ -514,12 +532,7 @@ __global__ void __launch_bounds__(kFwdThreads, (CIN <= 4 ? 4 : (CIN <= 8 ? 3 : 1
       // the previous tile: wait for its MMAs (bounded), read its accumulator back
       const int pb = sb ^ 1;
       if (warp == 0) {
-        bool ok = false;
-        for (int i = 0; i < kWaitLimit; ++i)
-          if (mbar_try_wait(&bar[pb], (ph >> pb) & 1u)) {
-            ok = true;
-            break;
-          }
+        const bool ok = mbar_wait_bounded(&bar[pb], (ph >> pb) & 1u);
         if (lane == 0) {
           mma_ok = ok ? 1 : 0;
           if (!ok) atomicExch(G.err, 1);
@@ -1031,6 +1044,28 @@ cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const CCoef
   int grid = int((n + 255) / 256);
   if (grid > 148 * 16) grid = 148 * 16;
   gcr_update_kernel<<<grid, 256, 0, st>>>(n, m, w, c, wj, are, aim, r);
+  return cudaGetLastError();
+}
+
+// Self-test of the bounded wait (iro_selftest_bounded_wait): one thread waits
+// on an mbarrier that nothing arrives at, gives up after limit_ns, and
+// records the time it waited and the error flag, as the tensor-core kernels
+// do on a wait that runs out.
+__global__ void bounded_wait_probe_kernel(uint64_t limit_ns, int* err, unsigned long long* waited_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint64_t t0 = global_ns();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
+    *waited_ns = global_ns() - t0;
+    if (!ok) atomicExch(err, 1);
+  }
+}
+
+cudaError_t launch_bounded_wait_probe(uint64_t limit_ns, int* err, unsigned long long* waited_ns,
+                                      cudaStream_t st) {
+  bounded_wait_probe_kernel<<<1, 32, 0, st>>>(limit_ns, err, waited_ns);
   return cudaGetLastError();
 }
 
@@ -1598,6 +1633,33 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
     if (e) return e;
   }
   if (!converged) return set_error(c, IRO_NOT_CONVERGED, "GCR not converged");
+  return IRO_OK;
+}
+
+int iro_selftest_bounded_wait(iro_ctx* c, double limit_ms, double* waited_ms) {
+  if (!c || !waited_ms || !(limit_ms > 0.0) || limit_ms > 1000.0) return IRO_BAD_ARG;
+  LCK(cudaSetDevice(device(c)));
+  cudaStream_t st = stream(c);
+  int* err = nullptr;
+  unsigned long long* ns = nullptr;
+  LCK(cudaMalloc(reinterpret_cast<void**>(&err), sizeof(int)));
+  const cudaError_t e0 = cudaMalloc(reinterpret_cast<void**>(&ns), sizeof(unsigned long long));
+  if (e0 != cudaSuccess) {
+    cudaFree(err);
+    return cuda_error(c, e0, "cudaMalloc");
+  }
+  int herr = 0;
+  unsigned long long hns = 0;
+  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = launch_bounded_wait_probe(uint64_t(limit_ms * 1e6), err, ns, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hns, ns, sizeof(hns), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(err);
+  cudaFree(ns);
+  if (e != cudaSuccess) return cuda_error(c, e, "bounded-wait self-test");
+  *waited_ms = double(hns) * 1e-6;
+  if (herr) return set_error(c, IRO_TIMEOUT, "bounded wait ran out (self-test)");
   return IRO_OK;
 }
 
