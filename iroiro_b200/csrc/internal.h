@@ -238,8 +238,9 @@ struct CFieldList {
 struct CCoef {
   float re[kMaxList], im[kMaxList];
 };
+// <w_q, t> (q < m): block partials into part, their block-order sums into out[2m]
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
-                        cudaStream_t st);
+                        double* out, cudaStream_t st);
 cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
                          cudaStream_t st);
 // one Gram-Schmidt step of GCR in one pass: wj += sum_{q<m} c_q w_q, then

@@ -1001,6 +1001,16 @@ __global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double*
   }
 }
 
+// the block partials of cdot_kernel summed in block order, one thread per
+// real component (the same order and rounding as a sequential host sum)
+__global__ void cdot_finish_kernel(int blocks, int m2, const double* part, double* out) {
+  const int q = threadIdx.x;
+  if (q >= m2) return;
+  double v = 0.0;
+  for (int b = 0; b < blocks; ++b) v += part[size_t(b) * m2 + q];
+  out[q] = v;
+}
+
 // y += sum_q c_q x_q  (complex coefficients)
 __global__ void caxpy_kernel(int64_t n, int m, CFieldList x, CCoef c, SpinorPtr y) {
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
@@ -1070,8 +1080,9 @@ cudaError_t launch_bounded_wait_probe(uint64_t limit_ns, int* err, unsigned long
 }
 
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
-                        cudaStream_t st) {
+                        double* out, cudaStream_t st) {
   cdot_kernel<<<blocks, 256, 0, st>>>(n, m, w, t, part);
+  cdot_finish_kernel<<<1, 64, 0, st>>>(blocks, 2 * m, part, out);
   return cudaGetLastError();
 }
 cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
@@ -1099,6 +1110,7 @@ namespace host {
 int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField& in, DevField& out,
           const Reduce* red, int red_mask, const int* skip);
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
+void* pinned(iro_ctx* c);
 int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
 int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
 int norms(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
@@ -1445,27 +1457,28 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   }
   const int64_t nel = R->sites();
   const int blocks = 296;
-  double* part = nullptr;
-  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * blocks * 2 * kMaxList, st));
+  double* part = nullptr;  // block partials, then the 2 kMaxList sums
+  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * (blocks + 1) * 2 * kMaxList, st));
+  double* dsum = part + size_t(blocks) * 2 * kMaxList;
+  // the sums come back through the context's pinned host buffer (the solvers
+  // use its first bytes for their flags; GCR does not run beside them)
+  double* hsum = reinterpret_cast<double*>(static_cast<char*>(pinned(c)) + 2048);
   struct Free {
     double* p;
     cudaStream_t s;
     ~Free() { if (p) cudaFreeAsync(p, s); }
   } free_part{part, st};
-  std::vector<double> hp(size_t(blocks) * 2 * kMaxList);
-  // <w_q, t> for the listed fields, summed on the host in block order
+  // <w_q, t> for the listed fields, summed on the device in block order
   auto cdots = [&](const std::vector<const DevField*>& ws, const DevField& t,
                    std::vector<std::complex<double>>& res) -> int {
     CFieldList L{};
     const int k = int(ws.size());
     for (int q = 0; q < k; ++q) L.f[q] = ws[q]->all();
-    LCK(launch_cdot(nel, k, L, t.all(), part, blocks, st));
-    LCK(cudaMemcpyAsync(hp.data(), part, sizeof(double) * blocks * 2 * k, cudaMemcpyDeviceToHost, st));
+    LCK(launch_cdot(nel, k, L, t.all(), part, blocks, dsum, st));
+    LCK(cudaMemcpyAsync(hsum, dsum, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, st));
     LCK(cudaStreamSynchronize(st));
     res.assign(k, {0.0, 0.0});
-    for (int bb = 0; bb < blocks; ++bb)
-      for (int q = 0; q < k; ++q)
-        res[q] += std::complex<double>(hp[size_t(bb) * 2 * k + 2 * q], hp[size_t(bb) * 2 * k + 2 * q + 1]);
+    for (int q = 0; q < k; ++q) res[q] = std::complex<double>(hsum[2 * q], hsum[2 * q + 1]);
     return IRO_OK;
   };
   auto caxpy = [&](const std::vector<const DevField*>& xs, const std::vector<std::complex<double>>& cs,
