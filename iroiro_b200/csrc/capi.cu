@@ -359,8 +359,9 @@ HopLaunch base_launch(iro_ctx* c, int prec, bool dag, int nrhs) {
 // reconstruction: fewer FP64 operations, more link bytes); FP32/FP16 with an
 // even nrhs 4..9 (two right-hand sides per thread); FP16 10..12 (the
 // mixed-precision kernel on the FP16 links with three stored rows at 3, 4 or
-// 2 blocks per SM, any nrhs).
-constexpr int kHopVariants = 13;
+// 2 blocks per SM, any nrhs) and 13..14 (the same kernel on the 12-real FP16
+// links, row 2 rebuilt per link, at 3 or 4 blocks per SM).
+constexpr int kHopVariants = 15;
 
 static bool variant_ok(const HopLaunch& L, int v) {
   if (v < 0 || v >= kHopVariants) return false;
@@ -375,7 +376,7 @@ static cudaError_t launch_variant(iro_ctx* c, HopLaunch L, cudaStream_t st) {
     L.variant -= 6;
     L.recon = 18;
     L.gauge.a = c->ga.d18;
-  } else if (L.prec == PREC_HALF && L.variant >= 10) {
+  } else if (L.prec == PREC_HALF && L.variant >= 10 && L.variant <= 12) {
     L.recon = 18;
     L.gauge.a = c->ga.h18a;
     L.gauge.b = c->ga.h18b;

@@ -170,9 +170,10 @@ struct HopParams {
 // direction's loads over another's, fewer live registers);
 // VAR bit 2 (FP64 only): 128-thread blocks, at least three per SM (register
 // cap 168: between the uncapped 254 and the spilling 128);
-// VAR bit 3 (FP16 on links with three stored rows only): the mixed-precision
-// direction code of dslash_mix.cuh, at least three 256-thread blocks per SM
-// (four with bit 0, two with bit 1).
+// VAR bit 3 (FP16 only): the mixed-precision direction code of
+// dslash_mix.cuh on the links with three stored rows (RECON 18) or two
+// (RECON 12, row 2 rebuilt), at least three 256-thread blocks per SM (four
+// with bit 0, two with bit 1).
 template <int VAR>
 struct HopBounds {
   static constexpr int threads = (VAR & 4) ? 128 : 256;
@@ -211,13 +212,13 @@ __global__ void __launch_bounds__(HopBounds<VAR>::threads, HopBounds<VAR>::block
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = {R(0), R(0)};
     if constexpr ((VAR & 8) != 0) {
-      static_assert(SP == PREC_HALF && RECON == 18, "mixed path: FP16 with three-row links");
+      static_assert(SP == PREC_HALF && (RECON == 18 || RECON == 12), "mixed path: FP16 links");
       const uint32_t vh = uint32_t(P.g.Vh);
       const uint32_t lown = uint32_t(p * 4) * vh, lnb = uint32_t((1 - p) * 4) * vh;
-      hop_dir_mix<0, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
-      hop_dir_mix<1, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
-      hop_dir_mix<2, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
-      hop_dir_mix<3, DAG>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<0, DAG, RECON>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<1, DAG, RECON>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<2, DAG, RECON>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
+      hop_dir_mix<3, DAG, RECON>(P.gauge, P.in[yi], lown, lnb, vh, hs, nb, nrhs, r, acc);
     } else if (VAR & 2) {
 #pragma unroll 1
       for (int mu = 0; mu < 4; ++mu) {

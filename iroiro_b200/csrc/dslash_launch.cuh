@@ -140,6 +140,8 @@ static cudaError_t hop_go_stage(const HopLaunch& L, cudaStream_t st) {
 // FP64: 4/5 the 168-register 128-thread hop_kernel (5 with the rolled loop).
 // FP16 on links with three stored rows (RECON 18): only 10/11/12, the
 // mixed-precision hop_kernel (VAR 8 / 9 / 10: 3 / 4 / 2 blocks per SM).
+// FP16 on the 12-real links: also 13/14, the mixed-precision hop_kernel with
+// row 2 rebuilt (VAR 8 / 9).
 template <int SP, int GP, int RECON, bool DAG, int EPI>
 static cudaError_t hop_var_more(const HopLaunch& L, cudaStream_t st);
 
@@ -180,8 +182,16 @@ static cudaError_t hop_var_more(const HopLaunch& L, cudaStream_t st) {
       case 7: return hop_go_pair<SP, RECON, DAG, EPI, 3>(L, st);
       case 8: return hop_go_stage<SP, RECON, DAG, EPI, 0>(L, st);
       case 9: return hop_go_stage<SP, RECON, DAG, EPI, 1>(L, st);
-      default: return cudaErrorInvalidValue;
+      default: break;
     }
+    if constexpr (SP == PREC_HALF && RECON == 12) {
+      switch (L.variant) {
+        case 13: return hop_go<SP, GP, RECON, DAG, EPI, 8>(L, st);
+        case 14: return hop_go<SP, GP, RECON, DAG, EPI, 9>(L, st);
+        default: break;
+      }
+    }
+    return cudaErrorInvalidValue;
   }
 }
 

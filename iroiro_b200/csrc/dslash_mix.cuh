@@ -7,8 +7,9 @@
 // can accumulate in FP32 straight from the stored halves.  The neighbour is
 // projected in packed FP16 (one HADD2/HFMA2 per complex; the only rounding
 // this path adds to the FP16 storage's), the links are the FP16 copies with
-// all three rows stored (GaugeIO<PREC_HALF, 18> layout: no reconstruction),
-// and the element norm joins the reconstruction's FP32 FMAs as a weight.
+// all three rows stored (GaugeIO<PREC_HALF, 18> layout: no reconstruction)
+// or with two (row 2 rebuilt per link, 12 bytes fewer per link), and the
+// element norm joins the reconstruction's FP32 FMAs as a weight.
 // The spin algebra is hop_kernel's (project / reconstruct above; Dirac_Wilson
 // mult_offdiag, lib/Dirac_ops/dirac_wilson.cpp:107-113).
 #pragma once
@@ -173,6 +174,36 @@ __device__ __forceinline__ void load_link_w(const GaugePtr& g, uint32_t j, uint3
   u[8] = __ldg(static_cast<const uint32_t*>(g.b) + j);
 }
 
+// FP16 links with two stored rows (GaugeIO<PREC_HALF, 12>: 24 bytes instead
+// of 36), as words: row 2 = conj(row 0 x row 1) is formed in FP32 from the
+// stored rows and rounded to FP16 words, so the product below runs as on the
+// three-row links (whose row 2 is the FP64 row rounded to FP16)
+__device__ __forceinline__ void load_link_w12(const GaugePtr& g, uint32_t j, uint32_t u[9]) {
+  const uint4 a = __ldg(static_cast<const uint4*>(g.a) + j);
+  const uint2 b = __ldg(static_cast<const uint2*>(g.b) + j);
+  u[0] = a.x; u[1] = a.y; u[2] = a.z; u[3] = a.w; u[4] = b.x; u[5] = b.y;
+  float2 x[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) x[k] = __half22float2(as_h2(u[k]));
+  // (p q - r s)^* of complex p, q, r, s
+  auto cross = [](float2 p, float2 q, float2 r, float2 s) {
+    const float re = fmaf(p.x, q.x, fmaf(-p.y, q.y, fmaf(-r.x, s.x, r.y * s.y)));
+    const float im = fmaf(p.x, q.y, fmaf(p.y, q.x, fmaf(-r.x, s.y, -r.y * s.x)));
+    return as_w(__floats2half2_rn(re, -im));
+  };
+  u[6] = cross(x[1], x[5], x[2], x[4]);  // (u01 u12 - u02 u11)^*
+  u[7] = cross(x[2], x[3], x[0], x[5]);  // (u02 u10 - u00 u12)^*
+  u[8] = cross(x[0], x[4], x[1], x[3]);  // (u00 u11 - u01 u10)^*
+}
+
+template <int RECON>
+__device__ __forceinline__ void load_link_mix(const GaugePtr& g, uint32_t j, uint32_t u[9]) {
+  if constexpr (RECON == 12)
+    load_link_w12(g, j, u);
+  else
+    load_link_w(g, j, u);
+}
+
 // the stored words and norm of FP16 element i: chunk 0 of a warp block of 32
 // elements sits at 16-byte unit (i / 32) * 96 + i % 32, i.e. at byte
 // 32 * (i & ~31) + 16 * i
@@ -193,7 +224,7 @@ __device__ __forceinline__ float load_raw_w(const SpinorPtr& s, uint32_t i, uint
 // forward and backward contributions of direction MU (as hop_dir); lown and
 // lnb are the link indices of direction 0 at parity p and 1 - p
 // ((p * 4) * Vh and ((1 - p) * 4) * Vh)
-template <int MU, bool DAG>
+template <int MU, bool DAG, int RECON>
 __device__ __forceinline__ void hop_dir_mix(const GaugePtr& gauge, const SpinorPtr& in, uint32_t lown,
                                             uint32_t lnb, uint32_t vh, int hs, const int nb[8],
                                             int nrhs, int r, Cx<float> acc[12]) {
@@ -201,7 +232,7 @@ __device__ __forceinline__ void hop_dir_mix(const GaugePtr& gauge, const SpinorP
   Cx<float> g[6];
   {
     constexpr int S = DAG ? -1 : 1;
-    load_link_w(gauge, lown + MU * vh + uint32_t(hs), u);
+    load_link_mix<RECON>(gauge, lown + MU * vh + uint32_t(hs), u);
     const float n = load_raw_w(in, uint32_t(nb[2 * MU]) * uint32_t(nrhs) + uint32_t(r), f);
     project_w<MU, S>(f, h);
     su3_w<false>(u, h, g);
@@ -209,7 +240,7 @@ __device__ __forceinline__ void hop_dir_mix(const GaugePtr& gauge, const SpinorP
   }
   {
     constexpr int S = DAG ? 1 : -1;
-    load_link_w(gauge, lnb + MU * vh + uint32_t(nb[2 * MU + 1]), u);
+    load_link_mix<RECON>(gauge, lnb + MU * vh + uint32_t(nb[2 * MU + 1]), u);
     const float n = load_raw_w(in, uint32_t(nb[2 * MU + 1]) * uint32_t(nrhs) + uint32_t(r), f);
     project_w<MU, S>(f, h);
     su3_w<true>(u, h, g);

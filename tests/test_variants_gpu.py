@@ -5,7 +5,8 @@ and a 12-RHS mixed-precision CG whose fused reductions drive the solve.
 Variants 4-7 are the two-right-hand-sides-per-thread kernel with four
 register caps, 8-9 the same with its neighbours staged through shared memory;
 FP64 variants 6-11 are 0-5 on the 18-real links; FP16 10-12 the
-mixed-precision kernel (FP16 x FP16 -> FP32 FMAs) on three-row FP16 links."""
+mixed-precision kernel (FP16 x FP16 -> FP32 FMAs) on three-row FP16 links,
+13-14 the same kernel on the 12-real FP16 links with row 2 rebuilt."""
 import json
 import os
 import subprocess
@@ -62,7 +63,8 @@ print("RESULT " + json.dumps(out))
 """
 
 
-@pytest.mark.parametrize("variant", ["0,256", "4,256", "5,128", "6,128", "7,256", "8,128", "9,256", "10,128", "11,256", "12,256"])
+@pytest.mark.parametrize("variant", ["0,256", "4,256", "5,128", "6,128", "7,256", "8,128", "9,256", "10,128", "11,256", "12,256",
+                                     "13,256", "14,128"])
 def test_forced_variant(variant):
     env = dict(os.environ, IRO_HOP_VARIANT=variant)
     r = subprocess.run([sys.executable, "-c", SCRIPT, str(ROOT)], env=env, capture_output=True,
@@ -72,13 +74,13 @@ def test_forced_variant(variant):
     res = json.loads(line[len("RESULT "):])
     v = int(variant.split(",")[0])
     # the forced variant ran: FP64 modulo 6 (12 on an SU(3) field, whose
-    # 18-real links are variants 6-11); otherwise modulo 13, a variant the
-    # shape lacks (4-9 need an even nrhs, 10-12 FP16) falling back modulo 4
+    # 18-real links are variants 6-11); otherwise modulo 15, a variant the
+    # shape lacks (4-9 need an even nrhs, 10-14 FP16) falling back modulo 4
     for t in res["autotune"]:
         if t["prec"] == 0:
             exp = v % (12 if t["recon"] == 12 else 6)
         else:
-            w = v % 13
+            w = v % 15
             ok = w < 4 or (w < 10 and t["nrhs"] % 2 == 0) or (w >= 10 and t["prec"] == 2)
             exp = w if ok else w % 4
         assert t["variant"] == exp, t
