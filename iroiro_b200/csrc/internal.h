@@ -235,17 +235,49 @@ constexpr int kMaxList = kMaxVec + 2;  // a cycle's directions and two more fiel
 struct CFieldList {
   SpinorPtr f[kMaxList];
 };
-struct CCoef {
-  float re[kMaxList], im[kMaxList];
+// The state of one GCR restart cycle on the device: its coefficients are
+// formed there (gcr_coef_kernel), so that the host enqueues a whole cycle and
+// reads back once.  Iteration k of the cycle is skipped (every kernel of it
+// returns at once) when skip[k] is set, which the coefficient kernel does for
+// the iterations after the one that met the restart test.
+struct GcrState {
+  double nw[kMaxVec];                   // |w'_q|^2
+  double tre[kMaxVec * kMaxVec];        // T[i][j] at i * kMaxVec + j: z'_j = sum_i T[i][j] z_i
+  double tim[kMaxVec * kMaxVec];
+  double are[kMaxVec], aim[kMaxVec];    // alpha_j
+  double bre[kMaxVec], bim[kMaxVec];    // the current iteration's Gram-Schmidt coefficients
+  double rr_it, rr_start, target, d2;   // iterated |r|^2, its value at the cycle start, the
+                                        // solve's target and delta^2
+  int limit;                            // iterations the cycle may take
+  int jdone;                            // iterations done
+  int skip[kMaxVec];                    // iteration k is not needed
+  int plain[kMaxVec];                   // iteration k needs no second pass
+  float cre[kMaxList], cim[kMaxList];   // the current coefficients in FP32 (update / correction)
+  float ure, uim;                       // the current alpha in FP32
 };
-// <w_q, t> (q < m): block partials into part, their block-order sums into out[2m]
+// <w_q, t> (q < m): block partials into part, their block-order sums into
+// out[2m]; nothing when skip is set
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
-                        double* out, cudaStream_t st);
-cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
-                         cudaStream_t st);
-// one Gram-Schmidt step of GCR in one pass: wj += sum_{q<m} c_q w_q, then
-// r -= a wj with the updated wj
-cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const CCoef& c, SpinorPtr wj,
-                              float are, float aim, SpinorPtr r, cudaStream_t st);
+                        double* out, const int* skip, cudaStream_t st);
+// y += sum_{q < m} c_q x_q with the coefficients s->cre/cim (q < *count when
+// count is given; sign -1: y -= ...); nothing when skip is set
+cudaError_t launch_caxpy_dev(int64_t n, int m, const CFieldList& x, const GcrState* s,
+                             const int* count, float sign, SpinorPtr y, const int* skip,
+                             cudaStream_t st);
+// one Gram-Schmidt step of GCR in one pass: wj += sum_{q<m} c_q w_q, then, if
+// s->plain[j], r -= alpha wj with the updated wj (coefficients from s)
+cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const GcrState* s, int j,
+                              SpinorPtr wj, SpinorPtr r, cudaStream_t st);
+// the cycle's state at its start
+cudaError_t launch_gcr_init(GcrState* s, double rr, double target, double d2, int limit,
+                            cudaStream_t st);
+// iteration j's coefficients from g = (<w_q, w_j> (q < j), |w_j|^2, <r, w_j>)
+// (second = 0), or, when the first pass found w_j nearly in the span of the
+// w_q, from g = (|w'_j|^2, <r, w'_j>) of the orthogonalised w'_j (second = 1)
+cudaError_t launch_gcr_coef(GcrState* s, const double* g, int j, int m, int second,
+                            cudaStream_t st);
+// the correction coefficients gamma = T alpha of the finished cycle into
+// s->cre/cim
+cudaError_t launch_gcr_gamma(GcrState* s, cudaStream_t st);
 
 }  // namespace iro

@@ -191,6 +191,7 @@ struct PtcGeo {
   GaugePtr gauge;  // FP32 two-row links
   int V;
   int* err;
+  const int* skip;  // forward only: when set and nonzero the launch does nothing
 };
 
 // Builds the BF16 A tile: rows (site, colour) of the tile, columns
@@ -417,6 +418,7 @@ __global__ void __launch_bounds__(kFwdThreads) ptc_fwd_kernel(PtcGeo G, const fl
                                                               float2* __restrict__ out,
                                                               const __nv_bfloat16* __restrict__ bop,
                                                               int ntiles) {
+  if (G.skip && *G.skip) return;  // the same value in every thread, before any allocation
   using S = Ptc<CIN, COUT>;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* A = smem;
@@ -490,6 +492,7 @@ __global__ void __launch_bounds__(kFwdThreads, (CIN <= 4 ? 4 : (CIN <= 8 ? 3 : 1
                                                                float2* __restrict__ out,
                                                                const __nv_bfloat16* __restrict__ bop,
                                                                int ntiles) {
+  if (G.skip && *G.skip) return;  // the same value in every thread, before any allocation
   using S = Ptc<CIN, COUT>;
   extern __shared__ __align__(1024) unsigned char smem[];
   // A tile of buffer b: A0 = smem + A96, A1 = smem
@@ -726,7 +729,8 @@ __global__ void sum_partials_kernel(const float* __restrict__ partial, int ntile
 }
 
 // spinor field (FP32, full lattice) <-> 4-channel features [site][spin][colour]
-__global__ void spinor_to_feat_kernel(int Vh, SpinorPtr e, SpinorPtr o, float2* feat) {
+__global__ void spinor_to_feat_kernel(int Vh, SpinorPtr e, SpinorPtr o, float2* feat, const int* skip) {
+  if (skip && *skip) return;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < 2 * Vh; s += gridDim.x * blockDim.x) {
     const int p = s >= Vh ? 1 : 0;
     Cx<float> v[12];
@@ -735,7 +739,8 @@ __global__ void spinor_to_feat_kernel(int Vh, SpinorPtr e, SpinorPtr o, float2* 
     for (int k = 0; k < 12; ++k) feat_set(feat, s, k / 3, k % 3, 2 * Vh, make_float2(v[k].re, v[k].im));
   }
 }
-__global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o) {
+__global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o, const int* skip) {
+  if (skip && *skip) return;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < 2 * Vh; s += gridDim.x * blockDim.x) {
     const int p = s >= Vh ? 1 : 0;
     Cx<float> v[12];
@@ -907,12 +912,14 @@ void ptc_dims(int cin, int cout, int* kf, int* kp, int* nf, int* np) {
   *np = *nf < 16 ? 16 : (*nf + 15) / 16 * 16;
 }
 
-cudaError_t launch_spinor_to_feat(int Vh, SpinorPtr e, SpinorPtr o, float2* feat, cudaStream_t st) {
-  spinor_to_feat_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, e, o, feat);
+cudaError_t launch_spinor_to_feat(int Vh, SpinorPtr e, SpinorPtr o, float2* feat, cudaStream_t st,
+                                  const int* skip = nullptr) {
+  spinor_to_feat_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, e, o, feat, skip);
   return cudaGetLastError();
 }
-cudaError_t launch_feat_to_spinor(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o, cudaStream_t st) {
-  feat_to_spinor_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, feat, e, o);
+cudaError_t launch_feat_to_spinor(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o, cudaStream_t st,
+                                  const int* skip = nullptr) {
+  feat_to_spinor_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, feat, e, o, skip);
   return cudaGetLastError();
 }
 
@@ -964,7 +971,8 @@ int loss_blocks() { return kRedBlocks; }
 
 // ---- complex linear algebra for GCR on FP32 fields ---------------------------------------
 // <w_q, t> = sum conj(w_q) t for q < m, per-block partials [block][2m]
-__global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double* part) {
+__global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double* part, const int* skip) {
+  if (skip && *skip) return;  // the same value in every thread
   __shared__ double sm[2 * kMaxList][64];
   double acc[2 * kMaxList];
 #pragma unroll
@@ -1003,7 +1011,8 @@ __global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double*
 
 // the block partials of cdot_kernel summed in block order, one thread per
 // real component (the same order and rounding as a sequential host sum)
-__global__ void cdot_finish_kernel(int blocks, int m2, const double* part, double* out) {
+__global__ void cdot_finish_kernel(int blocks, int m2, const double* part, double* out, const int* skip) {
+  if (skip && *skip) return;
   const int q = threadIdx.x;
   if (q >= m2) return;
   double v = 0.0;
@@ -1011,50 +1020,160 @@ __global__ void cdot_finish_kernel(int blocks, int m2, const double* part, doubl
   out[q] = v;
 }
 
-// y += sum_q c_q x_q  (complex coefficients)
-__global__ void caxpy_kernel(int64_t n, int m, CFieldList x, CCoef c, SpinorPtr y) {
+// y += sign sum_q c_q x_q  (complex coefficients from the cycle state; the
+// first *count of the m fields when count is given)
+__global__ void caxpy_dev_kernel(int64_t n, int m, CFieldList x, const GcrState* s, const int* count,
+                                 float sign, SpinorPtr y, const int* skip) {
+  if (skip && *skip) return;
+  __shared__ float cre[kMaxList], cim[kMaxList];
+  __shared__ int mm;
+  if (threadIdx.x < kMaxList) {
+    cre[threadIdx.x] = sign * s->cre[threadIdx.x];
+    cim[threadIdx.x] = sign * s->cim[threadIdx.x];
+  }
+  if (threadIdx.x == 0) mm = count ? min(*count, m) : m;
+  __syncthreads();
+  const int k = mm;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     Cx<float> yv[12], xv[12];
     SpinorIO<PREC_SINGLE>::load(y, i, yv);
-    for (int q = 0; q < m; ++q) {
+    for (int q = 0; q < k; ++q) {
       SpinorIO<PREC_SINGLE>::load(x.f[q], i, xv);
-      const Cx<float> cq = {c.re[q], c.im[q]};
+      const Cx<float> cq = {cre[q], cim[q]};
 #pragma unroll
-      for (int k = 0; k < 12; ++k) yv[k] = yv[k] + cq * xv[k];
+      for (int c = 0; c < 12; ++c) yv[c] = yv[c] + cq * xv[c];
     }
     SpinorIO<PREC_SINGLE>::store(y, i, yv);
   }
 }
 
-// wj += sum_q c_q w_q; r -= a wj (the updated wj), one pass over the fields
-__global__ void gcr_update_kernel(int64_t n, int m, CFieldList w, CCoef c, SpinorPtr wj, float are,
-                                  float aim, SpinorPtr r) {
+// iteration j: wj += sum_{q<m} c_q w_q; then, unless the coefficient kernel
+// found w_j nearly in the span of the w_q (s->plain[j] = 0: a second pass
+// forms |w'_j|^2 and <r, w'_j> first), r -= alpha wj with the updated wj
+__global__ void gcr_update_kernel(int64_t n, int m, CFieldList w, const GcrState* s, int j,
+                                  SpinorPtr wj, SpinorPtr r) {
+  if (s->skip[j]) return;
+  __shared__ float cre[kMaxList], cim[kMaxList];
+  if (threadIdx.x < kMaxList) {
+    cre[threadIdx.x] = s->cre[threadIdx.x];
+    cim[threadIdx.x] = s->cim[threadIdx.x];
+  }
+  __syncthreads();
+  const bool plain = s->plain[j] != 0;
+  const Cx<float> a = {s->ure, s->uim};
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     Cx<float> yv[12], xv[12];
     SpinorIO<PREC_SINGLE>::load(wj, i, yv);
     for (int q = 0; q < m; ++q) {
       SpinorIO<PREC_SINGLE>::load(w.f[q], i, xv);
-      const Cx<float> cq = {c.re[q], c.im[q]};
+      const Cx<float> cq = {cre[q], cim[q]};
 #pragma unroll
       for (int k = 0; k < 12; ++k) yv[k] = yv[k] + cq * xv[k];
     }
     SpinorIO<PREC_SINGLE>::store(wj, i, yv);
-    SpinorIO<PREC_SINGLE>::load(r, i, xv);
-    const Cx<float> a = {are, aim};
+    if (plain) {
+      SpinorIO<PREC_SINGLE>::load(r, i, xv);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) xv[k] = xv[k] - a * yv[k];
-    SpinorIO<PREC_SINGLE>::store(r, i, xv);
+      for (int k = 0; k < 12; ++k) xv[k] = xv[k] - a * yv[k];
+      SpinorIO<PREC_SINGLE>::store(r, i, xv);
+    }
   }
 }
 
-cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const CCoef& c, SpinorPtr wj,
-                              float are, float aim, SpinorPtr r, cudaStream_t st) {
-  int grid = int((n + 255) / 256);
-  if (grid > 148 * 16) grid = 148 * 16;
-  gcr_update_kernel<<<grid, 256, 0, st>>>(n, m, w, c, wj, are, aim, r);
-  return cudaGetLastError();
+__global__ void gcr_init_kernel(GcrState* s, double rr, double target, double d2, int limit) {
+  const int t = threadIdx.x;
+  if (t < kMaxVec) {
+    s->skip[t] = 0;
+    s->plain[t] = 1;
+  }
+  for (int i = t; i < kMaxVec * kMaxVec; i += blockDim.x) s->tre[i] = s->tim[i] = 0.0;
+  if (t == 0) {
+    s->rr_it = s->rr_start = rr;
+    s->target = target;
+    s->d2 = d2;
+    s->limit = limit;
+    s->jdone = 0;
+  }
+}
+
+// alpha_j, column j of T, the iterated |r|^2 and the restart test, from
+// |w'_j|^2 and <r, w'_j> (r is orthogonal to every earlier w'_q, so
+// <r, w'_j> = <r, w_j>); the beta_q of the iteration are in s->bre/bim
+__device__ void gcr_finish_iteration(GcrState* s, int j, int m, double nwj, double rre, double rim) {
+  constexpr int K = kMaxVec;
+  s->nw[j] = nwj;
+  const double ar = rre / nwj, ai = -rim / nwj;  // alpha = conj(<r, w'_j>) / |w'_j|^2
+  s->are[j] = ar;
+  s->aim[j] = ai;
+  s->ure = float(ar);
+  s->uim = float(ai);
+  // z'_j = z_j + sum_q beta_q z'_q
+  s->tre[j * K + j] = 1.0;
+  for (int q = 0; q < j; ++q) {
+    const double br = s->bre[q], bi = s->bim[q];
+    for (int i = 0; i <= q; ++i) {
+      const double tr = s->tre[i * K + q], ti = s->tim[i * K + q];
+      s->tre[i * K + j] += br * tr - bi * ti;
+      s->tim[i * K + j] += br * ti + bi * tr;
+    }
+  }
+  // r minus its projection on w'_j; only the restart test reads it, the FP64
+  // residual decides
+  s->rr_it = s->rr_it - (rre * rre + rim * rim) / nwj;
+  s->jdone = j + 1;
+  if (s->rr_it < s->target || s->rr_it < s->d2 * s->rr_start || s->jdone >= s->limit)
+    for (int k = j + 1; k < m; ++k) s->skip[k] = 1;
+}
+
+// One thread.  First pass (second = 0): g = <w_q, w_j> (q < j), |w_j|^2,
+// <r, w_j> as (re, im) pairs.  The w_q are orthogonal, hence for w'_j = w_j +
+// sum_q beta_q w_q with beta_q = -<w_q, w_j>/|w_q|^2, |w'_j|^2 = |w_j|^2 -
+// sum_q |<w_q, w_j>|^2/|w_q|^2; when that falls below 1e-4 |w_j|^2 the
+// orthogonalised vector is formed first and a second pass (second = 1, g =
+// |w'_j|^2, <r, w'_j>) finishes the iteration.
+__global__ void gcr_coef_kernel(GcrState* s, const double* g, int j, int m, int second) {
+  if (s->skip[j]) return;
+  if (!second) {
+    double nwj = g[2 * j];
+    for (int q = 0; q < j; ++q) {
+      const double gr = g[2 * q], gi = g[2 * q + 1], nq = s->nw[q];
+      const double br = -gr / nq, bi = -gi / nq;
+      s->bre[q] = br;
+      s->bim[q] = bi;
+      s->cre[q] = float(br);
+      s->cim[q] = float(bi);
+      nwj -= (gr * gr + gi * gi) / nq;
+    }
+    if (nwj > 1e-4 * g[2 * j]) {
+      gcr_finish_iteration(s, j, m, nwj, g[2 * j + 2], g[2 * j + 3]);
+    } else {
+      s->plain[j] = 0;
+      s->ure = s->uim = 0.f;
+    }
+  } else {
+    if (s->plain[j]) return;
+    gcr_finish_iteration(s, j, m, g[0], g[2], g[3]);
+    s->cre[0] = s->ure;  // r -= alpha w'_j (caxpy with sign -1)
+    s->cim[0] = s->uim;
+  }
+}
+
+// gamma_i = sum_{j >= i} T[i][j] alpha_j over the cycle's iterations, into
+// s->cre/cim (zero beyond them)
+__global__ void gcr_gamma_kernel(GcrState* s) {
+  const int jd = s->jdone;
+  for (int i = threadIdx.x; i < kMaxList; i += blockDim.x) {
+    double gr = 0.0, gi = 0.0;
+    for (int j = i; j < jd; ++j) {
+      const double tr = s->tre[i * kMaxVec + j], ti = s->tim[i * kMaxVec + j];
+      gr += tr * s->are[j] - ti * s->aim[j];
+      gi += tr * s->aim[j] + ti * s->are[j];
+    }
+    s->cre[i] = float(gr);
+    s->cim[i] = float(gi);
+  }
 }
 
 // Self-test of the bounded wait (iro_selftest_bounded_wait): one thread waits
@@ -1080,16 +1199,38 @@ cudaError_t launch_bounded_wait_probe(uint64_t limit_ns, int* err, unsigned long
 }
 
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
-                        double* out, cudaStream_t st) {
-  cdot_kernel<<<blocks, 256, 0, st>>>(n, m, w, t, part);
-  cdot_finish_kernel<<<1, 64, 0, st>>>(blocks, 2 * m, part, out);
+                        double* out, const int* skip, cudaStream_t st) {
+  cdot_kernel<<<blocks, 256, 0, st>>>(n, m, w, t, part, skip);
+  cdot_finish_kernel<<<1, 64, 0, st>>>(blocks, 2 * m, part, out, skip);
   return cudaGetLastError();
 }
-cudaError_t launch_caxpy(int64_t n, int m, const CFieldList& x, const CCoef& c, SpinorPtr y,
-                         cudaStream_t st) {
+static int blas_grid(int64_t n) {
   int grid = int((n + 255) / 256);
-  if (grid > 148 * 16) grid = 148 * 16;
-  caxpy_kernel<<<grid, 256, 0, st>>>(n, m, x, c, y);
+  return grid > 148 * 16 ? 148 * 16 : grid;
+}
+cudaError_t launch_caxpy_dev(int64_t n, int m, const CFieldList& x, const GcrState* s,
+                             const int* count, float sign, SpinorPtr y, const int* skip,
+                             cudaStream_t st) {
+  caxpy_dev_kernel<<<blas_grid(n), 256, 0, st>>>(n, m, x, s, count, sign, y, skip);
+  return cudaGetLastError();
+}
+cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const GcrState* s, int j,
+                              SpinorPtr wj, SpinorPtr r, cudaStream_t st) {
+  gcr_update_kernel<<<blas_grid(n), 256, 0, st>>>(n, m, w, s, j, wj, r);
+  return cudaGetLastError();
+}
+cudaError_t launch_gcr_init(GcrState* s, double rr, double target, double d2, int limit,
+                            cudaStream_t st) {
+  gcr_init_kernel<<<1, 64, 0, st>>>(s, rr, target, d2, limit);
+  return cudaGetLastError();
+}
+cudaError_t launch_gcr_coef(GcrState* s, const double* g, int j, int m, int second,
+                            cudaStream_t st) {
+  gcr_coef_kernel<<<1, 1, 0, st>>>(s, g, j, m, second);
+  return cudaGetLastError();
+}
+cudaError_t launch_gcr_gamma(GcrState* s, cudaStream_t st) {
+  gcr_gamma_kernel<<<1, 32, 0, st>>>(s);
   return cudaGetLastError();
 }
 
@@ -1214,11 +1355,13 @@ PtcGeo make_geo(iro_ctx* c, int* err) {
   G.gauge = gauge_single(c);
   G.V = int(volume(c));
   G.err = err;
+  G.skip = nullptr;
   return G;
 }
 
-// features of a full-lattice spinor field (FP32 or FP64; converted to FP32)
-int field_to_feat(iro_ctx* c, const DevField& f, float2* feat) {
+// features of a full-lattice spinor field (FP32 or FP64; converted to FP32);
+// `skip` (FP32 fields only) as the forward pass's
+int field_to_feat(iro_ctx* c, const DevField& f, float2* feat, const int* skip = nullptr) {
   const DevField* src = &f;
   int rc = IRO_OK;
   if (f.prec != PREC_SINGLE) {
@@ -1227,13 +1370,14 @@ int field_to_feat(iro_ctx* c, const DevField& f, float2* feat) {
     LRC(convert(c, f, *t));
     src = t;
   }
-  LCK(launch_spinor_to_feat(int(src->Vh), src->half(0), src->half(1), feat, stream(c)));
+  LCK(launch_spinor_to_feat(int(src->Vh), src->half(0), src->half(1), feat, stream(c),
+                            f.prec == PREC_SINGLE ? skip : nullptr));
   return IRO_OK;
 }
 
-int feat_to_field(iro_ctx* c, const float2* feat, DevField& f) {
+int feat_to_field(iro_ctx* c, const float2* feat, DevField& f, const int* skip = nullptr) {
   if (f.prec == PREC_SINGLE) {
-    LCK(launch_feat_to_spinor(int(f.Vh), feat, f.half(0), f.half(1), stream(c)));
+    LCK(launch_feat_to_spinor(int(f.Vh), feat, f.half(0), f.half(1), stream(c), skip));
     return IRO_OK;
   }
   int rc = IRO_OK;
@@ -1252,8 +1396,10 @@ int check_err(iro_ctx* c, iro_ptc* n) {
 }
 
 // act[0] must hold the input features; runs every layer
-int forward(iro_ctx* c, iro_ptc* n) {
+// the network's layers on n->act[0]; nothing when `skip` is set and nonzero
+int forward(iro_ctx* c, iro_ptc* n, const int* skip = nullptr) {
   PtcGeo G = make_geo(c, n->err);
+  G.skip = skip;
   for (int l = 0; l < n->nl; ++l)
     LCK(launch_ptc_fwd(n->w[l], n->w[l + 1], G, n->act[l], n->act[l + 1], n->bop[l], stream(c)));
   return IRO_OK;
@@ -1457,42 +1603,23 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   }
   const int64_t nel = R->sites();
   const int blocks = 296;
-  double* part = nullptr;  // block partials, then the 2 kMaxList sums
-  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * (blocks + 1) * 2 * kMaxList, st));
-  double* dsum = part + size_t(blocks) * 2 * kMaxList;
-  // the sums come back through the context's pinned host buffer (the solvers
-  // use its first bytes for their flags; GCR does not run beside them)
-  double* hsum = reinterpret_cast<double*>(static_cast<char*>(pinned(c)) + 2048);
+  // block partials, the first and second passes' sums, then the cycle state
+  const size_t sum_off = size_t(blocks) * 2 * kMaxList;
+  const size_t state_off = sum_off + 4 * kMaxList;
+  double* part = nullptr;
+  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * state_off + sizeof(GcrState), st));
+  double* dsum = part + sum_off;
+  double* dsum2 = dsum + 2 * kMaxList;
+  GcrState* gs = reinterpret_cast<GcrState*>(part + state_off);
+  // the cycle's iteration count comes back through the context's pinned host
+  // buffer (the solvers use its first bytes for their flags; GCR does not run
+  // beside them)
+  int* hjdone = reinterpret_cast<int*>(static_cast<char*>(pinned(c)) + 2048);
   struct Free {
     double* p;
     cudaStream_t s;
     ~Free() { if (p) cudaFreeAsync(p, s); }
   } free_part{part, st};
-  // <w_q, t> for the listed fields, summed on the device in block order
-  auto cdots = [&](const std::vector<const DevField*>& ws, const DevField& t,
-                   std::vector<std::complex<double>>& res) -> int {
-    CFieldList L{};
-    const int k = int(ws.size());
-    for (int q = 0; q < k; ++q) L.f[q] = ws[q]->all();
-    LCK(launch_cdot(nel, k, L, t.all(), part, blocks, dsum, st));
-    LCK(cudaMemcpyAsync(hsum, dsum, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, st));
-    LCK(cudaStreamSynchronize(st));
-    res.assign(k, {0.0, 0.0});
-    for (int q = 0; q < k; ++q) res[q] = std::complex<double>(hsum[2 * q], hsum[2 * q + 1]);
-    return IRO_OK;
-  };
-  auto caxpy = [&](const std::vector<const DevField*>& xs, const std::vector<std::complex<double>>& cs,
-                   DevField& y) -> int {
-    CFieldList L{};
-    CCoef C{};
-    for (size_t q = 0; q < xs.size(); ++q) {
-      L.f[q] = xs[q]->all();
-      C.re[q] = float(cs[q].real());
-      C.im[q] = float(cs[q].imag());
-    }
-    LCK(launch_caxpy(nel, int(xs.size()), L, C, y.all(), st));
-    return IRO_OK;
-  };
   // x = 0, r = b
   LRC(axpby(c, 0.0, *B, 0.0, *B, *X));
   LRC(axpby(c, 1.0, *B, 0.0, *B, *R));
@@ -1513,94 +1640,56 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   } free_mask{dmask, st};
   LCK(cudaMemcpyAsync(dmask, ones.data(), sizeof(int), cudaMemcpyHostToDevice, st));
   while (!converged && iters < prm->max_iter) {
+    // One restart cycle, enqueued whole: the coefficients of every iteration
+    // are formed on the device (gcr_coef_kernel), and the iterations after
+    // the one that meets the restart test (|r|^2 below delta^2 of its value
+    // at the cycle start, or the target) return at once.  The z_j are kept as
+    // the network produced them; the orthogonalised directions are z'_j =
+    // sum_i T[i][j] z_i (T unit upper triangular, from the Gram-Schmidt
+    // coefficients of the w_j), and the correction of the cycle e = sum_j
+    // alpha_j z'_j = sum_i gamma_i z_i is formed once at its end.
+    const int cyc = std::min(m, prm->max_iter - iters);
     LRC(convert(c, *R, *r32));
     LRC(axpby(c, 0.0, *r32, 0.0, *r32, *e32));
-    const double rr_start = rr;
-    double rr_it = rr;  // the iterated |r|^2
-    std::vector<double> nw(m, 0.0);
-    // The z_j are kept as the network produced them; the orthogonalised
-    // directions are z'_j = sum_i T[i][j] z_i (T unit upper triangular, from
-    // the Gram-Schmidt coefficients of the w_j), and the correction of the
-    // cycle e = sum_j alpha_j z'_j = sum_i gamma_i z_i is formed once at its
-    // end: one pass over the z_i instead of updating z_j and e every step.
-    std::vector<std::vector<std::complex<double>>> T(m, std::vector<std::complex<double>>(m));
-    std::vector<std::complex<double>> alph(m);
-    int jdone = 0;
-    for (int j = 0; j < m && iters < prm->max_iter; ++j) {
+    LCK(launch_gcr_init(gs, rr, target, delta * delta, cyc, st));
+    for (int j = 0; j < cyc; ++j) {
+      const int* skip = &gs->skip[j];
       // z_j = N(r) (or r without a network), w_j = A z_j
       if (net) {
-        LRC(field_to_feat(c, *r32, net->act[0]));
-        LRC(forward(c, const_cast<iro_ptc*>(net)));
-        LRC(feat_to_field(c, net->act[net->nl], *Z[j]));
-        ++pcapplies;
+        LRC(field_to_feat(c, *r32, net->act[0], skip));
+        LRC(forward(c, const_cast<iro_ptc*>(net), skip));
+        LRC(feat_to_field(c, net->act[net->nl], *Z[j], skip));
       } else {
         LRC(axpby(c, 1.0, *r32, 0.0, *r32, *Z[j]));
       }
-      LRC(apply(c, op, mass, csw, false, *Z[j], *t32, nullptr, 0, nullptr));
-      LRC(apply(c, op, mass, csw, true, *t32, *W[j], nullptr, 0, nullptr));
-      for (int i = 0; i < m; ++i) T[i][j] = 0.0;
-      T[j][j] = 1.0;
-      // One pass forms <w_q, w_j> (q < j), |w_j|^2 and <r, w_j>.  The w_q are
-      // orthogonal and r is orthogonal to every w_q (GCR keeps it so), hence
-      // for w'_j = w_j + sum_q beta_q w_q, beta_q = -<w_q, w_j>/|w_q|^2:
-      // |w'_j|^2 = |w_j|^2 - sum_q |<w_q, w_j>|^2/|w_q|^2 and <w'_j, r> =
-      // <w_j, r>.  A second pass then orthogonalises w_j and updates r.
-      std::vector<const DevField*> ws(W.begin(), W.begin() + j);
-      ws.push_back(W[j]);
-      ws.push_back(r32);
-      std::vector<std::complex<double>> g;
-      LRC(cdots(ws, *W[j], g));
-      std::vector<std::complex<double>> beta(j);
-      double nwj = g[j].real();
-      for (int q = 0; q < j; ++q) {
-        beta[q] = -g[q] / nw[q];
-        nwj -= std::norm(g[q]) / nw[q];
-      }
-      std::complex<double> rw = g[j + 1];  // <r, w'_j>
-      ws.resize(j);
-      std::complex<double> alpha;
-      if (nwj > 1e-4 * g[j].real()) {
-        nw[j] = nwj;
-        alpha = std::conj(rw) / nw[j];
-        CFieldList L{};
-        CCoef C{};
-        for (int q = 0; q < j; ++q) {
-          L.f[q] = ws[q]->all();
-          C.re[q] = float(beta[q].real());
-          C.im[q] = float(beta[q].imag());
-        }
-        LCK(launch_gcr_update(nel, j, L, C, W[j]->all(), float(alpha.real()), float(alpha.imag()),
-                              r32->all(), st));
-      } else {
-        // w_j nearly in the span of the w_q: orthogonalise first, then form
-        // |w'_j|^2 and <r, w'_j> from the vectors themselves
-        if (j > 0) LRC(caxpy(ws, beta, *W[j]));
-        std::vector<std::complex<double>> g2;
-        LRC(cdots({W[j], r32}, *W[j], g2));
-        nw[j] = g2[0].real();
-        rw = g2[1];
-        alpha = std::conj(rw) / nw[j];
-        LRC(caxpy({W[j]}, {-alpha}, *r32));
-      }
-      // z'_j = z_j + sum_q beta_q z'_q
-      for (int q = 0; q < j; ++q)
-        for (int i = 0; i <= q; ++i) T[i][j] += beta[q] * T[i][q];
-      alph[j] = alpha;
-      jdone = j + 1;
-      // the new |r|^2 = |r|^2 - |<w'_j, r>|^2 / |w'_j|^2 (r minus its
-      // projection on w'_j); only the restart test reads it, the FP64
-      // residual decides
-      rr_it = rr_it - std::norm(rw) / nw[j];
-      ++iters;
-      if (rr_it < target || rr_it < delta * delta * rr_start) break;
+      LRC(apply(c, op, mass, csw, false, *Z[j], *t32, nullptr, 0, skip));
+      LRC(apply(c, op, mass, csw, true, *t32, *W[j], nullptr, 0, skip));
+      // one pass forms <w_q, w_j> (q < j), |w_j|^2 and <r, w_j>; the
+      // coefficient kernel turns them into beta_q, |w'_j|^2 and alpha, and a
+      // second pass orthogonalises w_j and updates r -= alpha w'_j
+      CFieldList L{};
+      for (int q = 0; q <= j; ++q) L.f[q] = W[q]->all();
+      L.f[j + 1] = r32->all();
+      LCK(launch_cdot(nel, j + 2, L, W[j]->all(), part, blocks, dsum, skip, st));
+      LCK(launch_gcr_coef(gs, dsum, j, m, 0, st));
+      LCK(launch_gcr_update(nel, j, L, gs, j, W[j]->all(), r32->all(), st));
+      // w_j nearly in the span of the w_q (plain[j] = 0): |w'_j|^2 and
+      // <r, w'_j> from the orthogonalised vector, then r -= alpha w'_j
+      const int* single = &gs->plain[j];
+      CFieldList L2{};
+      L2.f[0] = W[j]->all();
+      L2.f[1] = r32->all();
+      LCK(launch_cdot(nel, 2, L2, W[j]->all(), part, blocks, dsum2, single, st));
+      LCK(launch_gcr_coef(gs, dsum2, j, m, 1, st));
+      LCK(launch_caxpy_dev(nel, 1, L2, gs, nullptr, -1.f, r32->all(), single, st));
     }
-    // e = sum_i gamma_i z_i, gamma = T alpha
-    if (jdone > 0) {
-      std::vector<const DevField*> zs(Z.begin(), Z.begin() + jdone);
-      std::vector<std::complex<double>> gam(jdone);
-      for (int i = 0; i < jdone; ++i)
-        for (int j = i; j < jdone; ++j) gam[i] += T[i][j] * alph[j];
-      LRC(caxpy(zs, gam, *e32));
+    // e = sum_i gamma_i z_i, gamma = T alpha over the iterations done
+    {
+      LCK(launch_gcr_gamma(gs, st));
+      CFieldList L{};
+      for (int i = 0; i < cyc; ++i) L.f[i] = Z[i]->all();
+      LCK(launch_caxpy_dev(nel, cyc, L, gs, &gs->jdone, 1.f, e32->all(), nullptr, st));
+      LCK(cudaMemcpyAsync(hjdone, &gs->jdone, sizeof(int), cudaMemcpyDeviceToHost, st));
     }
     // x += e, r = b - A x in FP64
     LCK(launch_mx_merge(PREC_SINGLE, X->sites(), 1, X->all(), e32->all(), dmask, st));
@@ -1609,6 +1698,9 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
     LRC(axpby(c, 1.0, *B, -1.0, *S, *R));
     std::vector<double> rnorm;
     LRC(norms(c, *R, nullptr, rnorm, nullptr));
+    const int jd = *hjdone;  // copied before the norms, which synchronise the stream
+    iters += jd;
+    if (net) pcapplies += jd;
     ++restarts;
     stalls = (rnorm[0] > 0.25 * rr) ? stalls + 1 : 0;
     rr = rnorm[0];
