@@ -77,6 +77,10 @@ struct iro_ctx {
   void* h_pinned = nullptr;  // host mirror of state + done
 
   std::map<std::tuple<int, int, int, int>, DevField> ws;
+  // small device scratch of the solvers that keep per-call state (GCR),
+  // allocated once and grown on demand: no allocation inside a solve
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
 
   // stencil autotuner: (prec, recon, dag, epilogue, nrhs, nparity) -> (variant, block cap)
   std::map<std::tuple<int, int, int, int, int, int>, Tune> tuned;
@@ -739,6 +743,7 @@ int iro_ctx_destroy(iro_ctx* c) {
       if (c->clAinv[pr][p]) cudaFree(c->clAinv[pr][p]);
     }
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->scratch) cudaFree(c->scratch);
   for (int i = 0; i < 2; ++i) {
     if (c->ring[i]) cudaFreeHost(c->ring[i]);
     if (c->ring_ev[i]) cudaEventDestroy(c->ring_ev[i]);
@@ -1219,6 +1224,26 @@ int64_t vh(iro_ctx* c) { return c->Vh; }
 void* state(iro_ctx* c) { return c->state; }
 int* done(iro_ctx* c) { return c->done; }
 void* pinned(iro_ctx* c) { return c->h_pinned; }
+void* scratch(iro_ctx* c, size_t bytes, int* rc) {
+  if (c->scratch_bytes < bytes) {
+    if (c->scratch) {
+      // the previous scratch may still be read by enqueued work
+      cudaError_t e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) { *rc = cuda_fail(c, e, "cudaStreamSynchronize"); return nullptr; }
+      cudaFree(c->scratch);
+      c->scratch = nullptr;
+      c->scratch_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&c->scratch, bytes);
+    if (e != cudaSuccess) {
+      c->scratch = nullptr;
+      *rc = cuda_fail(c, e, "cudaMalloc (solver scratch)");
+      return nullptr;
+    }
+    c->scratch_bytes = bytes;
+  }
+  return c->scratch;
+}
 int device(iro_ctx* c) { return c->device; }
 DevField* field_dev(iro_field* f) { return f ? &f->f : nullptr; }
 const Geom& geom(iro_ctx* c) { return c->g; }

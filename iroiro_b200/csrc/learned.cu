@@ -1229,6 +1229,11 @@ cudaError_t launch_gcr_coef(GcrState* s, const double* g, int j, int m, int seco
   gcr_coef_kernel<<<1, 1, 0, st>>>(s, g, j, m, second);
   return cudaGetLastError();
 }
+__global__ void fill_int_kernel(int* p, int v) { *p = v; }
+cudaError_t launch_fill_int(int* p, int v, cudaStream_t st) {
+  fill_int_kernel<<<1, 1, 0, st>>>(p, v);
+  return cudaGetLastError();
+}
 cudaError_t launch_gcr_gamma(GcrState* s, cudaStream_t st) {
   gcr_gamma_kernel<<<1, 32, 0, st>>>(s);
   return cudaGetLastError();
@@ -1252,6 +1257,7 @@ int apply(iro_ctx* c, int op, double mass, double csw, bool dag, const DevField&
           const Reduce* red, int red_mask, const int* skip);
 DevField* workspace(iro_ctx* c, int subset, int prec, int nrhs, int slot, int* rc);
 void* pinned(iro_ctx* c);
+void* scratch(iro_ctx* c, size_t bytes, int* rc);
 int import_field(iro_ctx* c, const double* host, bool full, DevField& f);
 int export_field(iro_ctx* c, const DevField& f, bool full, double* host);
 int norms(iro_ctx* c, const DevField& v, const DevField* w, std::vector<double>& nv,
@@ -1606,20 +1612,19 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   // block partials, the first and second passes' sums, then the cycle state
   const size_t sum_off = size_t(blocks) * 2 * kMaxList;
   const size_t state_off = sum_off + 4 * kMaxList;
-  double* part = nullptr;
-  LCK(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * state_off + sizeof(GcrState), st));
+  // (the context's solver scratch: a solve allocates nothing)
+  const size_t mask_off = sizeof(double) * state_off + (sizeof(GcrState) + 15) / 16 * 16;
+  char* scr = static_cast<char*>(scratch(c, mask_off + 16, &rc));
+  if (!scr) return rc;
+  double* part = reinterpret_cast<double*>(scr);
   double* dsum = part + sum_off;
   double* dsum2 = dsum + 2 * kMaxList;
   GcrState* gs = reinterpret_cast<GcrState*>(part + state_off);
+  int* dmask = reinterpret_cast<int*>(scr + mask_off);
   // the cycle's iteration count comes back through the context's pinned host
   // buffer (the solvers use its first bytes for their flags; GCR does not run
   // beside them)
   int* hjdone = reinterpret_cast<int*>(static_cast<char*>(pinned(c)) + 2048);
-  struct Free {
-    double* p;
-    cudaStream_t s;
-    ~Free() { if (p) cudaFreeAsync(p, s); }
-  } free_part{part, st};
   // x = 0, r = b
   LRC(axpby(c, 0.0, *B, 0.0, *B, *X));
   LRC(axpby(c, 1.0, *B, 0.0, *B, *R));
@@ -1630,15 +1635,7 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   const double delta = prm->delta > 0.0 ? prm->delta : 0.1;
   int iters = 0, restarts = 0, fallback = 0, pcapplies = 0, stalls = 0;
   bool converged = rr < target;
-  std::vector<int> ones(1, 1);
-  int* dmask = nullptr;
-  LCK(cudaMallocAsync(reinterpret_cast<void**>(&dmask), sizeof(int), st));
-  struct FreeI {
-    int* p;
-    cudaStream_t s;
-    ~FreeI() { if (p) cudaFreeAsync(p, s); }
-  } free_mask{dmask, st};
-  LCK(cudaMemcpyAsync(dmask, ones.data(), sizeof(int), cudaMemcpyHostToDevice, st));
+  LCK(launch_fill_int(dmask, 1, st));
   while (!converged && iters < prm->max_iter) {
     // One restart cycle, enqueued whole: the coefficients of every iteration
     // are formed on the device (gcr_coef_kernel), and the iterations after

@@ -39,6 +39,7 @@ int64_t vh(iro_ctx* c);
 void* state(iro_ctx* c);
 int* done(iro_ctx* c);
 void* pinned(iro_ctx* c);
+void* scratch(iro_ctx* c, size_t bytes, int* rc);
 int device(iro_ctx* c);
 bool op_is_full(int op);
 int op_subset(int op);
@@ -1158,13 +1159,14 @@ extern "C" int iro_md_force(iro_ctx* c, int op, double mass, double csw, const d
   RC(import_field(c, eta, full, *E));
   RC(import_field(c, zeta, full, *Z));
   const size_t nF = size_t(72) * size_t(volume(c));
-  double* F = nullptr;
-  CK(cudaMallocAsync(reinterpret_cast<void**>(&F), nF * sizeof(double), st));
-  struct FreeF {
-    double* p;
-    cudaStream_t s;
-    ~FreeF() { if (p) cudaFreeAsync(p, s); }
-  } guard{F, st};
+  const bool clover_term = op == IRO_OP_CLOVER_FULL && csw != 0.0;
+  const size_t nL = clover_term ? size_t(6) * 9 * size_t(volume(c)) : 0;
+  // the force and (clover) Lambda_k in the context's solver scratch, which
+  // stays allocated: repeated calls allocate nothing
+  const size_t f_bytes = (nF * sizeof(double) + 255) / 256 * 256;
+  char* scr = static_cast<char*>(scratch(c, f_bytes + nL * sizeof(double2), &rc));
+  if (!scr) return rc;
+  double* F = reinterpret_cast<double*>(scr);
   CK(cudaMemsetAsync(F, 0, nF * sizeof(double), st));
   const Geom& g = geom(c);
   const GaugePtr U = gauge_double(c);
@@ -1174,20 +1176,13 @@ extern "C" int iro_md_force(iro_ctx* c, int op, double mass, double csw, const d
       CK(launch_force(g, U, recon, p, E->half(1 - p), Z->half(p), 0, -k, F, st));
       CK(launch_force(g, U, recon, p, Z->half(1 - p), E->half(p), 1, -k, F, st));
     }
-    if (op == IRO_OP_CLOVER_FULL && csw != 0.0) {
+    if (clover_term) {
       // the clover block of Dirac_Clover::md_force: Lambda_k for the 6 planes
       // (6 * 9 complex per site), then the leaf derivatives; its site offsets
       // reach two sites out, which one periodic wrap covers for extents >= 2
       for (int d = 0; d < 4; ++d)
         if (g.L[d] < 2) return set_error(c, IRO_BAD_ARG, "clover force needs every extent >= 2");
-      const size_t nL = size_t(6) * 9 * size_t(volume(c));
-      double2* lam = nullptr;
-      CK(cudaMallocAsync(reinterpret_cast<void**>(&lam), nL * sizeof(double2), st));
-      struct FreeL {
-        double2* p;
-        cudaStream_t s;
-        ~FreeL() { if (p) cudaFreeAsync(p, s); }
-      } lguard{lam, st};
+      double2* lam = reinterpret_cast<double2*>(scr + f_bytes);
       CK(launch_clover_force(g, gauge_format_g(c), E->half(0), E->half(1), Z->half(0), Z->half(1),
                              -k * csw / 4.0, lam, F, st));
     }
