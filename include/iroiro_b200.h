@@ -359,7 +359,10 @@ typedef struct {
    restarted residual in FP64; convergence is declared on the FP64 true
    residual.  When two restart cycles in a row fail to reduce the residual by
    4x, the solve finishes with the mixed-precision reliable-update CG.  b and x
-   are FP64 full-lattice device fields, x0 = 0. */
+   are FP64 full-lattice device fields, x0 = 0.  Each restart cycle is
+   enqueued whole, its coefficients formed on the device, and the host waits
+   once per cycle; the workspaces and a small scratch are allocated by the
+   context's first solve and kept. */
 int iro_gcr_solve_field(iro_ctx* ctx, int op, double mass, double csw, const iro_ptc* net,
                         const iro_gcr_params* prm, const iro_field* b, iro_field* x,
                         iro_gcr_out* out);
