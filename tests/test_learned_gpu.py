@@ -96,3 +96,31 @@ def test_training_lowers_loss_and_gcr_iterations():
         its[name] = (o.iterations, o.fallback)
     # the trained network removes the stall (no CG fallback) and most iterations
     assert its["trained"][1] == 0 and its["trained"][0] < 0.6 * its["none"][0], its
+
+
+def test_solver_scratch_shared_by_gcr_and_md_force():
+    """GCR keeps its per-call state (block partials, the cycle's coefficients)
+    in the context's solver scratch, which the clover MD force then grows for
+    its force and Lambda buffers: on one context a GCR solve, a force and the
+    same GCR solve again give the same bits, and the force equals the one of a
+    fresh context."""
+    L = [8, 8, 8, 8]
+    V = int(np.prod(L))
+    m, csw = 0.5 / 0.12 - 4, 1.0
+    u = ib.synth_gauge(L, 0.2, 131)
+    ctx = ib.Context(L, 0)
+    ctx.upload_gauge(u, force=True)
+    Dw = ib.Dirac_Wilson(m, u, ctx=ctx)
+    b = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(V, 132))
+    net = learned.PTCNet(ctx, learned.DEFAULT_WIDTHS)
+    x1 = ib.DeviceField(ctx, 2, "double")
+    o1, st1 = learned.Solver_GCR(Dw, net).solve_field(b, x1)
+    e, z = ib.synth_gaussian(V, 133), ib.synth_gaussian(V, 134)
+    F1 = ib.Dirac_Clover(Dw, csw, u, ctx=ctx).md_force(e, z)
+    x2 = ib.DeviceField(ctx, 2, "double")
+    o2, st2 = learned.Solver_GCR(Dw, net).solve_field(b, x2)
+    assert st1 == ib.OK and st2 == ib.OK and o1.iterations == o2.iterations, (o1, o2)
+    assert np.array_equal(x1.download(), x2.download())
+    ctx2 = ib.Context(L, 0)
+    F2 = ib.Dirac_Clover(ib.Dirac_Wilson(m, u, ctx=ctx2), csw, u, ctx=ctx2).md_force(e, z)
+    assert np.array_equal(F1, F2)
