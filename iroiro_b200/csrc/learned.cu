@@ -1634,7 +1634,7 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   double rr = bn[0];
   const double delta = prm->delta > 0.0 ? prm->delta : 0.1;
   int iters = 0, restarts = 0, fallback = 0, pcapplies = 0, stalls = 0;
-  bool converged = rr < target;
+  bool converged = rr < target || rr == 0.0;  // b = 0: x = 0 is the solution
   LCK(launch_fill_int(dmask, 1, st));
   while (!converged && iters < prm->max_iter) {
     // One restart cycle, enqueued whole: the coefficients of every iteration
@@ -1724,7 +1724,7 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
     }
   }
   auto t1 = std::chrono::steady_clock::now();
-  out->diff = std::sqrt(rr / bn[0]);
+  out->diff = bn[0] > 0.0 ? std::sqrt(rr / bn[0]) : 0.0;
   out->iterations = converged ? iters : -1;
   out->timing_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   out->restarts = restarts;

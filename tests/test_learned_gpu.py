@@ -124,3 +124,14 @@ def test_solver_scratch_shared_by_gcr_and_md_force():
     ctx2 = ib.Context(L, 0)
     F2 = ib.Dirac_Clover(ib.Dirac_Wilson(m, u, ctx=ctx2), csw, u, ctx=ctx2).md_force(e, z)
     assert np.array_equal(F1, F2)
+
+
+def test_gcr_zero_source_returns_zero():
+    """b = 0: x = 0 is the solution, returned without an iteration."""
+    L = [4, 4, 4, 8]
+    ctx, D, _ = _pair(L, 141)
+    b = ib.DeviceField(ctx, 2, "double").upload(np.zeros(int(np.prod(L)) * 24))
+    x = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(int(np.prod(L)), 142))
+    o, st = learned.Solver_GCR(D, learned.PTCNet(ctx, learned.DEFAULT_WIDTHS)).solve_field(b, x)
+    assert st == ib.OK and o.iterations == 0 and o.diff == 0.0
+    assert not np.any(x.download())
