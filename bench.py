@@ -408,14 +408,16 @@ def batched_solves(torch, device):
     return out
 
 
-def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), nkrylov=16, delta=0.03):
+def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 4, 4, 4), nkrylov=16, delta=0.03,
+                   krylov="half"):
     """Learned preconditioner: a PTC network trained by the library's own
     forward/backward kernels on pairs (b = D^dag D v, v) from `nfields` seeded
     16^3x32 gauge fields (eps=0.2, kappa=0.12), then applied inside flexible
     GCR at 32^3x64 and 48^3x96 (unseen fields, one Gaussian source each)
     against GCR without it and against CG on the same full-lattice D^dag D:
     FP64 and mixed precision.  GCR restarts after `nkrylov` directions or once
-    its iterated residual has fallen by `delta`.  Every solve stops on the FP64
+    its iterated residual has fallen by `delta`; its directions z_j, w_j are
+    stored in `krylov` precision (FP16: D^dag D applied in mixed FP16).  Every solve stops on the FP64
     true residual 1e-10; each is timed after an untimed call, as the median
     (and the minimum) of 9 runs at 32^3x64 and one run at 48^3x96."""
     import iroiro_b200 as ib
@@ -433,7 +435,7 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
            "network": {"widths": list(widths), "train_fields": nfields, "train_lattice": "16^3x32",
                        "epochs": epochs, "train_s": round(train_s, 1),
                        "loss_first": round(hist[0], 4), "loss_last": round(hist[-1], 4)},
-           "gcr": {"nkrylov": nkrylov, "delta": delta}}
+           "gcr": {"nkrylov": nkrylov, "delta": delta, "krylov": krylov}}
 
     samples = {}
 
@@ -466,7 +468,7 @@ def learned_solves(torch, device, nfields=100, epochs=15, widths=(4, 8, 8, 4), n
         res = {}
         for name, n in (("gcr_network", net), ("gcr_plain", None)):
             x = ib.DeviceField(ctx, 2, "double")
-            slv = learned.Solver_GCR(D, n, nkrylov=nkrylov, delta=delta)
+            slv = learned.Solver_GCR(D, n, nkrylov=nkrylov, delta=delta, krylov=krylov)
             ms, (o, rc) = timed(lambda: slv.solve_field(b, x), reps)
             res[name] = {"ms": round(ms, 1), "ms_min": samples["min"], "ms_samples": samples["last"],
                          "iterations": o.iterations,

@@ -342,6 +342,8 @@ typedef struct {
   int max_iter;
   int nkrylov;      /* directions kept before a restart (1..16) */
   double delta;     /* restart when the iterated |r| fell by delta; <= 0: 0.1 */
+  int krylov_half;  /* 0: the directions z_j, w_j = A z_j in FP32; 1: in FP16 (A applied
+                       in mixed FP16; an SU(3) gauge field); r and the correction FP32 */
 } iro_gcr_params;
 
 typedef struct {

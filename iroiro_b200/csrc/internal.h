@@ -255,19 +255,22 @@ struct GcrState {
   float cre[kMaxList], cim[kMaxList];   // the current coefficients in FP32 (update / correction)
   float ure, uim;                       // the current alpha in FP32
 };
-// <w_q, t> (q < m): block partials into part, their block-order sums into
-// out[2m]; nothing when skip is set
+// The Krylov fields w, z (and t) are FP32 or FP16 (pw/px = PREC_SINGLE or
+// PREC_HALF); the residual r and the correction are FP32.
+// <w_q, t> (q < m; w_{m-1} is r): block partials into part, their
+// block-order sums into out[2m]; nothing when skip is set
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
-                        double* out, const int* skip, cudaStream_t st);
+                        double* out, const int* skip, int pw, cudaStream_t st);
 // y += sum_{q < m} c_q x_q with the coefficients s->cre/cim (q < *count when
 // count is given; sign -1: y -= ...); nothing when skip is set
-cudaError_t launch_caxpy_dev(int64_t n, int m, const CFieldList& x, const GcrState* s,
+cudaError_t launch_caxpy_dev(int64_t n, int m, const CFieldList& x, int px, const GcrState* s,
                              const int* count, float sign, SpinorPtr y, const int* skip,
                              cudaStream_t st);
 // one Gram-Schmidt step of GCR in one pass: wj += sum_{q<m} c_q w_q, then, if
-// s->plain[j], r -= alpha wj with the updated wj (coefficients from s)
-cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const GcrState* s, int j,
-                              SpinorPtr wj, SpinorPtr r, cudaStream_t st);
+// s->plain[j], r -= alpha wj with the updated wj (coefficients from s) and,
+// given feat, the network's input features of the new r
+cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, int pw, const GcrState* s, int j,
+                              SpinorPtr wj, SpinorPtr r, float2* feat, cudaStream_t st);
 // the cycle's state at its start
 cudaError_t launch_gcr_init(GcrState* s, double rr, double target, double d2, int limit,
                             cudaStream_t st);

@@ -739,6 +739,7 @@ __global__ void spinor_to_feat_kernel(int Vh, SpinorPtr e, SpinorPtr o, float2* 
     for (int k = 0; k < 12; ++k) feat_set(feat, s, k / 3, k % 3, 2 * Vh, make_float2(v[k].re, v[k].im));
   }
 }
+template <int PO>
 __global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o, const int* skip) {
   if (skip && *skip) return;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < 2 * Vh; s += gridDim.x * blockDim.x) {
@@ -749,7 +750,7 @@ __global__ void feat_to_spinor_kernel(int Vh, const float2* feat, SpinorPtr e, S
       const float2 t = feat_get(feat, s, k / 3, k % 3, 2 * Vh);
       v[k] = {t.x, t.y};
     }
-    SpinorIO<PREC_SINGLE>::store(p ? o : e, s - p * Vh, v);
+    SpinorIO<PO>::store(p ? o : e, s - p * Vh, v);
   }
 }
 
@@ -917,9 +918,13 @@ cudaError_t launch_spinor_to_feat(int Vh, SpinorPtr e, SpinorPtr o, float2* feat
   spinor_to_feat_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, e, o, feat, skip);
   return cudaGetLastError();
 }
+// to an FP32 (or, prec = PREC_HALF, FP16) spinor field
 cudaError_t launch_feat_to_spinor(int Vh, const float2* feat, SpinorPtr e, SpinorPtr o, cudaStream_t st,
-                                  const int* skip = nullptr) {
-  feat_to_spinor_kernel<<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, feat, e, o, skip);
+                                  const int* skip = nullptr, int prec = PREC_SINGLE) {
+  if (prec == PREC_HALF)
+    feat_to_spinor_kernel<PREC_HALF><<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, feat, e, o, skip);
+  else
+    feat_to_spinor_kernel<PREC_SINGLE><<<(2 * Vh + 255) / 256, 256, 0, st>>>(Vh, feat, e, o, skip);
   return cudaGetLastError();
 }
 
@@ -970,7 +975,9 @@ cudaError_t launch_loss_grad(int n, const float2* y, const float2* t, float scal
 int loss_blocks() { return kRedBlocks; }
 
 // ---- complex linear algebra for GCR on FP32 fields ---------------------------------------
-// <w_q, t> = sum conj(w_q) t for q < m, per-block partials [block][2m]
+// <w_q, t> = sum conj(w_q) t for q < m, per-block partials [block][2m]; the
+// last listed field is FP32 (GCR's residual), the others and t of type PW
+template <int PW>
 __global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double* part, const int* skip) {
   if (skip && *skip) return;  // the same value in every thread
   __shared__ double sm[2 * kMaxList][64];
@@ -980,11 +987,14 @@ __global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double*
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     Cx<float> tv[12], wv[12];
-    SpinorIO<PREC_SINGLE>::load(t, i, tv);
+    SpinorIO<PW>::load(t, i, tv);
 #pragma unroll
     for (int q = 0; q < kMaxList; ++q) {
       if (q >= m) break;
-      SpinorIO<PREC_SINGLE>::load(w.f[q], i, wv);
+      if (q == m - 1)
+        SpinorIO<PREC_SINGLE>::load(w.f[q], i, wv);
+      else
+        SpinorIO<PW>::load(w.f[q], i, wv);
       double re = 0.0, im = 0.0;
 #pragma unroll
       for (int k = 0; k < 12; ++k) {
@@ -1021,7 +1031,8 @@ __global__ void cdot_finish_kernel(int blocks, int m2, const double* part, doubl
 }
 
 // y += sign sum_q c_q x_q  (complex coefficients from the cycle state; the
-// first *count of the m fields when count is given)
+// first *count of the m fields when count is given); x of type PX, y FP32
+template <int PX>
 __global__ void caxpy_dev_kernel(int64_t n, int m, CFieldList x, const GcrState* s, const int* count,
                                  float sign, SpinorPtr y, const int* skip) {
   if (skip && *skip) return;
@@ -1039,7 +1050,7 @@ __global__ void caxpy_dev_kernel(int64_t n, int m, CFieldList x, const GcrState*
     Cx<float> yv[12], xv[12];
     SpinorIO<PREC_SINGLE>::load(y, i, yv);
     for (int q = 0; q < k; ++q) {
-      SpinorIO<PREC_SINGLE>::load(x.f[q], i, xv);
+      SpinorIO<PX>::load(x.f[q], i, xv);
       const Cx<float> cq = {cre[q], cim[q]};
 #pragma unroll
       for (int c = 0; c < 12; ++c) yv[c] = yv[c] + cq * xv[c];
@@ -1048,11 +1059,13 @@ __global__ void caxpy_dev_kernel(int64_t n, int m, CFieldList x, const GcrState*
   }
 }
 
-// iteration j: wj += sum_{q<m} c_q w_q; then, unless the coefficient kernel
+// iteration j (the w of type PW, r FP32): wj += sum_{q<m} c_q w_q; then, unless the coefficient kernel
 // found w_j nearly in the span of the w_q (s->plain[j] = 0: a second pass
-// forms |w'_j|^2 and <r, w'_j> first), r -= alpha wj with the updated wj
+// forms |w'_j|^2 and <r, w'_j> first), r -= alpha wj with the updated wj,
+// and, given feat, the network's input features of the new r
+template <int PW>
 __global__ void gcr_update_kernel(int64_t n, int m, CFieldList w, const GcrState* s, int j,
-                                  SpinorPtr wj, SpinorPtr r) {
+                                  SpinorPtr wj, SpinorPtr r, float2* feat) {
   if (s->skip[j]) return;
   __shared__ float cre[kMaxList], cim[kMaxList];
   if (threadIdx.x < kMaxList) {
@@ -1065,19 +1078,31 @@ __global__ void gcr_update_kernel(int64_t n, int m, CFieldList w, const GcrState
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
     Cx<float> yv[12], xv[12];
-    SpinorIO<PREC_SINGLE>::load(wj, i, yv);
+    SpinorIO<PW>::load(wj, i, yv);
     for (int q = 0; q < m; ++q) {
-      SpinorIO<PREC_SINGLE>::load(w.f[q], i, xv);
+      SpinorIO<PW>::load(w.f[q], i, xv);
       const Cx<float> cq = {cre[q], cim[q]};
 #pragma unroll
       for (int k = 0; k < 12; ++k) yv[k] = yv[k] + cq * xv[k];
     }
-    SpinorIO<PREC_SINGLE>::store(wj, i, yv);
+    SpinorIO<PW>::store(wj, i, yv);
     if (plain) {
       SpinorIO<PREC_SINGLE>::load(r, i, xv);
 #pragma unroll
       for (int k = 0; k < 12; ++k) xv[k] = xv[k] - a * yv[k];
       SpinorIO<PREC_SINGLE>::store(r, i, xv);
+      if (feat) {
+        // the network's input features of the new r (as spinor_to_feat: site
+        // i of the full field, spin pair q and colour c in float4 row 3q + c)
+        float4* f4 = reinterpret_cast<float4*>(feat);
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const Cx<float> lo = xv[6 * q + c], hi = xv[6 * q + 3 + c];
+            f4[size_t(3 * q + c) * size_t(n) + size_t(i)] = make_float4(lo.re, hi.re, lo.im, hi.im);
+          }
+      }
     }
   }
 }
@@ -1199,8 +1224,11 @@ cudaError_t launch_bounded_wait_probe(uint64_t limit_ns, int* err, unsigned long
 }
 
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
-                        double* out, const int* skip, cudaStream_t st) {
-  cdot_kernel<<<blocks, 256, 0, st>>>(n, m, w, t, part, skip);
+                        double* out, const int* skip, int pw, cudaStream_t st) {
+  if (pw == PREC_HALF)
+    cdot_kernel<PREC_HALF><<<blocks, 256, 0, st>>>(n, m, w, t, part, skip);
+  else
+    cdot_kernel<PREC_SINGLE><<<blocks, 256, 0, st>>>(n, m, w, t, part, skip);
   cdot_finish_kernel<<<1, 64, 0, st>>>(blocks, 2 * m, part, out, skip);
   return cudaGetLastError();
 }
@@ -1208,15 +1236,21 @@ static int blas_grid(int64_t n) {
   int grid = int((n + 255) / 256);
   return grid > 148 * 16 ? 148 * 16 : grid;
 }
-cudaError_t launch_caxpy_dev(int64_t n, int m, const CFieldList& x, const GcrState* s,
+cudaError_t launch_caxpy_dev(int64_t n, int m, const CFieldList& x, int px, const GcrState* s,
                              const int* count, float sign, SpinorPtr y, const int* skip,
                              cudaStream_t st) {
-  caxpy_dev_kernel<<<blas_grid(n), 256, 0, st>>>(n, m, x, s, count, sign, y, skip);
+  if (px == PREC_HALF)
+    caxpy_dev_kernel<PREC_HALF><<<blas_grid(n), 256, 0, st>>>(n, m, x, s, count, sign, y, skip);
+  else
+    caxpy_dev_kernel<PREC_SINGLE><<<blas_grid(n), 256, 0, st>>>(n, m, x, s, count, sign, y, skip);
   return cudaGetLastError();
 }
-cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, const GcrState* s, int j,
-                              SpinorPtr wj, SpinorPtr r, cudaStream_t st) {
-  gcr_update_kernel<<<blas_grid(n), 256, 0, st>>>(n, m, w, s, j, wj, r);
+cudaError_t launch_gcr_update(int64_t n, int m, const CFieldList& w, int pw, const GcrState* s, int j,
+                              SpinorPtr wj, SpinorPtr r, float2* feat, cudaStream_t st) {
+  if (pw == PREC_HALF)
+    gcr_update_kernel<PREC_HALF><<<blas_grid(n), 256, 0, st>>>(n, m, w, s, j, wj, r, feat);
+  else
+    gcr_update_kernel<PREC_SINGLE><<<blas_grid(n), 256, 0, st>>>(n, m, w, s, j, wj, r, feat);
   return cudaGetLastError();
 }
 cudaError_t launch_gcr_init(GcrState* s, double rr, double target, double d2, int limit,
@@ -1382,8 +1416,8 @@ int field_to_feat(iro_ctx* c, const DevField& f, float2* feat, const int* skip =
 }
 
 int feat_to_field(iro_ctx* c, const float2* feat, DevField& f, const int* skip = nullptr) {
-  if (f.prec == PREC_SINGLE) {
-    LCK(launch_feat_to_spinor(int(f.Vh), feat, f.half(0), f.half(1), stream(c), skip));
+  if (f.prec == PREC_SINGLE || f.prec == PREC_HALF) {
+    LCK(launch_feat_to_spinor(int(f.Vh), feat, f.half(0), f.half(1), stream(c), skip, f.prec));
     return IRO_OK;
   }
   int rc = IRO_OK;
@@ -1601,11 +1635,13 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
   DevField* S = workspace(c, 2, PREC_DOUBLE, 1, 82, &rc); if (!S) return rc;
   DevField* r32 = workspace(c, 2, PREC_SINGLE, 1, 83, &rc); if (!r32) return rc;
   DevField* e32 = workspace(c, 2, PREC_SINGLE, 1, 84, &rc); if (!e32) return rc;
-  DevField* t32 = workspace(c, 2, PREC_SINGLE, 1, 85, &rc); if (!t32) return rc;
+  // the Krylov fields z_j, w_j (and D z_j) in FP32 or FP16
+  const int kp = prm->krylov_half ? PREC_HALF : PREC_SINGLE;
+  DevField* tk = workspace(c, 2, kp, 1, 85, &rc); if (!tk) return rc;
   std::vector<DevField*> Z(m), W(m);
   for (int j = 0; j < m; ++j) {
-    Z[j] = workspace(c, 2, PREC_SINGLE, 1, 90 + j, &rc); if (!Z[j]) return rc;
-    W[j] = workspace(c, 2, PREC_SINGLE, 1, 90 + kMaxVec + j, &rc); if (!W[j]) return rc;
+    Z[j] = workspace(c, 2, kp, 1, 90 + j, &rc); if (!Z[j]) return rc;
+    W[j] = workspace(c, 2, kp, 1, 90 + kMaxVec + j, &rc); if (!W[j]) return rc;
   }
   const int64_t nel = R->sites();
   const int blocks = 296;
@@ -1653,39 +1689,44 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
       const int* skip = &gs->skip[j];
       // z_j = N(r) (or r without a network), w_j = A z_j
       if (net) {
-        LRC(field_to_feat(c, *r32, net->act[0], skip));
+        // the features of r: the previous iteration's update wrote them
+        // unless it took the second pass (plain[j - 1] = 0)
+        LRC(field_to_feat(c, *r32, net->act[0], j == 0 ? skip : &gs->plain[j - 1]));
         LRC(forward(c, const_cast<iro_ptc*>(net), skip));
         LRC(feat_to_field(c, net->act[net->nl], *Z[j], skip));
-      } else {
+      } else if (kp == PREC_SINGLE) {
         LRC(axpby(c, 1.0, *r32, 0.0, *r32, *Z[j]));
+      } else {
+        LRC(convert(c, *r32, *Z[j]));
       }
-      LRC(apply(c, op, mass, csw, false, *Z[j], *t32, nullptr, 0, skip));
-      LRC(apply(c, op, mass, csw, true, *t32, *W[j], nullptr, 0, skip));
+      LRC(apply(c, op, mass, csw, false, *Z[j], *tk, nullptr, 0, skip));
+      LRC(apply(c, op, mass, csw, true, *tk, *W[j], nullptr, 0, skip));
       // one pass forms <w_q, w_j> (q < j), |w_j|^2 and <r, w_j>; the
       // coefficient kernel turns them into beta_q, |w'_j|^2 and alpha, and a
       // second pass orthogonalises w_j and updates r -= alpha w'_j
       CFieldList L{};
       for (int q = 0; q <= j; ++q) L.f[q] = W[q]->all();
       L.f[j + 1] = r32->all();
-      LCK(launch_cdot(nel, j + 2, L, W[j]->all(), part, blocks, dsum, skip, st));
+      LCK(launch_cdot(nel, j + 2, L, W[j]->all(), part, blocks, dsum, skip, kp, st));
       LCK(launch_gcr_coef(gs, dsum, j, m, 0, st));
-      LCK(launch_gcr_update(nel, j, L, gs, j, W[j]->all(), r32->all(), st));
+      LCK(launch_gcr_update(nel, j, L, kp, gs, j, W[j]->all(), r32->all(),
+                            net ? net->act[0] : nullptr, st));
       // w_j nearly in the span of the w_q (plain[j] = 0): |w'_j|^2 and
       // <r, w'_j> from the orthogonalised vector, then r -= alpha w'_j
       const int* single = &gs->plain[j];
       CFieldList L2{};
       L2.f[0] = W[j]->all();
       L2.f[1] = r32->all();
-      LCK(launch_cdot(nel, 2, L2, W[j]->all(), part, blocks, dsum2, single, st));
+      LCK(launch_cdot(nel, 2, L2, W[j]->all(), part, blocks, dsum2, single, kp, st));
       LCK(launch_gcr_coef(gs, dsum2, j, m, 1, st));
-      LCK(launch_caxpy_dev(nel, 1, L2, gs, nullptr, -1.f, r32->all(), single, st));
+      LCK(launch_caxpy_dev(nel, 1, L2, kp, gs, nullptr, -1.f, r32->all(), single, st));
     }
     // e = sum_i gamma_i z_i, gamma = T alpha over the iterations done
     {
       LCK(launch_gcr_gamma(gs, st));
       CFieldList L{};
       for (int i = 0; i < cyc; ++i) L.f[i] = Z[i]->all();
-      LCK(launch_caxpy_dev(nel, cyc, L, gs, &gs->jdone, 1.f, e32->all(), nullptr, st));
+      LCK(launch_caxpy_dev(nel, cyc, L, kp, gs, &gs->jdone, 1.f, e32->all(), nullptr, st));
       LCK(cudaMemcpyAsync(hjdone, &gs->jdone, sizeof(int), cudaMemcpyDeviceToHost, st));
     }
     // x += e, r = b - A x in FP64

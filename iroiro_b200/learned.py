@@ -34,7 +34,8 @@ class GCROut(ctypes.Structure):
 
 class GCRParams(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_double), ("max_iter", ctypes.c_int),
-                ("nkrylov", ctypes.c_int), ("delta", ctypes.c_double)]
+                ("nkrylov", ctypes.c_int), ("delta", ctypes.c_double),
+                ("krylov_half", ctypes.c_int)]
 
 
 def _declare():
@@ -229,16 +230,20 @@ def train(net: PTCNet, pairs, epochs: int = 20, lr: float = 2e-3, log=None):
 
 class Solver_GCR:
     """Flexible GCR for (D^dag D) x = b on the full lattice with the network
-    as right preconditioner (net=None: plain GCR); FP32 inner iterations,
-    FP64 restarts and convergence test; mixed-precision CG fallback on a stall."""
+    as right preconditioner (net=None: plain GCR); FP32 inner iterations
+    (krylov="half": the directions z_j and w_j = A z_j stored in FP16 and A
+    applied in mixed FP16), FP64 restarts and convergence test;
+    mixed-precision CG fallback on a stall."""
 
     def __init__(self, D, net: PTCNet = None, prec: float = 1e-20, max_iter: int = 5000,
-                 nkrylov: int = 8, delta: float = 0.1):
+                 nkrylov: int = 8, delta: float = 0.1, krylov: str = "single"):
         if D.op not in (OP_WILSON_FULL, OP_CLOVER_FULL):
             raise IroError(BAD_ARG, "GCR needs a full-lattice Wilson or clover operator")
+        if krylov not in ("single", "half"):
+            raise IroError(BAD_ARG, "krylov must be 'single' or 'half'")
         self.L = _declare()
         self.D, self.net = D, net
-        self.params = GCRParams(prec, max_iter, nkrylov, delta)
+        self.params = GCRParams(prec, max_iter, nkrylov, delta, 1 if krylov == "half" else 0)
 
     def solve_field(self, b: DeviceField, x: DeviceField):
         """Returns (GCROut, status) with status OK or NOT_CONVERGED."""

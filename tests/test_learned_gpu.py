@@ -67,7 +67,9 @@ def _pair(L, seed):
     return ctx, D, b
 
 
-def test_gcr_converges_with_and_without_network():
+@pytest.mark.parametrize("krylov", ["single", "half"])
+def test_gcr_converges_with_and_without_network(krylov):
+    # FP32 or FP16 directions: the FP64 restarts bring both to the FP64 CG solution
     L = [8, 8, 8, 8]
     ctx, D, b = _pair(L, 61)
     x_cg = ib.DeviceField(ctx, 2, "double")
@@ -75,7 +77,7 @@ def test_gcr_converges_with_and_without_network():
     ref = x_cg.download()
     for net in (None, learned.PTCNet(ctx, learned.DEFAULT_WIDTHS)):
         x = ib.DeviceField(ctx, 2, "double")
-        o, st = learned.Solver_GCR(D, net).solve_field(b, x)
+        o, st = learned.Solver_GCR(D, net, krylov=krylov).solve_field(b, x)
         assert st == ib.OK and o.diff < 1e-10
         assert rel(x.download(), ref) < 1e-8
 
