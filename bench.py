@@ -1025,7 +1025,7 @@ def kernel_only(args):
     import torch
     import iroiro_b200 as ib
     Lk = [int(v) for v in args.lattice.split(",")]
-    if args.kernel.startswith(("ptc,", "batched,", "multishift,")) or \
+    if args.kernel.startswith(("ptc,", "batched,", "multishift,", "gcr,")) or \
             args.kernel in ("md_force_eo", "md_force_clover"):
         return kernel_only_other(args, Lk)
     opn, prec, nrhs = args.kernel.split(",")
@@ -1058,8 +1058,10 @@ def kernel_only_other(args, Lk):
     one even/odd Wilson MD force, --kernel md_force_clover one full-lattice
     Wilson-clover MD force; --kernel batched,INNER,DELTA runs the batched
     configuration's solve (the 12 point sources on the seeded field of
-    batched_solves, on the lattice given) once untimed and once profiled; all
-    inside cudaProfilerStart/Stop."""
+    batched_solves, on the lattice given) once untimed and once profiled;
+    --kernel gcr,W-W-...,KRYLOV trains that network as learned_solves does and
+    runs its GCR solve (learned_solves' field and source, on the lattice given)
+    once untimed and once profiled; all inside cudaProfilerStart/Stop."""
     import torch
     import iroiro_b200 as ib
     from iroiro_b200 import learned
@@ -1113,6 +1115,34 @@ def kernel_only_other(args, Lk):
         print(json.dumps({"kernel": args.kernel, "lattice": Lk, "ms": round(ms, 2),
                           "iterations": max(o.Iterations for o in outs),
                           "reliable_updates": max(o.reliable_updates for o in outs), "rc": rc}))
+        return 0
+    if args.kernel.startswith("gcr,"):
+        _, wtxt, krylov = args.kernel.split(",")
+        widths = tuple(int(v) for v in wtxt.split("-"))
+        pairs = learned.make_pairs([16, 16, 16, 32], 100, seed0=SEED + 300, device=0)
+        net0 = learned.PTCNet(pairs[0].ctx, widths)
+        learned.train(net0, pairs, epochs=15, lr=3e-3)
+        for pr in pairs:
+            pr.ctx.close()
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        u = ib.synth_gauge(Lk, EPS, SEED + 301)
+        ctx.upload_gauge(u, force=True)
+        D = ib.Dirac_Wilson(MASS, u, ctx=ctx)
+        b = ib.DeviceField(ctx, 2, "double").upload(ib.synth_gaussian(V, SEED + 302))
+        x = ib.DeviceField(ctx, 2, "double")
+        net = learned.PTCNet(ctx, widths, net0.W)
+        slv = learned.Solver_GCR(D, net, nkrylov=16, delta=0.03, krylov=krylov)
+        slv.solve_field(b, x)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        t0 = time.perf_counter()
+        o, rc = slv.solve_field(b, x)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        torch.cuda.profiler.stop()
+        print(json.dumps({"kernel": args.kernel, "lattice": Lk, "ms": round(ms, 2),
+                          "iterations": o.iterations, "restarts": o.restarts, "residual": o.diff,
+                          "rc": rc}))
         return 0
     u = ib.synth_gauge(Lk, EPS, SEED, gauge_transform=True)
     ctx.upload_gauge(u, force=True)
