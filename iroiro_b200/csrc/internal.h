@@ -258,7 +258,7 @@ struct GcrState {
 // The Krylov fields w, z (and t) are FP32 or FP16 (pw/px = PREC_SINGLE or
 // PREC_HALF); the residual r and the correction are FP32.
 // <w_q, t> (q < m; w_{m-1} is r): block partials into part, their
-// block-order sums into out[2m]; nothing when skip is set
+// sums (a fixed order) into out[2m]; nothing when skip is set
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
                         double* out, const int* skip, int pw, cudaStream_t st);
 // y += sum_{q < m} c_q x_q with the coefficients s->cre/cim (q < *count when

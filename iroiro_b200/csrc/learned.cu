@@ -977,21 +977,25 @@ int loss_blocks() { return kRedBlocks; }
 // ---- complex linear algebra for GCR on FP32 fields ---------------------------------------
 // <w_q, t> = sum conj(w_q) t for q < m, per-block partials [block][2m]; the
 // last listed field is FP32 (GCR's residual), the others and t of type PW
-template <int PW>
-__global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double* part, const int* skip) {
+// M fields (a compile-time count: the loads of every field of a site can be
+// issued together and only 2M accumulators are live), 128-thread blocks
+constexpr int kCdotThreads = 128;
+template <int PW, int M>
+__global__ void __launch_bounds__(kCdotThreads) cdot_kernel(int64_t n, CFieldList w, SpinorPtr t,
+                                                            double* part, const int* skip) {
   if (skip && *skip) return;  // the same value in every thread
-  __shared__ double sm[2 * kMaxList][64];
-  double acc[2 * kMaxList];
+  __shared__ double sm[2 * M][kCdotThreads / 32];
+  double acc[2 * M];
 #pragma unroll
-  for (int q = 0; q < 2 * kMaxList; ++q) acc[q] = 0.0;
+  for (int q = 0; q < 2 * M; ++q) acc[q] = 0.0;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x) {
-    Cx<float> tv[12], wv[12];
+    Cx<float> tv[12];
     SpinorIO<PW>::load(t, i, tv);
 #pragma unroll
-    for (int q = 0; q < kMaxList; ++q) {
-      if (q >= m) break;
-      if (q == m - 1)
+    for (int q = 0; q < M; ++q) {
+      Cx<float> wv[12];
+      if (q == M - 1)
         SpinorIO<PREC_SINGLE>::load(w.f[q], i, wv);
       else
         SpinorIO<PW>::load(w.f[q], i, wv);
@@ -1005,29 +1009,34 @@ __global__ void cdot_kernel(int64_t n, int m, CFieldList w, SpinorPtr t, double*
       acc[2 * q + 1] += im;
     }
   }
-  for (int q = 0; q < 2 * m; ++q) {
+#pragma unroll
+  for (int q = 0; q < 2 * M; ++q) {
     double v = acc[q];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) sm[q][threadIdx.x >> 5] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 2 * m) {
+  if (threadIdx.x < 2 * M) {
     double v = 0.0;
-    for (int wv = 0; wv < int(blockDim.x >> 5); ++wv) v += sm[threadIdx.x][wv];
-    part[size_t(blockIdx.x) * 2 * m + threadIdx.x] = v;
+#pragma unroll
+    for (int wv = 0; wv < kCdotThreads / 32; ++wv) v += sm[threadIdx.x][wv];
+    part[size_t(blockIdx.x) * 2 * M + threadIdx.x] = v;
   }
 }
 
-// the block partials of cdot_kernel summed in block order, one thread per
-// real component (the same order and rounding as a sequential host sum)
+// the block partials of cdot_kernel summed in a fixed order: one warp per
+// real component (block q), lane l summing blocks l, l + 32, ..., then a
+// shuffle tree over the lanes
 __global__ void cdot_finish_kernel(int blocks, int m2, const double* part, double* out, const int* skip) {
   if (skip && *skip) return;
-  const int q = threadIdx.x;
+  const int q = blockIdx.x, l = threadIdx.x;
   if (q >= m2) return;
   double v = 0.0;
-  for (int b = 0; b < blocks; ++b) v += part[size_t(b) * m2 + q];
-  out[q] = v;
+  for (int b = l; b < blocks; b += 32) v += part[size_t(b) * m2 + q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (l == 0) out[q] = v;
 }
 
 // y += sign sum_q c_q x_q  (complex coefficients from the cycle state; the
@@ -1223,13 +1232,32 @@ cudaError_t launch_bounded_wait_probe(uint64_t limit_ns, int* err, unsigned long
   return cudaGetLastError();
 }
 
+template <int PW, int M>
+static void cdot_go(int64_t n, const CFieldList& w, SpinorPtr t, double* part, int blocks,
+                    const int* skip, cudaStream_t st) {
+  cdot_kernel<PW, M><<<blocks, kCdotThreads, 0, st>>>(n, w, t, part, skip);
+}
+template <int PW>
+static cudaError_t cdot_count(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part,
+                              int blocks, const int* skip, cudaStream_t st) {
+  static_assert(kMaxList == 18, "one case per field count");
+  switch (m) {
+#define IRO_CD(M) \
+  case M: cdot_go<PW, M>(n, w, t, part, blocks, skip, st); break;
+    IRO_CD(1) IRO_CD(2) IRO_CD(3) IRO_CD(4) IRO_CD(5) IRO_CD(6) IRO_CD(7) IRO_CD(8) IRO_CD(9)
+    IRO_CD(10) IRO_CD(11) IRO_CD(12) IRO_CD(13) IRO_CD(14) IRO_CD(15) IRO_CD(16) IRO_CD(17)
+    IRO_CD(18)
+#undef IRO_CD
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaSuccess;
+}
 cudaError_t launch_cdot(int64_t n, int m, const CFieldList& w, SpinorPtr t, double* part, int blocks,
                         double* out, const int* skip, int pw, cudaStream_t st) {
-  if (pw == PREC_HALF)
-    cdot_kernel<PREC_HALF><<<blocks, 256, 0, st>>>(n, m, w, t, part, skip);
-  else
-    cdot_kernel<PREC_SINGLE><<<blocks, 256, 0, st>>>(n, m, w, t, part, skip);
-  cdot_finish_kernel<<<1, 64, 0, st>>>(blocks, 2 * m, part, out, skip);
+  const cudaError_t e = pw == PREC_HALF ? cdot_count<PREC_HALF>(n, m, w, t, part, blocks, skip, st)
+                                        : cdot_count<PREC_SINGLE>(n, m, w, t, part, blocks, skip, st);
+  if (e != cudaSuccess) return e;
+  cdot_finish_kernel<<<2 * m, 32, 0, st>>>(blocks, 2 * m, part, out, skip);
   return cudaGetLastError();
 }
 static int blas_grid(int64_t n) {
@@ -1644,7 +1672,7 @@ int iro_gcr_solve_field(iro_ctx* c, int op, double mass, double csw, const iro_p
     W[j] = workspace(c, 2, kp, 1, 90 + kMaxVec + j, &rc); if (!W[j]) return rc;
   }
   const int64_t nel = R->sites();
-  const int blocks = 296;
+  const int blocks = 148 * 8;  // inner-product partials: 8 blocks of 128 threads per SM
   // block partials, the first and second passes' sums, then the cycle state
   const size_t sum_off = size_t(blocks) * 2 * kMaxList;
   const size_t state_off = sum_off + 4 * kMaxList;
