@@ -1309,7 +1309,6 @@ cudaError_t launch_gcr_gamma(GcrState* s, cudaStream_t st) {
 #include <algorithm>
 #include <chrono>
 #include <cmath>
-#include <complex>
 #include <memory>
 #include <string>
 
