@@ -92,10 +92,6 @@ cudaError_t launch_dot(int prec, int64_t sites, int nrhs, SpinorPtr a, SpinorPtr
 // CG: r = b - s, p = r; reduce |r|^2, |b|^2 (stage ST_CG_INIT)
 cudaError_t launch_cg_init(int prec, int64_t Vh, int nrhs, SpinorPtr b, SpinorPtr s, SpinorPtr r,
                            SpinorPtr p, const Reduce& red, int max_blocks, cudaStream_t st);
-// CG: x += alpha p; r -= alpha s; reduce |r|^2 (stage ST_CG_BETA)
-cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr r, SpinorPtr p,
-                         SpinorPtr s, const CGState* state, const Reduce& red, int max_blocks,
-                         cudaStream_t st);
 // CG: p = beta p + r
 cudaError_t launch_cg_p(int prec, int64_t Vh, int nrhs, SpinorPtr p, SpinorPtr r, SpinorPtr x,
                         const CGState* state, const int* done, cudaStream_t st);

@@ -263,47 +263,6 @@ cudaError_t launch_cg_init(int prec, int64_t Vh, int nrhs, SpinorPtr b, SpinorPt
   return cudaGetLastError();
 }
 
-// solve_step (solver_CG.cpp:131-147): x += cr p; r -= cr s; rr = (r,r)
-template <int SP>
-__global__ void __launch_bounds__(256) cg_xr_kernel(int64_t vh, int nrhs, SpinorPtr x, SpinorPtr r, SpinorPtr p,
-                             SpinorPtr s, const CGState* state, Reduce red) {
-  using R = typename SpinorIO<SP>::Real;
-  const int64_t n = vh * nrhs;
-  double acc = 0.0;
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x) {
-    const int rhs = int(i % nrhs);
-    if (red.done[rhs]) continue;
-    const double a = state[rhs].alpha;
-    Cx<R> xv[12], rv[12], pv[12], sv[12];
-    SpinorIO<SP>::load(x, i, xv);
-    SpinorIO<SP>::load(r, i, rv);
-    SpinorIO<SP>::load(p, i, pv);
-    SpinorIO<SP>::load(s, i, sv);
-#pragma unroll
-    for (int k = 0; k < 12; ++k) {
-      xv[k] = xv[k] + R(a) * pv[k];
-      rv[k] = rv[k] - R(a) * sv[k];
-      acc += double(rv[k].re) * rv[k].re + double(rv[k].im) * rv[k].im;
-    }
-    SpinorIO<SP>::store(x, i, xv);
-    SpinorIO<SP>::store(r, i, rv);
-  }
-  block_reduce_finish<1>(red, &acc, nrhs, blockIdx.x, gridDim.x);
-}
-
-cudaError_t launch_cg_xr(int prec, int64_t Vh, int nrhs, SpinorPtr x, SpinorPtr r, SpinorPtr p,
-                         SpinorPtr s, const CGState* state, const Reduce& red, int max_blocks,
-                         cudaStream_t st) {
-  LaunchCfg c = launch_cfg(Vh, nrhs, max_blocks);
-  switch (prec) {
-    case PREC_DOUBLE: cg_xr_kernel<PREC_DOUBLE><<<c.grid, c.block, 0, st>>>(Vh, nrhs, x, r, p, s, state, red); break;
-    case PREC_SINGLE: cg_xr_kernel<PREC_SINGLE><<<c.grid, c.block, 0, st>>>(Vh, nrhs, x, r, p, s, state, red); break;
-    default: cg_xr_kernel<PREC_HALF><<<c.grid, c.block, 0, st>>>(Vh, nrhs, x, r, p, s, state, red); break;
-  }
-  return cudaGetLastError();
-}
-
 // x += alpha p (solver_CG.cpp:131-136, deferred from the fused r update)
 // and p = p*(rr/rrp) + r (solver_CG.cpp:150-153).  The x update runs for
 // every right-hand side whose iteration just completed (CGState::xpend), also
